@@ -1,0 +1,222 @@
+"""ctypes bindings to the oracle libraries.  TEST INFRASTRUCTURE: imported only
+by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg.
+
+* `RefLib`  - the reference renderer's own path tracer compiled from its
+  sources (oracle/_ref/libxyzref_{thinlens,pinhole}.so, see oracle/Makefile).
+* `PortLib` - the plain-C restatement of the same algorithm
+  (oracle/_port/libxyzport.so built from oracle/xyz_oracle.c).
+
+Both take the same scene arrays as the CUDA library and read the same Philox
+stream per (pixel, sample), so results can be compared path by path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+PORT_DIR = os.path.join(HERE, "_port")
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def ref_available(pinhole: bool = True) -> bool:
+    return os.path.exists(_ref_path(pinhole))
+
+
+def _ref_path(pinhole: bool) -> str:
+    return os.path.join(REF_DIR, "libxyzref_pinhole.so" if pinhole else "libxyzref_thinlens.so")
+
+
+def port_available() -> bool:
+    return os.path.exists(os.path.join(PORT_DIR, "libxyzport.so"))
+
+
+class _Common:
+    """Shared scene/camera/render plumbing of the two oracle libraries."""
+
+    prefix = ""
+
+    def _sym(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def set_path_params(self, max_depth: int, rr_threshold: float = 0.2, rr_start: int = 1):
+        """max_depth = maximum number of path segments (the reference's kMax - 1)."""
+        self._set_path(max_depth + 1, rr_threshold, rr_start)
+
+    def light_power_xyz(self):
+        out = np.zeros(3, np.float32)
+        self._sym("light_power_xyz")(out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def set_camera(self, cam, width: int, height: int):
+        eye = _f(cam.eye)
+        at = _f(cam.at)
+        self._sym("set_camera")(eye.ctypes.data_as(C.c_void_p), at.ctypes.data_as(C.c_void_p),
+                                C.c_float(cam.film_size), C.c_float(cam.focal_length),
+                                C.c_float(cam.f_number), width, height)
+        self.width, self.height = width, height
+
+    def trace(self, org, dirs, nthreads: int = 0):
+        org, dirs = _f(org), _f(dirs)
+        n = org.shape[0]
+        tri = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        f = np.empty(n, np.float32)
+        g = np.empty(n, np.float32)
+        back = np.empty(n, np.int32)
+        self._sym("trace")(n, org.ctypes.data_as(C.c_void_p), dirs.ctypes.data_as(C.c_void_p),
+                           tri.ctypes.data_as(C.c_void_p), t.ctypes.data_as(C.c_void_p),
+                           f.ctypes.data_as(C.c_void_p), g.ctypes.data_as(C.c_void_p),
+                           back.ctypes.data_as(C.c_void_p), nthreads)
+        return tri, t, f, g, back
+
+    def eval_path(self, px: int, py: int, s: int, seed: int):
+        out = np.zeros(3, np.float32)
+        dims = self._sym("eval_path")(px, py, s, C.c_uint64(seed), out.ctypes.data_as(C.c_void_p))
+        return out, dims
+
+    def render(self, spp: int, seed: int, s0: int = 0, y0: int = 0, y1=None,
+               film=None, nthreads: int = 0):
+        """Sum (not mean) of `spp` samples per pixel, film (H, W, 3) float32."""
+        if y1 is None:
+            y1 = self.height
+        if film is None:
+            film = np.zeros((self.height, self.width, 3), np.float32)
+        self._sym("render")(s0, spp, C.c_uint64(seed), y0, y1,
+                            film.ctypes.data_as(C.c_void_p), nthreads)
+        return film
+
+
+class RefLib(_Common):
+    prefix = "xyzref_"
+
+    def __init__(self, pinhole: bool = True):
+        path = _ref_path(pinhole)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference oracle not built: {path} (run make -C oracle)")
+        self.lib = C.CDLL(path)
+        L = self.lib
+        L.xyzref_scene_create.restype = C.c_int
+        L.xyzref_scene_create.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.xyzref_set_camera.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float,
+                                        C.c_int, C.c_int]
+        L.xyzref_set_path_params.argtypes = [C.c_int, C.c_float]
+        L.xyzref_trace.argtypes = [C.c_int] + [C.c_void_p] * 7 + [C.c_int]
+        L.xyzref_eval_path.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_void_p]
+        L.xyzref_eval_path.restype = C.c_int
+        L.xyzref_render.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_void_p, C.c_int]
+        L.xyzref_light_area.restype = C.c_float
+        L.xyzref_max_threads.restype = C.c_int
+        self.pinhole = bool(L.xyzref_is_pinhole())
+        self.kind = "reference"
+
+    def _set_path(self, kmax, rr_threshold, rr_start):
+        if rr_start != 1:
+            raise ValueError("the reference applies Russian roulette from the first vertex")
+        self.lib.xyzref_set_path_params(kmax, rr_threshold)
+
+    def scene_create(self, sd, kd_max_bucket: int = 16, kd_max_depth: int = 16):
+        """Loads a SceneData.  The reference scales every light by one global
+        Mercury-arc power (xyz/core/config.hpp:81-95); `light_scale` maps its
+        per-channel output to the scene's own Phi (the estimator is linear in
+        Phi per channel)."""
+        pos, tris, mat = _f(sd.positions), _i(sd.tris), _i(sd.tri_mat)
+        alb, lit = _f(sd.albedo_xyz), _i(sd.is_light)
+        nrm = _f(sd.normals) if sd.normals is not None else None
+        r = self.lib.xyzref_scene_create(pos.shape[0], pos.ctypes.data_as(C.c_void_p),
+                                         None if nrm is None else nrm.ctypes.data_as(C.c_void_p),
+                                         tris.shape[0], tris.ctypes.data_as(C.c_void_p),
+                                         mat.ctypes.data_as(C.c_void_p), alb.shape[0],
+                                         alb.ctypes.data_as(C.c_void_p), lit.ctypes.data_as(C.c_void_p),
+                                         kd_max_bucket, kd_max_depth)
+        if r < 0:
+            raise ValueError("reference rejected the scene")
+        self.light_scale = (np.asarray(sd.light_power_xyz, np.float64) /
+                            self.light_power_xyz().astype(np.float64))
+        self._keep = (pos, tris, mat, alb, lit, nrm)
+        return r
+
+    def max_threads(self):
+        return self.lib.xyzref_max_threads()
+
+
+class PortLib(_Common):
+    prefix = "xyzo_"
+
+    def __init__(self):
+        path = os.path.join(PORT_DIR, "libxyzport.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle port not built: {path} (run make -C oracle port)")
+        self.lib = C.CDLL(path)
+        L = self.lib
+        L.xyzo_scene_create.restype = C.c_int
+        L.xyzo_scene_create.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                        C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_int, C.c_int]
+        L.xyzo_set_camera_full.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float,
+                                           C.c_int, C.c_int, C.c_int]
+        L.xyzo_set_path_params.argtypes = [C.c_int, C.c_float, C.c_int]
+        L.xyzo_trace.argtypes = [C.c_int] + [C.c_void_p] * 7 + [C.c_int]
+        L.xyzo_eval_path.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_void_p]
+        L.xyzo_eval_path.restype = C.c_int
+        L.xyzo_render.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_void_p, C.c_int]
+        L.xyzo_light_area.restype = C.c_float
+        L.xyzo_max_threads.restype = C.c_int
+        L.xyzo_philox_u01.restype = C.c_float
+        L.xyzo_philox_u01.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.xyzo_kdtree_stats.argtypes = [C.c_void_p]
+        self.kind = "port"
+        self.light_scale = np.ones(3)
+
+    def _set_path(self, kmax, rr_threshold, rr_start):
+        self.lib.xyzo_set_path_params(kmax, rr_threshold, rr_start)
+
+    def set_camera(self, cam, width: int, height: int):
+        eye = _f(cam.eye)
+        at = _f(cam.at)
+        self.lib.xyzo_set_camera_full(eye.ctypes.data_as(C.c_void_p), at.ctypes.data_as(C.c_void_p),
+                                      C.c_float(cam.film_size), C.c_float(cam.focal_length),
+                                      C.c_float(cam.f_number), width, height, int(cam.pinhole))
+        self.width, self.height = width, height
+
+    def scene_create(self, sd, kd_max_bucket: int = 16, kd_max_depth: int = 16):
+        pos, tris, mat = _f(sd.positions), _i(sd.tris), _i(sd.tri_mat)
+        alb, lit = _f(sd.albedo_xyz), _i(sd.is_light)
+        nrm = _f(sd.normals) if sd.normals is not None else None
+        pw = _f(sd.light_power_xyz)
+        r = self.lib.xyzo_scene_create(pos.shape[0], pos.ctypes.data_as(C.c_void_p),
+                                       None if nrm is None else nrm.ctypes.data_as(C.c_void_p),
+                                       tris.shape[0], tris.ctypes.data_as(C.c_void_p),
+                                       mat.ctypes.data_as(C.c_void_p), alb.shape[0],
+                                       alb.ctypes.data_as(C.c_void_p), lit.ctypes.data_as(C.c_void_p),
+                                       pw.ctypes.data_as(C.c_void_p), kd_max_bucket, kd_max_depth)
+        if r < 0:
+            raise ValueError("oracle port rejected the scene")
+        self._keep = (pos, tris, mat, alb, lit, nrm, pw)
+        return r
+
+    def philox_u01(self, seed, pixel, sample, dim):
+        return self.lib.xyzo_philox_u01(C.c_uint64(seed), pixel, sample, dim)
+
+    def kdtree_stats(self):
+        out = np.zeros(8, np.int64)
+        self.lib.xyzo_kdtree_stats(out.ctypes.data_as(C.c_void_p))
+        return dict(zip(["nodes", "leaves", "empty_leaves", "refs", "max_depth", "tris", "_6", "_7"],
+                        out.tolist()))
+
+    def max_threads(self):
+        return self.lib.xyzo_max_threads()

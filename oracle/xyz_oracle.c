@@ -1,0 +1,793 @@
+/* Plain-C restatement of the reference renderer's path-tracing hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's
+ * CPU-baseline leg load this (oracle/_port/libxyzport.so); the CUDA product
+ * never does.  It is pinned to the reference itself: tests compare it with the
+ * reference's own code compiled from its sources (oracle/_ref, ref_harness.cpp)
+ * and with golden fixtures generated from that build (tests/golden/).
+ *
+ * What it restates, step for step and with the reference's float/double
+ * promotions (hi::basic_vector3 arithmetic promotes float x double to double,
+ * libhi/hi/math/vector3.hpp:75-94, promote_traits.hpp:45-50):
+ *   kd-tree build     KDTree::Build           xyz/geom/kdtree.cpp:207-357
+ *   kd-tree traversal KDNode/KDLeaf/KDTree    xyz/geom/kdtree.cpp:82-150,366-372
+ *   ray/triangle      FindIntersectionDF      xyz/geom/triangle.cpp:127-165
+ *   shading basis     Triangle::ShadingBasis  xyz/geom/triangle.cpp:194-219
+ *   light sampling    Scene::SampleLightPosition xyz/core/scene.cpp:42-78,
+ *                     Triangle::Sample        xyz/geom/triangle.cpp:232-263
+ *   camera            ThinLensCamera          xyz/core/thinlenscamera.cpp:71-205
+ *   estimator         Scene::EvalutePathTracing xyz/core/scene_pathtracing.cpp:11-144
+ *   NEE               Lambert::CalculateWeightedDirectLighting xyz/bsdf/lambert.cpp:125-173
+ *   BSDF sampling     Lambert::NextScatteringDirection xyz/bsdf/lambert.cpp:176-187,
+ *                     ComputeDiffusedVector   xyz/stdafx.hpp:50-63
+ *   film              PathTracer::run         xyz/integrator/integrator.cpp:119-128
+ *
+ * Random numbers: the Philox stream of philox.h, read in the order the
+ * reference consumes IPrimarySample::next() when built with g++.  g++ evaluates
+ * the two `sample.next()` arguments of SampleLightPosition,
+ * SampleLensPosition and ComputeDiffusedVector right to left, so the first draw
+ * feeds the second parameter.
+ *
+ * Extensions beyond the reference (off by default, used to check the CUDA
+ * path's options): `rr_start` (first vertex index that plays Russian roulette;
+ * the reference plays it from vertex 1) and a run-time pinhole switch (the
+ * reference selects it at compile time, CONFIG_PINHOLE_CAMERA_MODEL).
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#include "philox.h"
+
+#define XYZO_EPSILON 1e-6f                 /* xyz/stdafx.hpp:36 */
+#define XYZO_TMIN 1e-5f                    /* xyz/geom/intersection.hpp:12 */
+#define XYZO_M_1_PI 0.318309886183790671538 /* M_1_PI (double) */
+#define XYZO_M_PI 3.14159265358979323846
+
+typedef struct {
+  float x, y, z;
+} f3;
+
+static inline f3 mk(float x, float y, float z) {
+  f3 r = {x, y, z};
+  return r;
+}
+static inline float at3(f3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+static inline f3 add3(f3 a, f3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline f3 sub3(f3 a, f3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline f3 mul3(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline f3 scale3(f3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+static inline f3 neg3(f3 a) { return mk(-a.x, -a.y, -a.z); }
+/* hi::dot (vector3.hpp:120): a0*b0 + a1*b1 + a2*b2, left to right. */
+static inline float dot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+/* hi::cross (vector3.hpp:126-131). */
+static inline f3 cross3(f3 a, f3 b) {
+  return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+/* hi::normalize = a * rsqrt(length_squared(a)), rsqrt = 1/sqrt (math.hpp:155). */
+static inline f3 normalize3(f3 a) {
+  float const r = 1.0f / sqrtf(dot3(a, a));
+  return scale3(a, r);
+}
+
+/* ------------------------------------------------------------------ scene */
+typedef struct {
+  int nt, nm, nl;
+  f3 *v0, *e1, *e2, *ng, *n0, *s1, *s2;
+  int *mat;
+  f3 *albedo;
+  int *is_light;
+  int *lights;   /* light triangle ids in triangle order */
+  float *cdf;    /* nl + 1 entries, cdf[0] = 0 */
+  f3 power;      /* Phi, XYZ */
+  /* kd-tree (reference structure: interior / leaf / null nodes) */
+  int nnodes, cap_nodes;
+  int *kaxis;    /* 0..2 interior, -1 leaf, -2 null */
+  float *kvalue;
+  int *kchild;   /* 2 per node */
+  int *kbegin, *kcount;
+  int *refs;
+  int nrefs, cap_refs, kmaxdepth_seen;
+  f3 kmin, kmax;
+  size_t max_bucket, max_depth;
+} scene_t;
+
+typedef struct {
+  f3 eye, at;
+  float film, focal, fnum, aspect;
+  float L, V, R;
+  f3 right, up, back;
+  int pinhole, W, H;
+} camera_t;
+
+static scene_t S;
+static camera_t CAM;
+static size_t KMAX = 16;
+static float RR_THRESHOLD = 0.2f;
+static int RR_START = 1;
+
+/* Triangle::min(k)/max(k) without cached bounds (triangle.hpp:142-156). */
+static inline float tmin_k(int i, int k) {
+  float a = at3(S.v0[i], k), b = a + at3(S.e1[i], k), c = a + at3(S.e2[i], k);
+  float m = a;
+  if (b < m) m = b;
+  if (c < m) m = c;
+  return m;
+}
+static inline float tmax_k(int i, int k) {
+  float a = at3(S.v0[i], k), b = a + at3(S.e1[i], k), c = a + at3(S.e2[i], k);
+  float m = a;
+  if (b > m) m = b;
+  if (c > m) m = c;
+  return m;
+}
+
+/* ---------------------------------------------------------- kd-tree build */
+typedef struct {
+  int type; /* 0 open, 1 close */
+  float value;
+} event_t;
+
+static int event_cmp(const void *pa, const void *pb) {
+  const event_t *a = (const event_t *)pa, *b = (const event_t *)pb;
+  if (a->value < b->value) return -1;
+  if (a->value > b->value) return 1;
+  return a->type - b->type; /* open < close on ties */
+}
+
+static int new_node(void) {
+  if (S.nnodes == S.cap_nodes) {
+    S.cap_nodes = S.cap_nodes ? 2 * S.cap_nodes : 1024;
+    S.kaxis = (int *)realloc(S.kaxis, sizeof(int) * S.cap_nodes);
+    S.kvalue = (float *)realloc(S.kvalue, sizeof(float) * S.cap_nodes);
+    S.kchild = (int *)realloc(S.kchild, sizeof(int) * 2 * S.cap_nodes);
+    S.kbegin = (int *)realloc(S.kbegin, sizeof(int) * S.cap_nodes);
+    S.kcount = (int *)realloc(S.kcount, sizeof(int) * S.cap_nodes);
+  }
+  int n = S.nnodes++;
+  S.kaxis[n] = -2;
+  S.kvalue[n] = 0;
+  S.kchild[2 * n] = S.kchild[2 * n + 1] = -1;
+  S.kbegin[n] = S.kcount[n] = 0;
+  return n;
+}
+
+static int add_leaf(const int *set, int n) {
+  int node = new_node();
+  if (n == 0) return node; /* KDNull */
+  if (S.nrefs + n > S.cap_refs) {
+    while (S.nrefs + n > S.cap_refs) S.cap_refs = S.cap_refs ? 2 * S.cap_refs : 4096;
+    S.refs = (int *)realloc(S.refs, sizeof(int) * S.cap_refs);
+  }
+  S.kaxis[node] = -1;
+  S.kbegin[node] = S.nrefs;
+  S.kcount[node] = n;
+  memcpy(S.refs + S.nrefs, set, sizeof(int) * n);
+  S.nrefs += n;
+  return node;
+}
+
+/* KDTree::Build(set, min, max, depth), xyz/geom/kdtree.cpp:226-357. */
+static int build_rec(const int *set, int n, f3 bmin, f3 bmax, size_t depth) {
+  if (depth > (size_t)S.kmaxdepth_seen) S.kmaxdepth_seen = (int)depth;
+  if ((size_t)n <= S.max_bucket || depth > S.max_depth) return add_leaf(set, n);
+  depth++;
+  f3 const range = sub3(bmax, bmin);
+  int axis = -1;
+  float value = NAN;
+  float min_cost = 3.402823466e+38f; /* numeric_limits<float>::max() */
+  event_t *ev = (event_t *)malloc(sizeof(event_t) * 2 * (size_t)n);
+  for (int k = 0; k < 3; ++k) {
+    for (int i = 0; i < n; ++i) {
+      ev[i].type = 0;
+      ev[i].value = tmin_k(set[i], k);
+      ev[i + n].type = 1;
+      ev[i + n].value = tmax_k(set[i], k) + XYZO_EPSILON;
+    }
+    qsort(ev, 2 * (size_t)n, sizeof(event_t), event_cmp);
+    float const a = at3(range, (k + 1) % 3) * at3(range, (k + 2) % 3);
+    float const b = at3(range, (k + 1) % 3) + at3(range, (k + 2) % 3);
+    size_t n_left = 0, n_right = (size_t)n;
+#define XYZO_UPDATE(vv)                                                     \
+  do {                                                                      \
+    float const r = (vv) - at3(bmin, k);                                    \
+    float const sa_left = a + b * r;                                        \
+    float const sa_right = a + b * (at3(range, k) - r);                     \
+    float const cost = (float)n_left * sa_left + (float)n_right * sa_right; \
+    if (min_cost > cost) {                                                  \
+      min_cost = cost;                                                      \
+      axis = k;                                                             \
+      value = (vv);                                                         \
+    }                                                                       \
+  } while (0)
+    {
+      float const v = ev[0].value - XYZO_EPSILON;
+      XYZO_UPDATE(v);
+    }
+    size_t const size = 2 * (size_t)n;
+    for (size_t i = 0; i < size; ++i) {
+      if (ev[i].type) {
+        n_right--;
+      } else {
+        n_left++;
+      }
+      float v = ev[i].value;
+      if (i + 1 < size) {
+        if (v == ev[i + 1].value) continue;
+      } else {
+        v += XYZO_EPSILON;
+      }
+      XYZO_UPDATE(v);
+    }
+#undef XYZO_UPDATE
+  }
+  free(ev);
+  int *left = (int *)malloc(sizeof(int) * (size_t)n);
+  int *right = (int *)malloc(sizeof(int) * (size_t)n);
+  int nl = 0, nr = 0;
+  for (int i = 0; i < n; ++i) {
+    /* Triangle::Overlap (triangle.cpp:75-85) */
+    if (tmax_k(set[i], axis) < value) {
+      left[nl++] = set[i];
+    } else if (value <= tmin_k(set[i], axis)) {
+      right[nr++] = set[i];
+    } else {
+      left[nl++] = set[i];
+      right[nr++] = set[i];
+    }
+  }
+  int node = new_node();
+  S.kaxis[node] = axis;
+  S.kvalue[node] = value;
+  f3 max_left = bmax, min_right = bmin;
+  if (axis == 0) max_left.x = value, min_right.x = value;
+  if (axis == 1) max_left.y = value, min_right.y = value;
+  if (axis == 2) max_left.z = value, min_right.z = value;
+  int c0 = build_rec(left, nl, bmin, max_left, depth);
+  S.kchild[2 * node] = c0;
+  free(left);
+  int c1 = build_rec(right, nr, min_right, bmax, depth);
+  S.kchild[2 * node + 1] = c1;
+  free(right);
+  return node;
+}
+
+static void kd_build(void) {
+  S.nnodes = 0;
+  S.nrefs = 0;
+  S.kmaxdepth_seen = 0;
+  f3 mn = mk(INFINITY, INFINITY, INFINITY), mx = mk(-INFINITY, -INFINITY, -INFINITY);
+  for (int i = 0; i < S.nt; ++i) {
+    float v;
+    v = tmin_k(i, 0); if (mn.x > v) mn.x = v;
+    v = tmin_k(i, 1); if (mn.y > v) mn.y = v;
+    v = tmin_k(i, 2); if (mn.z > v) mn.z = v;
+    v = tmax_k(i, 0); if (mx.x < v) mx.x = v;
+    v = tmax_k(i, 1); if (mx.y < v) mx.y = v;
+    v = tmax_k(i, 2); if (mx.z < v) mx.z = v;
+  }
+  mx = add3(mx, scale3(sub3(mx, mn), 1e-5f)); /* kdtree.cpp:215-216 */
+  S.kmin = mn;
+  S.kmax = mx;
+  int *all = (int *)malloc(sizeof(int) * (size_t)(S.nt > 0 ? S.nt : 1));
+  for (int i = 0; i < S.nt; ++i) all[i] = i;
+  build_rec(all, S.nt, mn, mx, 0);
+  free(all);
+}
+
+/* ------------------------------------------------------------- traversal */
+typedef struct {
+  float tmin, tmax, f, g;
+  int back;
+} isect_t;
+
+/* Triangle::FindIntersectionDF, xyz/geom/triangle.cpp:127-165. */
+static inline int tri_hit(int i, f3 o, f3 d, isect_t *p) {
+  f3 const e2xe1 = cross3(S.e2[i], S.e1[i]);
+  float const det = dot3(d, e2xe1);
+  if (fabsf(det) < XYZO_EPSILON) return 0;
+  float const inv_det = 1.0f / det;
+  f3 const vmo = sub3(S.v0[i], o);
+  float const t = inv_det * dot3(vmo, e2xe1);
+  if ((t < p->tmin) || (p->tmax < t)) return 0;
+  f3 const dxvmo = cross3(d, vmo);
+  float const f = inv_det * dot3(S.e2[i], dxvmo);
+  if ((f < 0) || (f > 1)) return 0;
+  float const g = inv_det * -dot3(S.e1[i], dxvmo);
+  if ((g < 0) || ((f + g) > 1)) return 0;
+  p->tmax = t;
+  p->f = f;
+  p->g = g;
+  p->back = det > 0;
+  return 1;
+}
+
+static int find_rec(int node, f3 o, f3 d, isect_t *p) {
+  int const ax = S.kaxis[node];
+  if (ax == -2) return -1;
+  if (ax == -1) {
+    int s = -1;
+    for (int j = 0; j < S.kcount[node]; ++j) {
+      int const i = S.refs[S.kbegin[node] + j];
+      if (tri_hit(i, o, d, p)) s = i;
+    }
+    return s;
+  }
+  float const v = S.kvalue[node];
+  float const e = (v - at3(o, ax)) / at3(d, ax);
+  int const side = at3(o, ax) < v;
+  int const nearc = S.kchild[2 * node + (1 - side)];
+  int const farc = S.kchild[2 * node + side];
+  if ((e > p->tmax) || (e < 0)) {
+    return find_rec(nearc, o, d, p);
+  } else if (e < p->tmin) {
+    return find_rec(farc, o, d, p);
+  } else {
+    float const tmax = p->tmax;
+    p->tmax = e;
+    int const s = find_rec(nearc, o, d, p);
+    if (s >= 0) return s;
+    p->tmin = e;
+    p->tmax = tmax;
+    return find_rec(farc, o, d, p);
+  }
+}
+
+static int find_intersection(f3 o, f3 d, isect_t *p) {
+  p->tmin = XYZO_TMIN;
+  p->tmax = INFINITY;
+  if (S.nnodes == 0) return -1;
+  return find_rec(0, o, d, p);
+}
+
+/* ---------------------------------------------------------------- camera */
+static void camera_reset(void) {
+  f3 const view = sub3(CAM.eye, CAM.at);
+  CAM.L = sqrtf(dot3(view, view));
+  CAM.V = CAM.L * CAM.focal / (CAM.L - CAM.focal);
+  CAM.R = CAM.focal / (2 * CAM.fnum);
+  CAM.back = normalize3(view);
+  CAM.right = normalize3(cross3(mk(0, 1, 0), CAM.back));
+  CAM.up = cross3(CAM.back, CAM.right);
+}
+
+/* ------------------------------------------------------------- estimator */
+typedef struct {
+  f3 pos, sn, gn, tan, bin;
+} frame_t;
+
+/* Triangle::ShadingBasis (triangle.cpp:194-219). */
+static void shading_basis(int i, float f, float g, int back, frame_t *fr) {
+  f3 sn = normalize3(add3(add3(S.n0[i], scale3(S.s1[i], f)), scale3(S.s2[i], g)));
+  f3 gn = S.ng[i];
+  if (back) {
+    gn = neg3(gn);
+    sn = neg3(sn);
+  }
+  f3 t = mk(-sn.z, 0, sn.x);
+  float const l2 = dot3(t, t);
+  if (l2 > 0) {
+    t = scale3(t, 1.0f / sqrtf(l2));
+    fr->bin = cross3(t, sn);
+  } else {
+    fr->bin = mk(0, 0, (sn.y > 0) ? 1.0f : -1.0f);
+    t = cross3(sn, fr->bin);
+  }
+  fr->tan = t;
+  fr->sn = sn;
+  fr->gn = gn;
+}
+
+static float light_area(void) { return S.cdf[S.nl]; }
+
+/* float3 * double (promoted) accumulated into a float3 with per-component
+ * narrowing, as `*pColor += vector3<double>` does. */
+static inline void acc_d(f3 *c, double x, double y, double z) {
+  c->x += (float)x;
+  c->y += (float)y;
+  c->z += (float)z;
+}
+
+static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
+  xyzo_stream st;
+  xyzo_stream_init(&st, seed, (uint32_t)(py * CAM.W + px), (uint32_t)s, 0u);
+  float const jx = xyzo_stream_next(&st);
+  float const jy = xyzo_stream_next(&st);
+  float const x = ((float)px + jx) / (float)CAM.W;
+  float const y = ((float)py + jy) / (float)CAM.H;
+  *color = mk(0, 0, 0);
+
+  /* SampleLightPosition(s = second draw, t = first draw) */
+  float const lt = xyzo_stream_next(&st);
+  float const ls = xyzo_stream_next(&st);
+  int has_light = S.nl > 0;
+  f3 lpos = mk(0, 0, 0), lsn = mk(0, 0, 0), lgn = mk(0, 0, 0);
+  if (has_light) {
+    float const u = ls * S.cdf[S.nl];
+    int lo = 0, hi = S.nl + 1; /* upper_bound over cdf[0..nl] */
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (!(u < S.cdf[mid])) lo = mid + 1; else hi = mid;
+    }
+    int const n = lo - 1;
+    float const v = (u - S.cdf[n]) / (S.cdf[n + 1] - S.cdf[n]);
+    int const li = S.lights[n];
+    float const ss = sqrtf(v);
+    float const tt = lt;
+    float const uu = ss * (1 - tt);
+    float const vv = ss * tt;
+    lpos = add3(add3(S.v0[li], scale3(S.e1[li], uu)), scale3(S.e2[li], vv));
+    lsn = normalize3(add3(add3(S.n0[li], scale3(S.s1[li], uu)), scale3(S.s2[li], vv)));
+    lgn = S.ng[li];
+  }
+  f3 const lpow = S.power;
+
+  /* camera vertex */
+  f3 pos, dir;
+  f3 beta = mk(1, 1, 1);
+  int specular = 1;
+  float fSamplingNext = 0;
+  if (CAM.pinhole) {
+    pos = CAM.eye;
+    float const lx = (float)(((double)x - 0.5) * (double)CAM.film * (double)CAM.aspect);
+    float const ly = (float)(((double)y - 0.5) * (double)CAM.film);
+    float const lz = -CAM.V;
+    dir = normalize3(add3(add3(scale3(CAM.right, lx), scale3(CAM.up, ly)), scale3(CAM.back, lz)));
+  } else {
+    float const ct = xyzo_stream_next(&st);
+    float const cs = xyzo_stream_next(&st);
+    /* SampleDisk (thinlenscamera.cpp:4-15): the angle is stored as float */
+    float const radius = CAM.R * sqrtf(cs);
+    float const ang = (float)((2 * XYZO_M_PI) * (double)ct);
+    float const lensx = radius * cosf(ang);
+    float const lensy = radius * sinf(ang);
+    pos = add3(add3(CAM.eye, scale3(CAM.right, lensx)), scale3(CAM.up, lensy));
+    float const fps = CAM.film * CAM.L / CAM.V;
+    float const lx = (float)(((double)x - 0.5) * (double)fps * (double)CAM.aspect - (double)lensx);
+    float const ly = (float)(((double)y - 0.5) * (double)fps - (double)lensy);
+    float const lz = -CAM.L;
+    dir = normalize3(add3(add3(scale3(CAM.right, lx), scale3(CAM.up, ly)), scale3(CAM.back, lz)));
+  }
+
+  float const A = light_area();
+  for (size_t k = 1;;) {
+    isect_t p;
+    int const tri = find_intersection(pos, dir, &p);
+    if (tri < 0) break;
+    frame_t fr;
+    shading_basis(tri, p.f, p.g, p.back, &fr);
+    if (-dot3(dir, fr.sn) <= 0) break;
+    pos = add3(pos, scale3(dir, p.tmax));
+    int const m = S.mat[tri];
+    if (S.is_light[m] && !p.back) {
+      f3 const pb = mul3(lpow, beta);
+      if (specular) {
+        double const w = XYZO_M_1_PI / (double)A;
+        acc_d(color, (double)pb.x * w, (double)pb.y * w, (double)pb.z * w);
+      } else {
+        float const cosv = fabsf(dot3(dir, fr.sn));
+        float const d2 = p.tmax * p.tmax;
+        float const dimp = fSamplingNext * cosv / d2;
+        float const dexp = 1.0f / A;
+        float const dens = dexp / dimp;
+        double const w = XYZO_M_1_PI / (double)A;
+        float const mis = 1.0f / (1 + dens * dens);
+        acc_d(color, (double)pb.x * w * (double)mis, (double)pb.y * w * (double)mis,
+              (double)pb.z * w * (double)mis);
+      }
+      break;
+    }
+    if (++k >= KMAX) break;
+
+    /* NEE (Lambert::CalculateWeightedDirectLighting); a light's NEE is zero
+     * and leaves the throughput alone (xyz/bsdf/light.cpp:18-25). */
+    if (!S.is_light[m]) beta = mul3(beta, S.albedo[m]);
+    if (has_light && !S.is_light[m]) {
+      f3 const vin = normalize3(sub3(pos, lpos));
+      float const nk3 = dot3(vin, lgn);
+      if (!((nk3 <= 0) || (dot3(vin, lsn) <= 0))) {
+        float const nk2 = -dot3(vin, fr.sn);
+        if (!((nk2 <= 0) || (-dot3(vin, fr.gn) <= 0))) {
+          isect_t q;
+          if (find_intersection(lpos, vin, &q) == tri) {
+            float const G = nk2 * nk3 / (q.tmax * q.tmax);
+            float const dimp = (float)(XYZO_M_1_PI * (double)G);
+            float const dexp = 1.0f / A;
+            float const dens = dimp / dexp;
+            double const w =
+                ((double)G * (XYZO_M_1_PI * XYZO_M_1_PI)) * (double)(1.0f / (1 + dens * dens));
+            f3 const pb = mul3(lpow, beta);
+            f3 const c = mk((float)((double)pb.x * w), (float)((double)pb.y * w),
+                            (float)((double)pb.z * w));
+            *color = add3(*color, c);
+          }
+        }
+      }
+    }
+
+    /* Russian roulette */
+    if ((int)k - 1 >= RR_START) {
+      float const t = beta.y;
+      if (t < RR_THRESHOLD) {
+        float const q = t / RR_THRESHOLD;
+        if (xyzo_stream_next(&st) >= q) break;
+        beta = scale3(beta, 1.0f / q);
+      }
+    }
+
+    /* Light::NextScatteringDirection ends the path (xyz/bsdf/light.cpp:27-31). */
+    if (S.is_light[m]) break;
+
+    /* Lambert::NextScatteringDirection: fMuPhi = first draw, fMuTheta = second */
+    float const mu_phi = xyzo_stream_next(&st);
+    float const mu_theta = xyzo_stream_next(&st);
+    specular = 0;
+    float const phi = (float)(2 * XYZO_M_PI) * mu_phi;
+    float const cos_t = sqrtf(mu_theta);
+    float const sin_t = sqrtf(1 - mu_theta);
+    dir = add3(add3(scale3(fr.tan, sin_t * cosf(phi)), scale3(fr.bin, sin_t * sinf(phi))),
+               scale3(fr.sn, cos_t));
+    fSamplingNext = (float)(XYZO_M_1_PI * (double)cos_t);
+    if (!(dot3(dir, fr.gn) > 0)) break;
+  }
+  return (int)st.dim;
+}
+
+/* --------------------------------------------------------------- C API */
+static void free_scene(void) {
+  free(S.v0); free(S.e1); free(S.e2); free(S.ng); free(S.n0); free(S.s1); free(S.s2);
+  free(S.mat); free(S.albedo); free(S.is_light); free(S.lights); free(S.cdf);
+  free(S.kaxis); free(S.kvalue); free(S.kchild); free(S.kbegin); free(S.kcount); free(S.refs);
+  memset(&S, 0, sizeof(S));
+}
+
+int xyzo_scene_create(int nv, const float *pos, const float *nrm, int nt, const int *tri,
+                      const int *tri_mat, int nm, const float *albedo, const int *is_light,
+                      const float *power, int kd_max_bucket, int kd_max_depth) {
+  free_scene();
+  S.nt = nt;
+  S.nm = nm;
+  S.v0 = (f3 *)malloc(sizeof(f3) * (size_t)(nt + 1));
+  S.e1 = (f3 *)malloc(sizeof(f3) * (size_t)(nt + 1));
+  S.e2 = (f3 *)malloc(sizeof(f3) * (size_t)(nt + 1));
+  S.ng = (f3 *)malloc(sizeof(f3) * (size_t)(nt + 1));
+  S.n0 = (f3 *)malloc(sizeof(f3) * (size_t)(nt + 1));
+  S.s1 = (f3 *)malloc(sizeof(f3) * (size_t)(nt + 1));
+  S.s2 = (f3 *)malloc(sizeof(f3) * (size_t)(nt + 1));
+  S.mat = (int *)malloc(sizeof(int) * (size_t)(nt + 1));
+  S.albedo = (f3 *)malloc(sizeof(f3) * (size_t)(nm + 1));
+  S.is_light = (int *)malloc(sizeof(int) * (size_t)(nm + 1));
+  S.lights = (int *)malloc(sizeof(int) * (size_t)(nt + 1));
+  S.cdf = (float *)malloc(sizeof(float) * (size_t)(nt + 2));
+  for (int m = 0; m < nm; ++m) {
+    S.albedo[m] = mk(albedo[3 * m], albedo[3 * m + 1], albedo[3 * m + 2]);
+    S.is_light[m] = is_light[m] != 0;
+  }
+  S.cdf[0] = 0;
+  S.nl = 0;
+  for (int i = 0; i < nt; ++i) {
+    int const a = tri[3 * i], b = tri[3 * i + 1], c = tri[3 * i + 2];
+    int const m = tri_mat[i];
+    if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv || m < 0 || m >= nm) {
+      free_scene();
+      return -1;
+    }
+    f3 const p0 = mk(pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]);
+    f3 const p1 = mk(pos[3 * b], pos[3 * b + 1], pos[3 * b + 2]);
+    f3 const p2 = mk(pos[3 * c], pos[3 * c + 1], pos[3 * c + 2]);
+    S.v0[i] = p0;
+    S.e1[i] = sub3(p1, p0);
+    S.e2[i] = sub3(p2, p0);
+    S.ng[i] = normalize3(cross3(S.e2[i], S.e1[i])); /* NormalVector (triangle.hpp:202) */
+    if (nrm) {
+      f3 const m0 = mk(nrm[3 * a], nrm[3 * a + 1], nrm[3 * a + 2]);
+      f3 const m1 = mk(nrm[3 * b], nrm[3 * b + 1], nrm[3 * b + 2]);
+      f3 const m2 = mk(nrm[3 * c], nrm[3 * c + 1], nrm[3 * c + 2]);
+      S.n0[i] = m0;
+      S.s1[i] = sub3(m1, m0);
+      S.s2[i] = sub3(m2, m0);
+    } else {
+      S.n0[i] = S.ng[i];
+      S.s1[i] = mk(0, 0, 0);
+      S.s2[i] = mk(0, 0, 0);
+    }
+    S.mat[i] = m;
+    if (S.is_light[m]) {
+      f3 const cr = cross3(S.e2[i], S.e1[i]);
+      float const area = sqrtf(dot3(cr, cr)) * 0.5f; /* Triangle::area */
+      S.lights[S.nl] = i;
+      S.cdf[S.nl + 1] = S.cdf[S.nl] + area;
+      S.nl++;
+    }
+  }
+  S.power = mk(power[0], power[1], power[2]);
+  S.max_bucket = (size_t)kd_max_bucket;
+  S.max_depth = (size_t)kd_max_depth;
+  kd_build();
+  return S.nl;
+}
+
+void xyzo_scene_destroy(void) { free_scene(); }
+
+float xyzo_light_area(void) { return S.nl ? S.cdf[S.nl] : 0.0f; }
+
+void xyzo_light_power_xyz(float *out) {
+  out[0] = S.power.x;
+  out[1] = S.power.y;
+  out[2] = S.power.z;
+}
+
+void xyzo_set_path_params(int kmax, float rr_threshold, int rr_start) {
+  KMAX = (size_t)kmax;
+  RR_THRESHOLD = rr_threshold;
+  RR_START = rr_start;
+}
+
+void xyzo_set_camera_full(const float *eye, const float *at, float film, float focal, float fnum,
+                          int W, int H, int pinhole) {
+  CAM.eye = mk(eye[0], eye[1], eye[2]);
+  CAM.at = mk(at[0], at[1], at[2]);
+  CAM.film = film;
+  CAM.focal = focal;
+  CAM.fnum = fnum;
+  CAM.W = W;
+  CAM.H = H;
+  CAM.aspect = (float)W / (float)H; /* Scene::SetDimension (scene.hpp:226-230) */
+  CAM.pinhole = pinhole;
+  camera_reset();
+}
+
+void xyzo_set_camera(const float *eye, const float *at, float film, float focal, float fnum, int W,
+                     int H) {
+  xyzo_set_camera_full(eye, at, film, focal, fnum, W, H, 0);
+}
+
+float xyzo_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim) {
+  return xyzo_stream_at(seed, pixel, sample, dim);
+}
+
+/* nodes, leaves, empty leaves, leaf references, max depth, triangles */
+void xyzo_kdtree_stats(int64_t *out) {
+  int64_t leaves = 0, empty = 0;
+  for (int i = 0; i < S.nnodes; ++i) {
+    if (S.kaxis[i] == -1) leaves++;
+    if (S.kaxis[i] == -2) empty++;
+  }
+  out[0] = S.nnodes;
+  out[1] = leaves;
+  out[2] = empty;
+  out[3] = S.nrefs;
+  out[4] = S.kmaxdepth_seen;
+  out[5] = S.nt;
+  out[6] = 0;
+  out[7] = 0;
+}
+
+/* ------------------------------------------------------ threaded drivers */
+typedef struct {
+  int mode; /* 0 trace, 1 render */
+  int lo, hi, chunk;
+  volatile int next;
+  pthread_mutex_t mu;
+  /* trace */
+  const float *org, *dir;
+  int *tri;
+  float *t, *f, *g;
+  int *back;
+  /* render */
+  int s;
+  uint64_t seed;
+  float *film;
+} job_t;
+
+static int job_take(job_t *j, int *b, int *e) {
+  pthread_mutex_lock(&j->mu);
+  int const x = j->next;
+  j->next = x + j->chunk;
+  pthread_mutex_unlock(&j->mu);
+  if (x >= j->hi) return 0;
+  *b = x;
+  *e = x + j->chunk < j->hi ? x + j->chunk : j->hi;
+  return 1;
+}
+
+static void *job_worker(void *arg) {
+  job_t *j = (job_t *)arg;
+  int b, e;
+  while (job_take(j, &b, &e)) {
+    for (int i = b; i < e; ++i) {
+      if (j->mode == 0) {
+        isect_t p;
+        f3 const o = mk(j->org[3 * i], j->org[3 * i + 1], j->org[3 * i + 2]);
+        f3 const d = mk(j->dir[3 * i], j->dir[3 * i + 1], j->dir[3 * i + 2]);
+        int const t = find_intersection(o, d, &p);
+        j->tri[i] = t;
+        j->t[i] = t >= 0 ? p.tmax : 0;
+        j->f[i] = t >= 0 ? p.f : 0;
+        j->g[i] = t >= 0 ? p.g : 0;
+        j->back[i] = t >= 0 ? p.back : 0;
+      } else {
+        int const y = i;
+        for (int x = 0; x < CAM.W; ++x) {
+          f3 c;
+          eval_path(x, y, j->s, j->seed, &c);
+          float *fp = j->film + 3 * ((size_t)y * CAM.W + x);
+          fp[0] += c.x;
+          fp[1] += c.y;
+          fp[2] += c.z;
+        }
+      }
+    }
+  }
+  return NULL;
+}
+
+static int default_threads(int n) {
+  if (n > 0) return n;
+  long c = sysconf(_SC_NPROCESSORS_ONLN);
+  return c > 0 ? (int)c : 1;
+}
+
+static void run_job(job_t *j, int nthreads) {
+  nthreads = default_threads(nthreads);
+  pthread_mutex_init(&j->mu, NULL);
+  j->next = j->lo;
+  if (nthreads == 1) {
+    job_worker(j);
+  } else {
+    pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)nthreads);
+    for (int t = 0; t < nthreads; ++t) pthread_create(&th[t], NULL, job_worker, j);
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+    free(th);
+  }
+  pthread_mutex_destroy(&j->mu);
+}
+
+void xyzo_trace(int n, const float *org, const float *dir, int *tri, float *t, float *f, float *g,
+                int *back, int nthreads) {
+  job_t j;
+  memset(&j, 0, sizeof(j));
+  j.mode = 0;
+  j.lo = 0;
+  j.hi = n;
+  j.chunk = 256;
+  j.org = org;
+  j.dir = dir;
+  j.tri = tri;
+  j.t = t;
+  j.f = f;
+  j.g = g;
+  j.back = back;
+  run_job(&j, nthreads);
+}
+
+int xyzo_eval_path(int px, int py, int s, uint64_t seed, float *out) {
+  f3 c;
+  int const dims = eval_path(px, py, s, seed, &c);
+  out[0] = c.x;
+  out[1] = c.y;
+  out[2] = c.z;
+  return dims;
+}
+
+/* PathTracer::run's loop for samples [s0, s0+spp), rows [y0, y1): film += color
+ * per sample in sample order (sum, not mean). */
+void xyzo_render(int s0, int spp, uint64_t seed, int y0, int y1, float *film, int nthreads) {
+  for (int s = s0; s < s0 + spp; ++s) {
+    job_t j;
+    memset(&j, 0, sizeof(j));
+    j.mode = 1;
+    j.lo = y0;
+    j.hi = y1;
+    j.chunk = 1;
+    j.s = s;
+    j.seed = seed;
+    j.film = film;
+    run_job(&j, nthreads);
+  }
+}
+
+int xyzo_max_threads(void) { return default_threads(0); }

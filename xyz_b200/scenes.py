@@ -1,0 +1,331 @@
+"""Seeded synthetic scenes for the path tracer.
+
+The reference renderer loads Metasequoia (.mqo) scenes that are not part of its
+tree, so every workload here is generated from a seed.  Triangle ids are the
+generator's order (the reference's loader would Morton-sort them,
+xyz/core/scene_mqo.cpp:676-692).
+
+Conventions shared with the reference (xyz/geom/triangle.cpp:10-33):
+  * a triangle (v0, v1, v2) has geometric normal normalize(cross(v2-v0, v1-v0));
+    its *front* side is the side that normal points to, and an emitter radiates
+    only from its front side (xyz/core/scene_pathtracing.cpp:84);
+  * lights share one power Phi (XYZ), spread as radiance Phi / (pi * A_lights)
+    (xyz/core/scene_pathtracing.cpp:87-109).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from .spectrum import ccir601_rgb_to_xyz, flat_spd_xyz
+
+
+@dataclass
+class Camera:
+    """Reference camera model (xyz/core/thinlenscamera.cpp:20-28, 71-90).
+
+    `pinhole` selects the CONFIG_PINHOLE_CAMERA_MODEL ray generation
+    (thinlenscamera.cpp:111-124); otherwise the thin lens of :188-205."""
+
+    eye: tuple = (0.0, 1.0, 4.0)
+    at: tuple = (0.0, 1.0, 0.0)
+    film_size: float = 0.025
+    focal_length: float = 0.035
+    f_number: float = 1.4
+    pinhole: bool = False
+
+    @staticmethod
+    def with_fov(eye, at, fov_y_deg: float, pinhole: bool = True,
+                 focal_length: float = 0.035, f_number: float = 1.4) -> "Camera":
+        """Film size that gives vertical field of view `fov_y_deg` with the
+        reference's lens-film distance V = L f / (L - f)."""
+        L = math.dist(eye, at)
+        V = L * focal_length / (L - focal_length)
+        film = 2.0 * V * math.tan(math.radians(fov_y_deg) / 2.0)
+        return Camera(tuple(map(float, eye)), tuple(map(float, at)), float(film),
+                      float(focal_length), float(f_number), pinhole)
+
+
+@dataclass
+class SceneData:
+    positions: np.ndarray              # (nv, 3) float32
+    tris: np.ndarray                   # (nt, 3) int32
+    tri_mat: np.ndarray                # (nt,) int32
+    albedo_xyz: np.ndarray             # (nm, 3) float32
+    is_light: np.ndarray               # (nm,) int32
+    light_power_xyz: np.ndarray        # (3,) float32, Phi shared by all lights
+    normals: Optional[np.ndarray] = None  # (nv, 3) float32 shading normals
+    camera: Camera = field(default_factory=Camera)
+    name: str = ""
+
+    @property
+    def n_tris(self) -> int:
+        return int(self.tris.shape[0])
+
+    def light_area(self) -> float:
+        """Total emitter area in float32, accumulated in triangle order."""
+        lit = self.is_light[self.tri_mat] != 0
+        acc = np.float32(0.0)
+        for a in triangle_areas(self.positions, self.tris[lit]):
+            acc = np.float32(acc + a)
+        return float(acc)
+
+
+def triangle_areas(pos: np.ndarray, tris: np.ndarray) -> np.ndarray:
+    """|cross(e2, e1)| * 0.5 in float32 (xyz/geom/triangle.hpp:57-59)."""
+    p = pos.astype(np.float32)
+    v0 = p[tris[:, 0]]
+    e1 = (p[tris[:, 1]] - v0).astype(np.float32)
+    e2 = (p[tris[:, 2]] - v0).astype(np.float32)
+    c = np.cross(e2, e1).astype(np.float32)
+    return (np.sqrt((c * c).sum(axis=1, dtype=np.float32)) * np.float32(0.5)).astype(np.float32)
+
+
+def flat_emitter_power(radiance: float, light_area: float) -> np.ndarray:
+    """Phi (XYZ) for a spectrally flat emitter of `radiance` W/m^2/sr per bin:
+    the reference spreads Phi as Phi / (pi * A), so Phi = pi * A * L_xyz."""
+    return (flat_spd_xyz(radiance) * np.float32(math.pi * light_area)).astype(np.float32)
+
+
+# --------------------------------------------------------------------------
+# geometry helpers
+# --------------------------------------------------------------------------
+
+class _Builder:
+    def __init__(self):
+        self.pos: list = []
+        self.tris: list = []
+        self.mat: list = []
+
+    def add_tri(self, a, b, c, m, front=None):
+        """Adds (a, b, c); if `front` is given, orders the vertices so that the
+        reference's geometric normal cross(v2-v0, v1-v0) points along it."""
+        a, b, c = (np.asarray(v, dtype=np.float64) for v in (a, b, c))
+        if front is not None:
+            n = np.cross(c - a, b - a)
+            if np.dot(n, np.asarray(front, dtype=np.float64)) < 0:
+                b, c = c, b
+        base = len(self.pos)
+        self.pos.extend([a, b, c])
+        self.tris.append((base, base + 1, base + 2))
+        self.mat.append(m)
+
+    def add_quad(self, p0, p1, p2, p3, m, front):
+        self.add_tri(p0, p1, p2, m, front)
+        self.add_tri(p0, p2, p3, m, front)
+
+    def add_box(self, lo, hi, m):
+        """Axis-aligned box, faces pointing outwards (12 triangles)."""
+        x0, y0, z0 = lo
+        x1, y1, z1 = hi
+        c = [(x0, y0, z0), (x1, y0, z0), (x1, y1, z0), (x0, y1, z0),
+             (x0, y0, z1), (x1, y0, z1), (x1, y1, z1), (x0, y1, z1)]
+        faces = [((0, 1, 2, 3), (0, 0, -1)), ((4, 5, 6, 7), (0, 0, 1)),
+                 ((0, 1, 5, 4), (0, -1, 0)), ((3, 2, 6, 7), (0, 1, 0)),
+                 ((0, 3, 7, 4), (-1, 0, 0)), ((1, 2, 6, 5), (1, 0, 0))]
+        for (i, j, k, l), n in faces:
+            self.add_quad(c[i], c[j], c[k], c[l], m, n)
+
+    def arrays(self):
+        return (np.asarray(self.pos, dtype=np.float32).reshape(-1, 3),
+                np.asarray(self.tris, dtype=np.int32).reshape(-1, 3),
+                np.asarray(self.mat, dtype=np.int32))
+
+
+def cornell_box(res_fov: float = 40.0, pinhole: bool = True,
+                radiance: float = 15.0) -> SceneData:
+    """Cornell-style closed room: 2x2x2 m (x in [-1,1], y in [0,2], z in [-1,1]),
+    10 wall triangles (floor, ceiling, back, red left, green right; the front is
+    open towards the camera), two axis-aligned boxes (24 triangles) and a
+    0.5 x 0.5 m ceiling light 1 mm below the ceiling facing down (2 triangles).
+    Albedos (linear RGB -> XYZ): white 0.8, red (0.63, 0.06, 0.05),
+    green (0.14, 0.45, 0.09).  Spectrally flat emission of `radiance`
+    W/m^2/sr.  Pinhole camera, vertical fov `res_fov` degrees."""
+    WHITE, RED, GREEN, LIGHT = 0, 1, 2, 3
+    b = _Builder()
+    b.add_quad((-1, 0, -1), (1, 0, -1), (1, 0, 1), (-1, 0, 1), WHITE, (0, 1, 0))     # floor
+    b.add_quad((-1, 2, -1), (1, 2, -1), (1, 2, 1), (-1, 2, 1), WHITE, (0, -1, 0))    # ceiling
+    b.add_quad((-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1), WHITE, (0, 0, 1))   # back
+    b.add_quad((-1, 0, -1), (-1, 2, -1), (-1, 2, 1), (-1, 0, 1), RED, (1, 0, 0))     # left
+    b.add_quad((1, 0, -1), (1, 2, -1), (1, 2, 1), (1, 0, 1), GREEN, (-1, 0, 0))      # right
+    b.add_box((-0.70, 0.0, -0.70), (-0.10, 1.2, -0.10), WHITE)                     # tall box
+    b.add_box((0.10, 0.0, -0.20), (0.70, 0.6, 0.40), WHITE)                        # short box
+    y = 2.0 - 0.001
+    b.add_quad((-0.25, y, -0.25), (0.25, y, -0.25), (0.25, y, 0.25), (-0.25, y, 0.25),
+               LIGHT, (0, -1, 0))
+    pos, tris, mat = b.arrays()
+    albedo = np.stack([ccir601_rgb_to_xyz((0.8, 0.8, 0.8)),
+                       ccir601_rgb_to_xyz((0.63, 0.06, 0.05)),
+                       ccir601_rgb_to_xyz((0.14, 0.45, 0.09)),
+                       np.zeros(3, np.float32)]).astype(np.float32)
+    is_light = np.array([0, 0, 0, 1], dtype=np.int32)
+    sd = SceneData(pos, tris, mat, albedo, is_light, np.zeros(3, np.float32),
+                   camera=Camera.with_fov((0.0, 1.0, 3.75), (0.0, 1.0, 0.0), res_fov,
+                                          pinhole=pinhole),
+                   name="cornell")
+    sd.light_power_xyz = flat_emitter_power(radiance, sd.light_area())
+    return sd
+
+
+# --------------------------------------------------------------------------
+# icospheres and value noise
+# --------------------------------------------------------------------------
+
+def icosphere(level: int):
+    """Unit icosphere subdivided `level` times: 20 * 4**level faces.  Face
+    winding makes cross(v2-v0, v1-v0) point outwards (front side outside)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array([(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0),
+                  (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+                  (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)], dtype=np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11),
+                  (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8),
+                  (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9),
+                  (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)], dtype=np.int64)
+    for _ in range(level):
+        nv = v.shape[0]
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        e.sort(axis=1)
+        key = e[:, 0] * (nv + 1) + e[:, 1]
+        uniq, inv = np.unique(key, return_inverse=True)
+        a, bb = uniq // (nv + 1), uniq % (nv + 1)
+        mid = v[a] + v[bb]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        v = np.concatenate([v, mid])
+        m = inv.reshape(3, -1).T + nv          # midpoints of edges 01, 12, 20
+        f0, f1, f2 = f[:, 0], f[:, 1], f[:, 2]
+        m01, m12, m20 = m[:, 0], m[:, 1], m[:, 2]
+        f = np.concatenate([np.stack([f0, m01, m20], 1), np.stack([f1, m12, m01], 1),
+                            np.stack([f2, m20, m12], 1), np.stack([m01, m12, m20], 1)])
+    # The 20 seed faces are counter-clockwise seen from outside; the reference's
+    # front normal is cross(v2-v0, v1-v0), so flip the winding.
+    f = f[:, [0, 2, 1]]
+    return v, f
+
+
+def _hash3(ix, iy, iz, seed):
+    h = (ix.astype(np.uint32) * np.uint32(0x8DA6B343)) ^ \
+        (iy.astype(np.uint32) * np.uint32(0xD8163841)) ^ \
+        (iz.astype(np.uint32) * np.uint32(0xCB1AB31F)) ^ np.uint32(seed * 0x9E3779B1 & 0xFFFFFFFF)
+    h ^= h >> np.uint32(16)
+    h *= np.uint32(0x7FEB352D)
+    h ^= h >> np.uint32(15)
+    h *= np.uint32(0x846CA68B)
+    h ^= h >> np.uint32(16)
+    return h.astype(np.float64) / 4294967295.0 * 2.0 - 1.0
+
+
+def value_noise(p: np.ndarray, seed: int, octaves: int = 4, base_freq: float = 2.0) -> np.ndarray:
+    """Seeded lattice value noise in [-1, 1]: per-octave trilinear
+    interpolation of hashed lattice values with smoothstep weights; octave o
+    has frequency base_freq * 2**o and weight 0.5**o (weights normalised)."""
+    total = np.zeros(p.shape[0])
+    norm = 0.0
+    with np.errstate(over="ignore"):
+        for o in range(octaves):
+            q = p * (base_freq * 2 ** o)
+            i0 = np.floor(q).astype(np.int64)
+            fr = q - i0
+            w = fr * fr * (3.0 - 2.0 * fr)
+            acc = np.zeros(p.shape[0])
+            for dx in (0, 1):
+                for dy in (0, 1):
+                    for dz in (0, 1):
+                        h = _hash3(i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz, seed * 7 + o)
+                        wx = w[:, 0] if dx else 1 - w[:, 0]
+                        wy = w[:, 1] if dy else 1 - w[:, 1]
+                        wz = w[:, 2] if dz else 1 - w[:, 2]
+                        acc += h * wx * wy * wz
+            total += acc * 0.5 ** o
+            norm += 0.5 ** o
+    return total / norm
+
+
+def vertex_normals(pos: np.ndarray, tris: np.ndarray) -> np.ndarray:
+    """Area-weighted vertex normals along the reference's front normal
+    cross(v2-v0, v1-v0), normalised."""
+    p = pos.astype(np.float64)
+    n = np.cross(p[tris[:, 2]] - p[tris[:, 0]], p[tris[:, 1]] - p[tris[:, 0]])
+    acc = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(acc, tris[:, k], n)
+    acc /= np.maximum(np.linalg.norm(acc, axis=1, keepdims=True), 1e-30)
+    return acc.astype(np.float32)
+
+
+def displaced_icosphere(level: int, seed: int, amplitude: float = 0.15):
+    """Unit icosphere radially displaced by 4-octave value noise:
+    r = 1 + amplitude * noise(direction)."""
+    v, f = icosphere(level)
+    r = 1.0 + amplitude * value_noise(v, seed)
+    return v * r[:, None], f
+
+
+def spheres_scene(level: int = 7, n_spheres: int = 3, seed: int = 0,
+                  radiance: float = 15.0, smooth: bool = True,
+                  fov: float = 40.0, light_level: int = 3) -> SceneData:
+    """Large-mesh workload: `n_spheres` displaced level-`level` icospheres
+    (radius 0.6, noise amplitude 0.15) over a 40 x 40 m ground plane, lit by one
+    tessellated spherical area light of radius 0.3.  Every triangle has its own
+    grey Lambert albedo drawn uniformly from [0.2, 0.9] (seeded).  At level 7 and
+    three spheres this is 983,040 + 2 + 1,280 = 984,322 triangles."""
+    rng = np.random.default_rng(seed)
+    pos_l, tri_l, norm_l = [], [], []
+    base = 0
+    xs = np.linspace(-1.4, 1.4, n_spheres) if n_spheres > 1 else np.zeros(1)
+    for s, x in enumerate(xs):
+        v, f = displaced_icosphere(level, seed * 101 + s, 0.15)
+        v = v * 0.6 + np.array([x, 0.72, 0.0])
+        pos_l.append(v)
+        tri_l.append(f + base)
+        norm_l.append(vertex_normals(v, f) if smooth else None)
+        base += v.shape[0]
+    # ground (front side up)
+    g = np.array([(-20, 0, -20), (20, 0, -20), (20, 0, 20), (-20, 0, 20)], dtype=np.float64)
+    gt = np.array([(0, 2, 1), (0, 3, 2)], dtype=np.int64)
+    pos_l.append(g)
+    tri_l.append(gt + base)
+    norm_l.append(np.tile(np.array([[0, 1, 0]], np.float32), (4, 1)))
+    base += 4
+    # spherical light, front side outwards
+    lv, lf = icosphere(light_level)
+    lv = lv * 0.3 + np.array([0.0, 2.6, 1.2])
+    pos_l.append(lv)
+    tri_l.append(lf + base)
+    norm_l.append(vertex_normals(lv, lf))
+    pos = np.concatenate(pos_l).astype(np.float32)
+    tris = np.concatenate(tri_l).astype(np.int32)
+    n_geom = tris.shape[0] - lf.shape[0]
+    grey = rng.uniform(0.2, 0.9, size=n_geom)
+    white = ccir601_rgb_to_xyz((1.0, 1.0, 1.0))
+    albedo = np.concatenate([(grey[:, None] * white[None, :]).astype(np.float32),
+                             np.zeros((1, 3), np.float32)])
+    is_light = np.zeros(n_geom + 1, dtype=np.int32)
+    is_light[-1] = 1
+    tri_mat = np.concatenate([np.arange(n_geom, dtype=np.int32),
+                              np.full(lf.shape[0], n_geom, dtype=np.int32)])
+    normals = np.concatenate(norm_l).astype(np.float32) if smooth else None
+    sd = SceneData(pos, tris, tri_mat, albedo, is_light, np.zeros(3, np.float32),
+                   normals=normals,
+                   camera=Camera.with_fov((0.0, 1.6, 4.8), (0.0, 0.6, 0.0), fov, pinhole=True),
+                   name=f"spheres-l{level}x{n_spheres}")
+    sd.light_power_xyz = flat_emitter_power(radiance, sd.light_area())
+    return sd
+
+
+def random_rays(scene: SceneData, n: int, seed: int = 0):
+    """Seeded test rays: origins uniform in the scene box grown by 20 %,
+    directions uniform on the sphere.  Returns (org, dir) float32 (n, 3)."""
+    rng = np.random.default_rng(seed)
+    lo = scene.positions.min(axis=0)
+    hi = scene.positions.max(axis=0)
+    c, h = (lo + hi) / 2, (hi - lo) / 2 * 1.2
+    org = (c + h * rng.uniform(-1, 1, size=(n, 3))).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return org, d.astype(np.float32)
