@@ -1,0 +1,393 @@
+#!/usr/bin/env python3
+"""Path-tracing throughput benchmark (Msamples/s) on the large-mesh workload.
+
+Workload (one "step"): render 1024 x 1024 pixels x 64 samples of the seeded
+spheres scene - three displaced level-7 icospheres (983,040 triangles), a
+ground plane and a tessellated spherical area light of radius 0.3, 984,322
+triangles in all, per-triangle Lambert albedo in [0.2, 0.9] - through a pinhole
+camera (40 degree fov), max path depth 10, SAH kd-tree (traversal cost 1,
+intersection cost 1.5, leaves of <= 4 triangles).  One sample is one camera
+path.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl xyz|reference]
+
+Prints one JSON line on rank 0.  `value` is device-timed with the scene resident
+in HBM; `e2e` is the same metric through the C ABI with host buffers (scene
+arrays uploaded, tree built and film read back every step).  Multi-GPU: one
+process per GPU under torchrun; every rank renders its own 64 samples per pixel
+(sample offset rank * 64) and the films are summed on rank 0 with one NCCL
+reduce per step (weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+W_PIX, H_PIX, SPP, MAX_DEPTH, SEED = 1024, 1024, 64, 10, 0
+METRIC = "Msamples/s on 1 B200 (path samples per second, 1M-triangle scene)"
+UNIT = "Msamples/s"
+L2_FLUSH_BYTES = 256 << 20
+TRI_BYTES_ALGO = 36   # v0, e1, e2 as the reference stores a triangle
+NODE_BYTES = 8
+REF_BYTES = 4
+RAY_IO_BYTES = 32 + 16
+
+
+def workload_config(stats=None):
+    cfg = {
+        "workload": "spheres-1M: 3 displaced level-7 icospheres + ground + spherical light r=0.3, "
+                    "984,322 triangles, 1024x1024, 64 spp, max depth 10, pinhole fov 40, "
+                    "SAH kd-tree (Ct=1, Ci=1.5, leaf<=4), Lambert + NEE/MIS + Russian roulette, XYZ film",
+        "triangles": 984322, "width": W_PIX, "height": H_PIX, "spp": SPP, "max_depth": MAX_DEPTH,
+        "seed": SEED, "l2_flush": "256 MiB buffer written between timed steps",
+    }
+    if stats:
+        cfg["kd_tree"] = {"nodes": stats["n_nodes"], "leaf_refs": stats["n_leaf_refs"],
+                          "depth": stats["max_depth"], "build_ms": round(stats["build_ms"], 1)}
+    return cfg
+
+
+def make_scene():
+    from xyz_b200 import scenes
+    return scenes.spheres_scene(level=7, n_spheres=3, seed=SEED)
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(device_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+# ----------------------------------------------------------------- CPU arms
+def reference_lib():
+    """The reference's own renderer built from its sources (oracle/_ref), else
+    the C restatement (oracle/_port)."""
+    from oracle import refbind
+    if refbind.ref_available(pinhole=True):
+        return refbind.RefLib(pinhole=True), "reference"
+    if not refbind.port_available():
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "port"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return refbind.PortLib(), "port"
+
+
+def cpu_setup(sd):
+    lib, kind = reference_lib()
+    threads = lib.max_threads()
+    t0 = time.perf_counter()
+    lib.scene_create(sd)
+    build_s = time.perf_counter() - t0
+    lib.set_camera(sd.camera, W_PIX, H_PIX)
+    lib.set_path_params(max_depth=MAX_DEPTH)
+    return lib, kind, threads, build_s
+
+
+def cpu_rows_for(lib, threads, target_s):
+    """Row band (1 spp) that takes about target_s seconds on `threads` threads."""
+    y0 = H_PIX // 2 - 8
+    t0 = time.perf_counter()
+    lib.render(1, seed=SEED + 7, y0=y0, y1=y0 + 16, nthreads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    rows = int(16 * target_s / dt)
+    return max(16, min(H_PIX, rows))
+
+
+def cpu_sample(lib, threads, rows, s):
+    y0 = max(0, H_PIX // 2 - rows // 2)
+    t0 = time.perf_counter()
+    lib.render(1, seed=SEED, s0=s, y0=y0, y1=y0 + rows, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return rows * W_PIX / dt / 1e6, dt
+
+
+def cpu_baseline(sd, target_s=12.0):
+    lib, kind, threads, build_s = cpu_setup(sd)
+    rows = cpu_rows_for(lib, threads, target_s)
+    v, dt = cpu_sample(lib, threads, rows, 0)
+    return {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"1 spp over {rows} of 1024 rows (centre band) of the same scene and camera, "
+                      f"{rows * W_PIX} paths in {dt:.1f} s; tree build {build_s:.1f} s untimed"}
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    sd = make_scene()
+    lib, kind, threads, build_s = cpu_setup(sd)
+    per_step_s = max(2.0, min(15.0, 100.0 / max(1, args.steps + args.warmup)))
+    rows = cpu_rows_for(lib, threads, per_step_s)
+    for w in range(args.warmup):
+        cpu_sample(lib, threads, max(16, rows // 4), 1000 + w)
+    vals, times = [], []
+    for k in range(args.steps):
+        v, dt = cpu_sample(lib, threads, rows, k)
+        vals.append(v)
+        times.append(dt)
+    total = sum(times)
+    value = rows * W_PIX * args.steps / total / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * total / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene generator)", "config": workload_config(),
+        "impl": "reference",
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"each step: 1 spp over {rows} of 1024 rows (centre band), "
+                                   f"{rows * W_PIX} paths; tree build {build_s:.1f} s untimed"},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- GPU arm
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per traced ray of the trace kernel from the committed ncu
+    summary (profiles/trace_queue_spheres1m.txt), if present."""
+    p = os.path.join(ROOT, "profiles", "trace_queue_spheres1m.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_ray:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_gpu_arm(args, rank, world):
+    import torch
+    from xyz_b200 import api
+
+    dev = torch.cuda.current_device()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    sd = make_scene()
+    scene = api.Scene(sd)
+    stats = scene.stats()
+    cam = sd.camera
+    film = torch.zeros((H_PIX, W_PIX, 3), dtype=torch.float32, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    offset = rank * SPP
+
+    def step(s_off, profile=0):
+        scene.render(cam, W_PIX, H_PIX, SPP, seed=SEED, spp_offset=s_off, max_depth=MAX_DEPTH,
+                     film=film, profile=profile)
+        if dist is not None:
+            dist.reduce(film, dst=0)
+        flush.zero_()
+
+    for _ in range(args.warmup):
+        step(offset)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+
+    clocks = ClockSampler(dev)
+    ms_cls = {k: 0.0 for k in api.KERNEL_CLASSES}
+    n_cls = {k: 0 for k in api.KERNEL_CLASSES}
+    launches = 0
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for k in range(args.steps):
+        step(offset, profile=1)
+        prof = scene.render_profile()
+        for c in api.KERNEL_CLASSES:
+            ms_cls[c] += prof["ms"][c]
+            n_cls[c] += prof["launches"][c]
+        launches += scene.render_counters()["kernel_launches"]
+    ev1.record()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    wall_ms = 1000 * (time.perf_counter() - t_wall)
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    samples_per_step = W_PIX * H_PIX * SPP
+    value = samples_per_step * world * args.steps / (ms / 1000.0) / 1e6
+
+    # work per ray from one counted render (outside the timed region)
+    step(offset, profile=2)
+    cp = scene.render_profile()
+    counters = scene.render_counters()
+    ext_bytes = (cp["ext_rays"] * RAY_IO_BYTES + cp["ext_nodes"] * NODE_BYTES +
+                 cp["ext_tri_tests"] * (REF_BYTES + TRI_BYTES_ALGO))
+    sh_bytes = (cp["shadow_rays"] * RAY_IO_BYTES + cp["shadow_nodes"] * NODE_BYTES +
+                cp["shadow_tri_tests"] * (REF_BYTES + TRI_BYTES_ALGO))
+    trace_ms = (ms_cls["trace_extension"] + ms_cls["trace_shadow"]) / max(1, args.steps)
+    trace_launches = (n_cls["trace_extension"] + n_cls["trace_shadow"]) / max(1, args.steps)
+    peak, peak_kind = measured_peaks()
+    achieved = (ext_bytes + sh_bytes) / (trace_ms / 1000.0) / 1e9 if trace_ms > 0 else 0.0
+    rays = cp["ext_rays"] + cp["shadow_rays"]
+    per_ray_traffic = profiled_traffic()
+    traffic = None
+    if per_ray_traffic is not None and trace_launches:
+        traffic = per_ray_traffic * rays / trace_launches
+    roofline = {
+        "bound": "hbm", "kernel": "k_trace_queue (extension + shadow closest hit)",
+        "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+        "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+        "traffic": traffic,
+        "algorithmic_bytes_per_ray": round((ext_bytes + sh_bytes) / max(1, rays), 1),
+        "per_ray": {"nodes": round((cp["ext_nodes"] + cp["shadow_nodes"]) / max(1, rays), 2),
+                    "tri_tests": round((cp["ext_tri_tests"] + cp["shadow_tri_tests"]) / max(1, rays), 2)},
+        "rays_per_step": rays,
+        "trace_ms_per_step": round(trace_ms, 3),
+        "kernel_ms_per_step": {c: round(ms_cls[c] / max(1, args.steps), 3) for c in api.KERNEL_CLASSES},
+        "kernel_share": {c: round(ms_cls[c] / max(1e-9, sum(ms_cls.values())), 4) for c in api.KERNEL_CLASSES},
+        "grays_per_s": round(rays / (trace_ms / 1000.0) / 1e9, 3) if trace_ms > 0 else None,
+    }
+
+    # end to end through the C ABI with host buffers: upload + build + render + read back
+    e2e = None
+    if rank == 0 or world > 1:
+        h2d = sum(int(a.nbytes) for a in (sd.positions, sd.tris, sd.tri_mat, sd.albedo_xyz, sd.is_light))
+        if sd.normals is not None:
+            h2d += int(sd.normals.nbytes)
+        host_film = np.zeros((H_PIX, W_PIX, 3), np.float32)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            with api.Scene(sd) as s2:
+                s2.render(cam, W_PIX, H_PIX, SPP, seed=SEED, spp_offset=offset, max_depth=MAX_DEPTH,
+                          film=host_film)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": round(samples_per_step * world * args.steps / e2e_s / 1e6, 3), "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(host_film.nbytes),
+               "includes": "scene upload + kd-tree build + render + film read-back, every step"}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(sd)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene generator)",
+            "config": workload_config(stats) | {"parallelism": f"sample-parallel x{world}",
+                                                 "wave_paths": 1 << 22},
+            "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk, "wall_ms_timed_region": round(wall_ms, 1),
+            "render_counters": counters,
+        }
+        print(json.dumps(line), flush=True)
+    scene.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["xyz", "reference"], default="xyz")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    try:
+        run_gpu_arm(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,208 @@
+/* xyzgpu: B200 (sm_100a) path-tracing hot path of the xyz renderer behind a C ABI.
+ *
+ * The reference renderer (goofoo/xyz) exposes its hot path as the C++ singleton
+ * `xyz::Scene` driven by an integrator thread:
+ *   Scene::Load / Scene::Build                    xyz/core/scene.hpp:51-52
+ *   Scene::FindIntersection (closest hit)         xyz/core/scene.hpp:236-238, 277-295
+ *   Scene::EvalutePathTracing (one path sample)   xyz/core/scene.hpp:56-58
+ *   PathTracer::run (spp x pixel loop, film +=)   xyz/integrator/integrator.cpp:88-162
+ * This header is the batch form of those calls.  Every function returns 0 or a
+ * negative XYZGPU_E_* code; no exception crosses the ABI; the message of the
+ * last failure on the calling thread is xyzgpu_last_error().  The reference has
+ * no status codes (it prints to stderr and returns early,
+ * xyz/core/scene.cpp:47-51); invalid input here is an error instead.
+ *
+ * Conventions (same as the reference unless stated):
+ *  - Triangles are double-faced; the front normal of (v0, v1, v2) is
+ *    normalize(cross(v2 - v0, v1 - v0))  (xyz/geom/triangle.cpp:10-20).
+ *  - Materials are Lambert (XYZ albedo) or light.  Lights radiate from their
+ *    front side only and share one power Phi (XYZ) spread over the total light
+ *    area as radiance Phi / (pi * A)  (xyz/core/scene_pathtracing.cpp:81-112).
+ *  - Film: W*H*3 floats, CIE XYZ, row y = 0 at the bottom (film[y*W+x]),
+ *    holding the SUM over samples (the reference divides by spp when saving,
+ *    xyz/core/imagefilm.cpp:90-105).
+ *  - Random numbers: Philox4x32-10 (Salmon et al., SC'11) keyed by the seed;
+ *    dimension `dim` of sample `s` of pixel `p` is
+ *      u = (Philox(ctr = {p, s, dim / 4, 0}, key = {seed, seed >> 32})[dim % 4] >> 8) * 2^-24.
+ *    Dimensions are consumed in the order the reference's estimator reads
+ *    IPrimarySample::next() (xyz/bsdf/bsdf.hpp:10-14): 0-1 pixel jitter,
+ *    2-3 light sample, (thin lens) 4-5 lens sample, then per vertex an optional
+ *    Russian-roulette draw and two BSDF draws.
+ */
+#ifndef XYZGPU_H_
+#define XYZGPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XYZGPU_ABI_VERSION 1
+
+#define XYZGPU_OK 0
+#define XYZGPU_E_INVALID -1   /* bad argument or scene description */
+#define XYZGPU_E_CUDA -2      /* CUDA runtime error (message has the CUDA text) */
+#define XYZGPU_E_NOMEM -3     /* device or host allocation failed */
+#define XYZGPU_E_LIMIT -4     /* size beyond a documented limit */
+#define XYZGPU_E_NODEVICE -5  /* no usable sm_100 device */
+
+typedef struct xyzgpu_scene_s *xyzgpu_scene;
+
+/* Scene description, host memory, copied by xyzgpu_scene_create.
+ * Replaces Scene::Load (xyz/core/scene_mqo.cpp:547-777), which fills the same
+ * triangle / material / light lists from an MQO file. */
+typedef struct {
+  const float *positions;       /* 3 * n_vertices */
+  const float *normals;         /* 3 * n_vertices shading normals, or NULL (flat) */
+  int n_vertices;
+  const int32_t *triangles;     /* 3 * n_triangles vertex indices */
+  const int32_t *tri_material;  /* n_triangles material ids */
+  int n_triangles;
+  const float *albedo_xyz;      /* 3 * n_materials (ignored for lights) */
+  const int32_t *is_light;      /* n_materials flags */
+  int n_materials;
+  float light_power_xyz[3];     /* Phi shared by all light triangles */
+} xyzgpu_scene_desc;
+
+/* kd-tree construction parameters (the reference: KDTree(max_bucket = 16,
+ * max_depth = 16), SAH without traversal / intersection constants,
+ * xyz/geom/kdtree.hpp:19-20, kdtree.cpp:261-272). */
+typedef struct {
+  int leaf_max_tris;      /* make a leaf at or below this many triangles (4) */
+  int max_depth;          /* depth limit; 0 = 8 + 1.3 * log2(n_triangles) */
+  float cost_traversal;   /* SAH traversal cost (1.0) */
+  float cost_intersect;   /* SAH intersection cost (1.5) */
+  float empty_bonus;      /* SAH discount for a split with an empty side (0.2) */
+  int bins;               /* SAH bins per axis per node (32, max 64) */
+  int builder;            /* XYZGPU_BUILD_HOST (default) or XYZGPU_BUILD_DEVICE */
+  int max_refs_factor;    /* reference budget = factor * n_triangles (6) */
+} xyzgpu_build_params;
+
+#define XYZGPU_BUILD_DEVICE 0
+#define XYZGPU_BUILD_HOST 1
+
+void xyzgpu_build_params_default(xyzgpu_build_params *bp);
+
+/* Uploads the scene and builds its kd-tree (Scene::Load + Scene::Build,
+ * xyz/core/scene.cpp:35).  The device is the current CUDA device. */
+int xyzgpu_scene_create(const xyzgpu_scene_desc *desc, const xyzgpu_build_params *bp,
+                        xyzgpu_scene *out);
+
+/* Frees the scene's device memory. */
+void xyzgpu_scene_destroy(xyzgpu_scene scene);
+
+typedef struct {
+  int64_t n_triangles, n_lights, n_nodes, n_leaves, n_empty_leaves, n_leaf_refs;
+  int64_t max_depth, device_bytes;
+  double build_ms;        /* wall time of the last kd-tree build */
+  float light_area;
+  float bounds_min[3], bounds_max[3];
+} xyzgpu_scene_stats;
+
+int xyzgpu_scene_stats_get(xyzgpu_scene scene, xyzgpu_scene_stats *out);
+
+/* Copies the flattened kd-tree to host memory (for inspection and tests).
+ * nodes: 2 * n_nodes uint32 (see the node layout in csrc/kdtree.h); refs:
+ * n_leaf_refs int32.  Either pointer may be NULL. */
+int xyzgpu_scene_copy_tree(xyzgpu_scene scene, uint32_t *nodes, int32_t *refs);
+
+/* Closest hit for a batch of rays: the batch form of Scene::FindIntersection
+ * (xyz/core/scene.hpp:277-295 -> KDTree::FindIntersection, kdtree.cpp:366-372;
+ * triangle test FindIntersectionDF, triangle.cpp:127-165).
+ *   rays: device, n * 8 floats per ray: ox oy oz tmin dx dy dz tmax
+ *         (the reference's interval is tmin = 1e-5, tmax = +inf,
+ *          xyz/geom/intersection.hpp:11-14)
+ *   hits: device, n * 4 words: t, f, g (floats) and an int32
+ *         (triangle_id << 1 | back_side), or -1 for a miss.
+ *   stream: cudaStream_t or NULL. */
+int xyzgpu_trace_closest(xyzgpu_scene scene, const float *rays, int n, float *hits,
+                         void *stream);
+
+/* Counters of the instrumented traversal (per batch, summed over rays). */
+typedef struct {
+  uint64_t rays, nodes_visited, leaves_visited, tri_tests, hits;
+} xyzgpu_trace_counters;
+
+/* Same as xyzgpu_trace_closest plus work counters (slower; for roofline
+ * accounting outside timed regions).  Synchronises `stream`. */
+int xyzgpu_trace_closest_counted(xyzgpu_scene scene, const float *rays, int n, float *hits,
+                                 void *stream, xyzgpu_trace_counters *counters);
+
+/* Camera as the reference models it (xyz/core/thinlenscamera.cpp:20-28, 71-90):
+ * eye, gaze point, film size, focal length, F-number; up = +y.  pinhole != 0
+ * selects the CONFIG_PINHOLE_CAMERA_MODEL ray generation (thinlenscamera.cpp:
+ * 111-124), otherwise the thin lens (:159-205). */
+typedef struct {
+  float eye[3];
+  float at[3];
+  float film_size;
+  float focal_length;
+  float f_number;
+  int pinhole;
+} xyzgpu_camera;
+
+#define XYZGPU_FILM_DEVICE 0
+#define XYZGPU_FILM_HOST 1
+
+typedef struct {
+  int width, height;
+  int spp;                 /* samples per pixel rendered by this call */
+  int spp_offset;          /* index of the first sample (progressive rendering) */
+  int max_depth;           /* max path segments; the reference's kMax - 1 (15) */
+  int rr_start_depth;      /* first vertex that plays Russian roulette (1) */
+  float rr_threshold;      /* Russian roulette on throughput Y below this (0.2) */
+  uint64_t seed;
+  int film_location;       /* XYZGPU_FILM_DEVICE or XYZGPU_FILM_HOST */
+  int accumulate;          /* nonzero: add into film; zero: overwrite */
+  int wave_paths;          /* paths in flight per wave; 0 = default (1 << 22) */
+  int profile;             /* XYZGPU_PROFILE_*: per-kernel timing or work counters */
+} xyzgpu_render_params;
+
+#define XYZGPU_PROFILE_OFF 0
+#define XYZGPU_PROFILE_TIMING 1   /* CUDA events around every kernel launch */
+#define XYZGPU_PROFILE_COUNTERS 2 /* traversal work counters (slower kernels) */
+
+void xyzgpu_render_params_default(xyzgpu_render_params *rp);
+
+/* Renders rp->spp samples per pixel (PathTracer::run's loop around
+ * Scene::EvalutePathTracing, xyz/integrator/integrator.cpp:119-128) into
+ * `film` (W*H*3 XYZ sums).  Wavefront: ray generation, closest hit, shading
+ * (emitter MIS, next-event estimation, Russian roulette, Lambert sampling),
+ * shadow rays and film accumulation are separate kernels over SoA queues.
+ * A host film is copied in and out through pinned staging inside the call. */
+int xyzgpu_render(xyzgpu_scene scene, const xyzgpu_camera *camera,
+                  const xyzgpu_render_params *rp, float *film, void *stream);
+
+typedef struct {
+  uint64_t paths, extension_rays, shadow_rays, shadow_hits_visible, waves, kernel_launches;
+} xyzgpu_render_counters;
+
+/* Counters of the last xyzgpu_render on this scene (synchronises). */
+int xyzgpu_render_counters_get(xyzgpu_scene scene, xyzgpu_render_counters *out);
+
+/* Per-kernel-class profile of the last xyzgpu_render that had profile != 0
+ * (synchronises).  Classes: 0 raygen, 1 extension trace, 2 shade,
+ * 3 shadow trace, 4 film.  ms: summed CUDA-event time (TIMING); the traversal
+ * counters are filled by a COUNTERS render. */
+#define XYZGPU_KERNEL_CLASSES 5
+typedef struct {
+  uint64_t launches[XYZGPU_KERNEL_CLASSES];
+  double ms[XYZGPU_KERNEL_CLASSES];
+  uint64_t ext_rays, ext_nodes, ext_leaves, ext_tri_tests;
+  uint64_t shadow_rays, shadow_nodes, shadow_leaves, shadow_tri_tests, shadow_visible;
+} xyzgpu_render_profile;
+
+int xyzgpu_render_profile_get(xyzgpu_scene scene, xyzgpu_render_profile *out);
+
+/* Host evaluation of the random stream defined above (for tests). */
+float xyzgpu_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim);
+
+const char *xyzgpu_last_error(void);
+int xyzgpu_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XYZGPU_H_ */

@@ -1,0 +1,304 @@
+"""ctypes binding of libxyzgpu.so (the C ABI declared in include/xyzgpu.h).
+
+This module is plumbing for Python callers (tests, benchmarks): every call goes
+through the C ABI to the CUDA kernels.  There is no CPU code path; if the shared
+library is missing or no sm_100 device is present, calls raise.
+Device buffers are torch CUDA tensors (torch provides memory and streams only).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libxyzgpu.so")
+
+XYZGPU_BUILD_DEVICE = 0
+XYZGPU_BUILD_HOST = 1
+XYZGPU_FILM_DEVICE = 0
+XYZGPU_FILM_HOST = 1
+
+ERRORS = {0: "OK", -1: "XYZGPU_E_INVALID", -2: "XYZGPU_E_CUDA", -3: "XYZGPU_E_NOMEM",
+          -4: "XYZGPU_E_LIMIT", -5: "XYZGPU_E_NODEVICE"}
+
+# every symbol declared in include/xyzgpu.h
+EXPORTED = [
+    "xyzgpu_build_params_default", "xyzgpu_scene_create", "xyzgpu_scene_destroy",
+    "xyzgpu_scene_stats_get", "xyzgpu_scene_copy_tree", "xyzgpu_trace_closest",
+    "xyzgpu_trace_closest_counted", "xyzgpu_render_params_default", "xyzgpu_render",
+    "xyzgpu_render_counters_get", "xyzgpu_render_profile_get", "xyzgpu_philox_u01", "xyzgpu_last_error", "xyzgpu_abi_version",
+]
+
+
+class XyzGpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("positions", C.c_void_p), ("normals", C.c_void_p), ("n_vertices", C.c_int),
+                ("triangles", C.c_void_p), ("tri_material", C.c_void_p), ("n_triangles", C.c_int),
+                ("albedo_xyz", C.c_void_p), ("is_light", C.c_void_p), ("n_materials", C.c_int),
+                ("light_power_xyz", C.c_float * 3)]
+
+
+class BuildParams(C.Structure):
+    _fields_ = [("leaf_max_tris", C.c_int), ("max_depth", C.c_int), ("cost_traversal", C.c_float),
+                ("cost_intersect", C.c_float), ("empty_bonus", C.c_float), ("bins", C.c_int),
+                ("builder", C.c_int), ("max_refs_factor", C.c_int)]
+
+
+class SceneStats(C.Structure):
+    _fields_ = [("n_triangles", C.c_int64), ("n_lights", C.c_int64), ("n_nodes", C.c_int64),
+                ("n_leaves", C.c_int64), ("n_empty_leaves", C.c_int64), ("n_leaf_refs", C.c_int64),
+                ("max_depth", C.c_int64), ("device_bytes", C.c_int64), ("build_ms", C.c_double),
+                ("light_area", C.c_float), ("bounds_min", C.c_float * 3), ("bounds_max", C.c_float * 3)]
+
+
+class TraceCounters(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("nodes_visited", C.c_uint64), ("leaves_visited", C.c_uint64),
+                ("tri_tests", C.c_uint64), ("hits", C.c_uint64)]
+
+
+class CameraDesc(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("at", C.c_float * 3), ("film_size", C.c_float),
+                ("focal_length", C.c_float), ("f_number", C.c_float), ("pinhole", C.c_int)]
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("spp", C.c_int), ("spp_offset", C.c_int),
+                ("max_depth", C.c_int), ("rr_start_depth", C.c_int), ("rr_threshold", C.c_float),
+                ("seed", C.c_uint64), ("film_location", C.c_int), ("accumulate", C.c_int),
+                ("wave_paths", C.c_int), ("profile", C.c_int)]
+
+
+class RenderProfile(C.Structure):
+    _fields_ = [("launches", C.c_uint64 * 5), ("ms", C.c_double * 5), ("ext_rays", C.c_uint64),
+                ("ext_nodes", C.c_uint64), ("ext_leaves", C.c_uint64), ("ext_tri_tests", C.c_uint64),
+                ("shadow_rays", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_leaves", C.c_uint64),
+                ("shadow_tri_tests", C.c_uint64), ("shadow_visible", C.c_uint64)]
+
+
+KERNEL_CLASSES = ["raygen", "trace_extension", "shade", "trace_shadow", "film"]
+
+
+class RenderCounters(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("shadow_hits_visible", C.c_uint64), ("waves", C.c_uint64), ("kernel_launches", C.c_uint64)]
+
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Loads libxyzgpu.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C xyz_b200/csrc` "
+                          "(or __graft_entry__.build())")
+    L = C.CDLL(path)
+    L.xyzgpu_last_error.restype = C.c_char_p
+    L.xyzgpu_abi_version.restype = C.c_int
+    L.xyzgpu_scene_create.argtypes = [C.POINTER(SceneDesc), C.POINTER(BuildParams), C.POINTER(C.c_void_p)]
+    L.xyzgpu_scene_destroy.argtypes = [C.c_void_p]
+    L.xyzgpu_scene_stats_get.argtypes = [C.c_void_p, C.POINTER(SceneStats)]
+    L.xyzgpu_scene_copy_tree.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.xyzgpu_trace_closest.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.xyzgpu_trace_closest_counted.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                               C.POINTER(TraceCounters)]
+    L.xyzgpu_render.argtypes = [C.c_void_p, C.POINTER(CameraDesc), C.POINTER(RenderParams), C.c_void_p,
+                                C.c_void_p]
+    L.xyzgpu_render_counters_get.argtypes = [C.c_void_p, C.POINTER(RenderCounters)]
+    L.xyzgpu_render_profile_get.argtypes = [C.c_void_p, C.POINTER(RenderProfile)]
+    L.xyzgpu_philox_u01.restype = C.c_float
+    L.xyzgpu_philox_u01.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+    L.xyzgpu_build_params_default.argtypes = [C.POINTER(BuildParams)]
+    L.xyzgpu_render_params_default.argtypes = [C.POINTER(RenderParams)]
+    _LIB = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise XyzGpuError(rc, _LIB.xyzgpu_last_error().decode(errors="replace"))
+
+
+def default_build_params(**kw) -> BuildParams:
+    bp = BuildParams()
+    load_library().xyzgpu_build_params_default(C.byref(bp))
+    for k, v in kw.items():
+        if k == "builder" and isinstance(v, str):
+            v = {"device": XYZGPU_BUILD_DEVICE, "host": XYZGPU_BUILD_HOST}[v]
+        setattr(bp, k, v)
+    return bp
+
+
+def _stream_ptr(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+class Scene:
+    """A scene on the current CUDA device (xyzgpu_scene_create).
+
+    Mirrors the reference's Scene::Load + Scene::Build; trace() is the batch
+    Scene::FindIntersection and render() the PathTracer::run loop."""
+
+    def __init__(self, sd, **build_kw):
+        L = load_library()
+        self._arrays = []
+
+        def keep(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._arrays.append(a)
+            return a.ctypes.data
+
+        d = SceneDesc()
+        d.positions = keep(sd.positions, np.float32)
+        d.normals = keep(sd.normals, np.float32) if sd.normals is not None else None
+        d.n_vertices = int(sd.positions.shape[0])
+        d.triangles = keep(sd.tris, np.int32)
+        d.tri_material = keep(sd.tri_mat, np.int32)
+        d.n_triangles = int(sd.tris.shape[0])
+        d.albedo_xyz = keep(sd.albedo_xyz, np.float32)
+        d.is_light = keep(sd.is_light, np.int32)
+        d.n_materials = int(sd.albedo_xyz.shape[0])
+        for k in range(3):
+            d.light_power_xyz[k] = float(sd.light_power_xyz[k])
+        bp = default_build_params(**build_kw)
+        h = C.c_void_p()
+        _check(L.xyzgpu_scene_create(C.byref(d), C.byref(bp), C.byref(h)))
+        self.handle = h
+        self._arrays = []
+        self.data = sd
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _LIB.xyzgpu_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def stats(self) -> dict:
+        s = SceneStats()
+        _check(_LIB.xyzgpu_scene_stats_get(self.handle, C.byref(s)))
+        out = {f: getattr(s, f) for f, _ in SceneStats._fields_}
+        out["bounds_min"] = list(s.bounds_min)
+        out["bounds_max"] = list(s.bounds_max)
+        return out
+
+    def tree(self):
+        st = self.stats()
+        nodes = np.zeros(2 * st["n_nodes"], np.uint32)
+        refs = np.zeros(max(1, st["n_leaf_refs"]), np.int32)
+        _check(_LIB.xyzgpu_scene_copy_tree(self.handle, nodes.ctypes.data, refs.ctypes.data))
+        return nodes.reshape(-1, 2), refs[: st["n_leaf_refs"]]
+
+    # -- closest hit -----------------------------------------------------
+    def trace_device(self, rays, hits, stream=None, counted: bool = False):
+        """rays: CUDA float32 tensor (n, 8) = o.xyz, tmin, d.xyz, tmax; hits:
+        CUDA float32 tensor (n, 4).  Returns TraceCounters if counted."""
+        n = int(rays.shape[0])
+        sp = _stream_ptr(stream)
+        if counted:
+            c = TraceCounters()
+            _check(_LIB.xyzgpu_trace_closest_counted(self.handle, rays.data_ptr(), n, hits.data_ptr(), sp,
+                                                     C.byref(c)))
+            return {f: getattr(c, f) for f, _ in TraceCounters._fields_}
+        _check(_LIB.xyzgpu_trace_closest(self.handle, rays.data_ptr(), n, hits.data_ptr(), sp))
+        return None
+
+    def trace(self, org, dirs, tmin: float = 1e-5, tmax: float = float("inf")):
+        """Host convenience: numpy (n,3) origins/directions -> (tri, t, f, g, back)."""
+        import torch
+        org = np.asarray(org, np.float32)
+        dirs = np.asarray(dirs, np.float32)
+        n = org.shape[0]
+        r = np.empty((n, 8), np.float32)
+        r[:, 0:3] = org
+        r[:, 3] = tmin
+        r[:, 4:7] = dirs
+        r[:, 7] = tmax
+        rays = torch.from_numpy(r).cuda()
+        hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        self.trace_device(rays, hits)
+        torch.cuda.synchronize()
+        h = hits.cpu().numpy()
+        code = h[:, 3].view(np.int32)
+        tri = np.where(code >= 0, code >> 1, -1).astype(np.int32)
+        back = np.where(code >= 0, code & 1, 0).astype(np.int32)
+        return tri, h[:, 0].copy(), h[:, 1].copy(), h[:, 2].copy(), back
+
+    # -- rendering --------------------------------------------------------
+    def render(self, camera, width: int, height: int, spp: int, *, seed: int = 0,
+               spp_offset: int = 0, max_depth: int = 15, rr_start_depth: int = 1,
+               rr_threshold: float = 0.2, film=None, accumulate: bool = False,
+               wave_paths: int = 0, profile: int = 0, stream=None):
+        """Renders into `film`: a CUDA tensor (H, W, 3) (device film) or a numpy
+        float32 array (host film).  Allocates a CUDA tensor if film is None.
+        Returns the film (sums over samples, not means)."""
+        cam = CameraDesc()
+        for k in range(3):
+            cam.eye[k] = float(camera.eye[k])
+            cam.at[k] = float(camera.at[k])
+        cam.film_size = float(camera.film_size)
+        cam.focal_length = float(camera.focal_length)
+        cam.f_number = float(camera.f_number)
+        cam.pinhole = int(bool(camera.pinhole))
+        rp = RenderParams()
+        _LIB.xyzgpu_render_params_default(C.byref(rp))
+        rp.width, rp.height, rp.spp, rp.spp_offset = width, height, spp, spp_offset
+        rp.max_depth, rp.rr_start_depth, rp.rr_threshold = max_depth, rr_start_depth, rr_threshold
+        rp.seed = seed
+        rp.accumulate = int(bool(accumulate))
+        rp.wave_paths = wave_paths
+        rp.profile = profile
+        if film is None:
+            import torch
+            film = torch.zeros((height, width, 3), dtype=torch.float32, device="cuda")
+        if isinstance(film, np.ndarray):
+            assert film.dtype == np.float32 and film.flags["C_CONTIGUOUS"] and film.size == width * height * 3
+            rp.film_location = XYZGPU_FILM_HOST
+            ptr = film.ctypes.data
+        else:
+            assert film.is_cuda and film.dtype.__str__() == "torch.float32" and film.is_contiguous()
+            rp.film_location = XYZGPU_FILM_DEVICE
+            ptr = film.data_ptr()
+        _check(_LIB.xyzgpu_render(self.handle, C.byref(cam), C.byref(rp), ptr, _stream_ptr(stream)))
+        return film
+
+    def render_profile(self) -> dict:
+        p = RenderProfile()
+        _check(_LIB.xyzgpu_render_profile_get(self.handle, C.byref(p)))
+        out = {f: getattr(p, f) for f, _ in RenderProfile._fields_ if f not in ("launches", "ms")}
+        out["launches"] = dict(zip(KERNEL_CLASSES, list(p.launches)))
+        out["ms"] = dict(zip(KERNEL_CLASSES, list(p.ms)))
+        return out
+
+    def render_counters(self) -> dict:
+        c = RenderCounters()
+        _check(_LIB.xyzgpu_render_counters_get(self.handle, C.byref(c)))
+        return {f: getattr(c, f) for f, _ in RenderCounters._fields_}
+
+
+def philox_u01(seed: int, pixel: int, sample: int, dim: int) -> float:
+    return load_library().xyzgpu_philox_u01(seed, pixel, sample, dim)

@@ -1,0 +1,426 @@
+// C ABI of the path-tracing library (declarations and reference citations in
+// include/xyzgpu.h): argument checking, scene upload and kd-tree build
+// dispatch, error reporting.  Kernels live in trace.cu, render.cu, kdbuild.cu.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "scene.h"
+
+namespace xyzgpu {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+int set_error(int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+int sm_count(int device) {
+  static int cached[64] = {0};
+  if (device < 0 || device >= 64) return 148;
+  if (cached[device] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0)
+      v = 148;
+    cached[device] = v;
+  }
+  return cached[device];
+}
+
+namespace {
+
+template <class T>
+int dev_upload(T **dst, const std::vector<T> &src, int64_t *bytes) {
+  size_t const n = src.empty() ? 1 : src.size();
+  XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(dst), n * sizeof(T)));
+  if (!src.empty())
+    XYZ_CUDA_TRY(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *bytes += static_cast<int64_t>(n * sizeof(T));
+  return XYZGPU_OK;
+}
+
+void free_scene(SceneImpl *s) {
+  if (!s) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(s->device);
+  render_workspace_free(s->ws);
+  cudaFree(s->d_tri);
+  cudaFree(s->d_ng);
+  cudaFree(s->d_sn);
+  cudaFree(s->d_mat);
+  cudaFree(s->d_lights);
+  cudaFree(s->d_cdf);
+  cudaFree(s->d_nodes);
+  cudaFree(s->d_refs);
+  cudaFree(s->d_fetch);
+  cudaFree(s->d_trace_counts);
+  cudaSetDevice(prev);
+  delete s;
+}
+
+int check_device(int *dev) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return set_error(XYZGPU_E_NODEVICE, "no CUDA device: %s",
+                     e == cudaSuccess ? "device count is 0" : cudaGetErrorString(e));
+  XYZ_CUDA_TRY(cudaGetDevice(dev));
+  int major = 0;
+  XYZ_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, *dev));
+  if (major != 10)
+    return set_error(XYZGPU_E_NODEVICE, "device %d has compute capability %d.x; this library is built for sm_100a",
+                     *dev, major);
+  return XYZGPU_OK;
+}
+
+}  // namespace
+}  // namespace xyzgpu
+
+using namespace xyzgpu;
+
+extern "C" {
+
+int xyzgpu_abi_version(void) { return XYZGPU_ABI_VERSION; }
+
+const char *xyzgpu_last_error(void) { return g_last_error.c_str(); }
+
+float xyzgpu_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim) {
+  uint32_t w[4];
+  philox4x32_10(pixel, sample, dim >> 2, 0u, static_cast<uint32_t>(seed),
+                static_cast<uint32_t>(seed >> 32), w);
+  return u01_from_bits(w[dim & 3u]);
+}
+
+void xyzgpu_build_params_default(xyzgpu_build_params *bp) {
+  if (!bp) return;
+  bp->leaf_max_tris = 4;
+  bp->max_depth = 0;
+  bp->cost_traversal = 1.0f;
+  bp->cost_intersect = 1.5f;
+  bp->empty_bonus = 0.2f;
+  bp->bins = 32;
+  bp->builder = XYZGPU_BUILD_HOST;
+  bp->max_refs_factor = 6;
+}
+
+void xyzgpu_render_params_default(xyzgpu_render_params *rp) {
+  if (!rp) return;
+  std::memset(rp, 0, sizeof(*rp));
+  rp->width = 256;
+  rp->height = 256;
+  rp->spp = 1;
+  rp->spp_offset = 0;
+  rp->max_depth = 15;
+  rp->rr_start_depth = 1;
+  rp->rr_threshold = 0.2f;
+  rp->seed = 0;
+  rp->film_location = XYZGPU_FILM_DEVICE;
+  rp->accumulate = 0;
+  rp->wave_paths = 0;
+  rp->profile = XYZGPU_PROFILE_OFF;
+}
+
+int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *bp_in,
+                        xyzgpu_scene *out) {
+  clear_error();
+  if (!d || !out) return set_error(XYZGPU_E_INVALID, "scene_create: null argument");
+  *out = nullptr;
+  xyzgpu_build_params bp;
+  if (bp_in) {
+    bp = *bp_in;
+  } else {
+    xyzgpu_build_params_default(&bp);
+  }
+  if (d->n_triangles < 0 || d->n_vertices < 0 || d->n_materials < 0)
+    return set_error(XYZGPU_E_INVALID, "scene_create: negative count");
+  if (d->n_triangles >= (1 << 29))
+    return set_error(XYZGPU_E_LIMIT, "scene_create: %d triangles exceeds the limit of 2^29 - 1",
+                     d->n_triangles);
+  if (d->n_triangles > 0 && (!d->positions || !d->triangles || !d->tri_material))
+    return set_error(XYZGPU_E_INVALID, "scene_create: null geometry array");
+  if (d->n_materials > 0 && (!d->albedo_xyz || !d->is_light))
+    return set_error(XYZGPU_E_INVALID, "scene_create: null material array");
+  if (bp.leaf_max_tris < 1 || bp.bins < 2 || bp.bins > kKdMaxBins || bp.max_depth < 0 ||
+      bp.max_depth > kKdMaxDepthLimit || !(bp.cost_traversal >= 0) || !(bp.cost_intersect > 0) ||
+      !(bp.empty_bonus >= 0 && bp.empty_bonus < 1) || bp.max_refs_factor < 1)
+    return set_error(XYZGPU_E_INVALID, "scene_create: build parameters out of range");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(d->light_power_xyz[k]))
+      return set_error(XYZGPU_E_INVALID, "scene_create: light power is not finite");
+  int dev = 0;
+  int rc = check_device(&dev);
+  if (rc) return rc;
+
+  int const nt = d->n_triangles, nv = d->n_vertices, nm = d->n_materials;
+  for (int64_t i = 0; i < 3ll * nv; ++i)
+    if (!std::isfinite(d->positions[i]))
+      return set_error(XYZGPU_E_INVALID, "scene_create: vertex coordinate %lld is not finite",
+                       static_cast<long long>(i));
+  std::vector<float4> tri(3 * static_cast<size_t>(nt)), ng(nt), sn;
+  std::vector<float4> mat(nm > 0 ? nm : 1);
+  std::vector<float> trv(9 * static_cast<size_t>(nt));
+  std::vector<int32_t> lights;
+  std::vector<float> cdf(1, 0.0f);
+  bool const smooth = d->normals != nullptr;
+  if (smooth) sn.resize(3 * static_cast<size_t>(nt));
+  for (int m = 0; m < nm; ++m) {
+    mat[m] = make_float4(d->albedo_xyz[3 * m], d->albedo_xyz[3 * m + 1], d->albedo_xyz[3 * m + 2],
+                         d->is_light[m] ? 1.0f : 0.0f);
+  }
+  for (int i = 0; i < nt; ++i) {
+    int32_t const a = d->triangles[3 * i], b = d->triangles[3 * i + 1], c = d->triangles[3 * i + 2];
+    int32_t const m = d->tri_material[i];
+    if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv)
+      return set_error(XYZGPU_E_INVALID, "scene_create: triangle %d has a vertex index out of range", i);
+    if (m < 0 || m >= nm)
+      return set_error(XYZGPU_E_INVALID, "scene_create: triangle %d has material %d out of range", i, m);
+    f3 const p0 = mk3(d->positions[3 * a], d->positions[3 * a + 1], d->positions[3 * a + 2]);
+    f3 const p1 = mk3(d->positions[3 * b], d->positions[3 * b + 1], d->positions[3 * b + 2]);
+    f3 const p2 = mk3(d->positions[3 * c], d->positions[3 * c + 1], d->positions[3 * c + 2]);
+    // Triangle constructor (xyz/geom/triangle.cpp:35-60)
+    f3 const e1 = sub3(p1, p0), e2 = sub3(p2, p0);
+    f3 const n = cross3(e2, e1);
+    float const r = 1.0f / std::sqrt(dot3(n, n));
+    f3 const g = scl3(n, r);
+    tri[3 * i + 0] = make_float4(p0.x, p0.y, p0.z, n.x);
+    tri[3 * i + 1] = make_float4(e1.x, e1.y, e1.z, n.y);
+    tri[3 * i + 2] = make_float4(e2.x, e2.y, e2.z, n.z);
+    int32_t mbits = m;
+    float mf;
+    std::memcpy(&mf, &mbits, 4);
+    ng[i] = make_float4(g.x, g.y, g.z, mf);
+    f3 const q1 = add3(p0, e1), q2 = add3(p0, e2);
+    float *tv = &trv[9 * static_cast<size_t>(i)];
+    tv[0] = p0.x, tv[1] = p0.y, tv[2] = p0.z;
+    tv[3] = q1.x, tv[4] = q1.y, tv[5] = q1.z;
+    tv[6] = q2.x, tv[7] = q2.y, tv[8] = q2.z;
+    if (smooth) {
+      f3 const n0 = mk3(d->normals[3 * a], d->normals[3 * a + 1], d->normals[3 * a + 2]);
+      f3 const n1 = mk3(d->normals[3 * b], d->normals[3 * b + 1], d->normals[3 * b + 2]);
+      f3 const n2 = mk3(d->normals[3 * c], d->normals[3 * c + 1], d->normals[3 * c + 2]);
+      f3 const s1 = sub3(n1, n0), s2 = sub3(n2, n0);
+      sn[3 * i + 0] = make_float4(n0.x, n0.y, n0.z, 0.0f);
+      sn[3 * i + 1] = make_float4(s1.x, s1.y, s1.z, 0.0f);
+      sn[3 * i + 2] = make_float4(s2.x, s2.y, s2.z, 0.0f);
+    }
+    if (d->is_light[m]) {
+      // light CDF in triangle order (xyz/core/scene_mqo.cpp:512-519)
+      float const area = std::sqrt(dot3(n, n)) * 0.5f;
+      lights.push_back(i);
+      cdf.push_back(cdf.back() + area);
+    }
+  }
+
+  SceneImpl *s = new (std::nothrow) SceneImpl();
+  if (!s) return set_error(XYZGPU_E_NOMEM, "scene_create: host allocation failed");
+  s->device = dev;
+  s->n_tris = nt;
+  s->n_lights = static_cast<int>(lights.size());
+  s->n_materials = nm;
+  s->smooth = smooth;
+  int64_t bytes = 0;
+#define XYZ_TRY_UP(dst, src)                 \
+  do {                                       \
+    int const r_ = dev_upload(dst, src, &bytes); \
+    if (r_) {                                \
+      free_scene(s);                         \
+      return r_;                             \
+    }                                        \
+  } while (0)
+  XYZ_TRY_UP(&s->d_tri, tri);
+  XYZ_TRY_UP(&s->d_ng, ng);
+  if (smooth) XYZ_TRY_UP(&s->d_sn, sn);
+  XYZ_TRY_UP(&s->d_mat, mat);
+  XYZ_TRY_UP(&s->d_lights, lights);
+  XYZ_TRY_UP(&s->d_cdf, cdf);
+#undef XYZ_TRY_UP
+  if (cudaMalloc(&s->d_fetch, 64 * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&s->d_trace_counts, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+    free_scene(s);
+    return set_error(XYZGPU_E_NOMEM, "scene_create: device allocation failed");
+  }
+
+  BuildConfig cfg;
+  cfg.leaf_max_tris = bp.leaf_max_tris;
+  cfg.max_depth = kd_resolve_max_depth(bp.max_depth, nt);
+  cfg.cost_traversal = bp.cost_traversal;
+  cfg.cost_intersect = bp.cost_intersect;
+  cfg.empty_bonus = bp.empty_bonus;
+  cfg.bins = bp.bins;
+  cfg.max_refs = static_cast<int64_t>(bp.max_refs_factor) * nt + 1024;
+  auto const t0 = std::chrono::steady_clock::now();
+  if (bp.builder == XYZGPU_BUILD_HOST) {
+    KdTreeHost tree;
+    std::string err;
+    if (!kd_build_host(trv.data(), nt, cfg, &tree, &err)) {
+      free_scene(s);
+      return set_error(XYZGPU_E_LIMIT, "scene_create: %s", err.c_str());
+    }
+    s->n_nodes = static_cast<int64_t>(tree.nodes.size() / 2);
+    s->n_refs = static_cast<int64_t>(tree.refs.size());
+    s->n_leaves = tree.leaves;
+    s->n_empty = tree.empty_leaves;
+    s->depth = tree.depth;
+    std::vector<uint2> nodes(s->n_nodes);
+    for (int64_t j = 0; j < s->n_nodes; ++j) nodes[j] = make_uint2(tree.nodes[2 * j], tree.nodes[2 * j + 1]);
+    int r2 = dev_upload(&s->d_nodes, nodes, &bytes);
+    if (!r2) r2 = dev_upload(&s->d_refs, tree.refs, &bytes);
+    if (r2) {
+      free_scene(s);
+      return r2;
+    }
+    s->dev.bmin = mk3(tree.bmin[0], tree.bmin[1], tree.bmin[2]);
+    s->dev.bmax = mk3(tree.bmax[0], tree.bmax[1], tree.bmax[2]);
+  } else if (bp.builder == XYZGPU_BUILD_DEVICE) {
+    float bmin[3], bmax[3];
+    kd_root_bounds(trv.data(), nt, bmin, bmax);
+    s->dev.bmin = mk3(bmin[0], bmin[1], bmin[2]);
+    s->dev.bmax = mk3(bmax[0], bmax[1], bmax[2]);
+    int r2 = kd_build_device(*s, s->d_tri, nt, cfg, nullptr);
+    if (r2) {
+      free_scene(s);
+      return r2;
+    }
+    bytes += s->n_nodes * 8 + s->n_refs * 4;
+  } else {
+    free_scene(s);
+    return set_error(XYZGPU_E_INVALID, "scene_create: unknown builder %d", bp.builder);
+  }
+  s->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  s->device_bytes = bytes;
+
+  DevScene &v = s->dev;
+  v.tri = s->d_tri;
+  v.tri_ng = s->d_ng;
+  v.tri_sn = s->d_sn;
+  v.mat = s->d_mat;
+  v.lights = s->d_lights;
+  v.cdf = s->d_cdf;
+  v.nodes = s->d_nodes;
+  v.refs = s->d_refs;
+  // Lights of zero total area cannot be sampled: next-event estimation is off
+  // (the reference would divide by that area, xyz/core/scene.cpp:65).
+  v.n_lights = cdf.back() > 0.0f ? s->n_lights : 0;
+  v.light_area = cdf.back();
+  v.power = mk3(d->light_power_xyz[0], d->light_power_xyz[1], d->light_power_xyz[2]);
+  cudaError_t const e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    free_scene(s);
+    return set_error(XYZGPU_E_CUDA, "scene_create: %s", cudaGetErrorString(e));
+  }
+  *out = reinterpret_cast<xyzgpu_scene>(s);
+  return XYZGPU_OK;
+}
+
+void xyzgpu_scene_destroy(xyzgpu_scene scene) { free_scene(reinterpret_cast<SceneImpl *>(scene)); }
+
+int xyzgpu_scene_stats_get(xyzgpu_scene scene, xyzgpu_scene_stats *o) {
+  clear_error();
+  if (!scene || !o) return set_error(XYZGPU_E_INVALID, "scene_stats_get: null argument");
+  SceneImpl const *s = reinterpret_cast<SceneImpl *>(scene);
+  o->n_triangles = s->n_tris;
+  o->n_lights = s->n_lights;
+  o->n_nodes = s->n_nodes;
+  o->n_leaves = s->n_leaves;
+  o->n_empty_leaves = s->n_empty;
+  o->n_leaf_refs = s->n_refs;
+  o->max_depth = s->depth;
+  o->device_bytes = s->device_bytes;
+  o->build_ms = s->build_ms;
+  o->light_area = s->dev.light_area;
+  o->bounds_min[0] = s->dev.bmin.x, o->bounds_min[1] = s->dev.bmin.y, o->bounds_min[2] = s->dev.bmin.z;
+  o->bounds_max[0] = s->dev.bmax.x, o->bounds_max[1] = s->dev.bmax.y, o->bounds_max[2] = s->dev.bmax.z;
+  return XYZGPU_OK;
+}
+
+int xyzgpu_scene_copy_tree(xyzgpu_scene scene, uint32_t *nodes, int32_t *refs) {
+  clear_error();
+  if (!scene) return set_error(XYZGPU_E_INVALID, "scene_copy_tree: null scene");
+  SceneImpl const *s = reinterpret_cast<SceneImpl *>(scene);
+  if (nodes && s->n_nodes)
+    XYZ_CUDA_TRY(cudaMemcpy(nodes, s->d_nodes, s->n_nodes * 8, cudaMemcpyDeviceToHost));
+  if (refs && s->n_refs)
+    XYZ_CUDA_TRY(cudaMemcpy(refs, s->d_refs, s->n_refs * 4, cudaMemcpyDeviceToHost));
+  return XYZGPU_OK;
+}
+
+int xyzgpu_trace_closest(xyzgpu_scene scene, const float *rays, int n, float *hits, void *stream) {
+  clear_error();
+  if (!scene) return set_error(XYZGPU_E_INVALID, "trace_closest: null scene");
+  if (n < 0) return set_error(XYZGPU_E_INVALID, "trace_closest: negative ray count");
+  if (n > 0 && (!rays || !hits)) return set_error(XYZGPU_E_INVALID, "trace_closest: null buffer");
+  if ((reinterpret_cast<uintptr_t>(rays) | reinterpret_cast<uintptr_t>(hits)) & 15u)
+    return set_error(XYZGPU_E_INVALID, "trace_closest: buffers must be 16-byte aligned");
+  return trace_api_launch(*reinterpret_cast<SceneImpl *>(scene), rays, n, hits,
+                          static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int xyzgpu_trace_closest_counted(xyzgpu_scene scene, const float *rays, int n, float *hits,
+                                 void *stream, xyzgpu_trace_counters *counters) {
+  clear_error();
+  if (!scene || !counters) return set_error(XYZGPU_E_INVALID, "trace_closest_counted: null argument");
+  if (n < 0) return set_error(XYZGPU_E_INVALID, "trace_closest_counted: negative ray count");
+  if (n > 0 && (!rays || !hits)) return set_error(XYZGPU_E_INVALID, "trace_closest_counted: null buffer");
+  if ((reinterpret_cast<uintptr_t>(rays) | reinterpret_cast<uintptr_t>(hits)) & 15u)
+    return set_error(XYZGPU_E_INVALID, "trace_closest_counted: buffers must be 16-byte aligned");
+  return trace_api_launch(*reinterpret_cast<SceneImpl *>(scene), rays, n, hits,
+                          static_cast<cudaStream_t>(stream), counters);
+}
+
+int xyzgpu_render(xyzgpu_scene scene, const xyzgpu_camera *cam, const xyzgpu_render_params *rp,
+                  float *film, void *stream) {
+  clear_error();
+  if (!scene || !cam || !rp || !film) return set_error(XYZGPU_E_INVALID, "render: null argument");
+  if (rp->width <= 0 || rp->height <= 0 || rp->spp < 0 || rp->spp_offset < 0 ||
+      rp->max_depth < 1 || rp->max_depth > 1000 || rp->rr_start_depth < 1 ||
+      !(rp->rr_threshold >= 0.0f) || rp->wave_paths < 0 || rp->profile < 0 || rp->profile > 2 ||
+      (rp->film_location != XYZGPU_FILM_DEVICE && rp->film_location != XYZGPU_FILM_HOST))
+    return set_error(XYZGPU_E_INVALID, "render: parameters out of range");
+  if (static_cast<int64_t>(rp->width) * rp->height >= (1ll << 31))
+    return set_error(XYZGPU_E_LIMIT, "render: image of %d x %d pixels exceeds 2^31", rp->width,
+                     rp->height);
+  if (static_cast<int64_t>(rp->spp_offset) + rp->spp >= (1ll << 32))
+    return set_error(XYZGPU_E_LIMIT, "render: sample index exceeds 2^32");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(cam->eye[k]) || !std::isfinite(cam->at[k]))
+      return set_error(XYZGPU_E_INVALID, "render: camera position is not finite");
+  if (!(cam->film_size > 0) || !(cam->focal_length > 0) || !(cam->f_number > 0))
+    return set_error(XYZGPU_E_INVALID, "render: camera film size, focal length and F-number must be > 0");
+  return render_launch(*reinterpret_cast<SceneImpl *>(scene), *cam, *rp, film,
+                       static_cast<cudaStream_t>(stream));
+}
+
+int xyzgpu_render_counters_get(xyzgpu_scene scene, xyzgpu_render_counters *out) {
+  clear_error();
+  if (!scene || !out) return set_error(XYZGPU_E_INVALID, "render_counters_get: null argument");
+  SceneImpl &s = *reinterpret_cast<SceneImpl *>(scene);
+  int const rc = render_collect(s);
+  if (rc) return rc;
+  *out = s.counters;
+  return XYZGPU_OK;
+}
+
+int xyzgpu_render_profile_get(xyzgpu_scene scene, xyzgpu_render_profile *out) {
+  clear_error();
+  if (!scene || !out) return set_error(XYZGPU_E_INVALID, "render_profile_get: null argument");
+  SceneImpl &s = *reinterpret_cast<SceneImpl *>(scene);
+  int const rc = render_collect(s);
+  if (rc) return rc;
+  *out = s.profile;
+  return XYZGPU_OK;
+}
+
+}  // extern "C"

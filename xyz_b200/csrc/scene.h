@@ -1,0 +1,87 @@
+// Host-side scene object behind the xyzgpu_scene handle, plus the error and
+// CUDA-check helpers shared by the C ABI implementation files.
+#pragma once
+
+#include <cstdarg>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/xyzgpu.h"
+#include "common.cuh"
+#include "kdtree.h"
+
+namespace xyzgpu {
+
+int set_error(int code, const char *fmt, ...);
+void clear_error();
+
+#define XYZ_CUDA_TRY(call)                                                                   \
+  do {                                                                                       \
+    cudaError_t const e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                                   \
+      return ::xyzgpu::set_error(XYZGPU_E_CUDA, "%s failed: %s (%s:%d)", #call,              \
+                                 cudaGetErrorString(e_), __FILE__, __LINE__);                \
+  } while (0)
+
+// Device buffers of one render wave (paths in flight), kept between calls.
+struct RenderWorkspace {
+  int64_t capacity = 0;   // paths
+  int max_iters = 0;      // count slots allocated
+  float4 *beta = nullptr;     // throughput xyz, fSamplingNext
+  uint32_t *misc = nullptr;   // dim | k << 16 | specular << 31
+  float4 *radiance = nullptr; // accumulated XYZ of the path
+  float4 *q_o[2] = {nullptr, nullptr};
+  float4 *q_d[2] = {nullptr, nullptr};
+  int32_t *q_slot[2] = {nullptr, nullptr};
+  float4 *hits = nullptr;
+  float4 *s_o = nullptr, *s_d = nullptr, *s_pb = nullptr;
+  int32_t *s_target = nullptr;
+  int32_t *counts = nullptr;  // per iteration counters (see render.cu)
+  unsigned long long *tally = nullptr;  // [0] ext rays [1] shadow rays [2] visible, then
+                                        // [8..] traversal counters of COUNTERS renders
+  std::vector<cudaEvent_t> events;      // timing pairs of TIMING renders
+  float *film_dev = nullptr;  // staging film for host-film renders
+  float *film_pinned = nullptr;
+  int64_t film_elems = 0;
+};
+
+struct SceneImpl {
+  int device = 0;
+  int n_tris = 0, n_lights = 0, n_materials = 0;
+  bool smooth = false;
+  DevScene dev{};
+  // device allocations owned here
+  float4 *d_tri = nullptr, *d_ng = nullptr, *d_sn = nullptr, *d_mat = nullptr;
+  int32_t *d_lights = nullptr;
+  float *d_cdf = nullptr;
+  uint2 *d_nodes = nullptr;
+  int32_t *d_refs = nullptr;
+  int64_t n_nodes = 0, n_refs = 0, n_leaves = 0, n_empty = 0;
+  int depth = 0;
+  int64_t device_bytes = 0;
+  double build_ms = 0.0;
+  RenderWorkspace ws;
+  xyzgpu_render_counters counters{};
+  xyzgpu_render_profile profile{};
+  bool profile_pending = false;  // profile needs the events / counters read back
+  int profile_mode = 0;
+  std::vector<int> event_class;   // class of each recorded event pair
+  int32_t *d_fetch = nullptr;  // work-fetch counters of the trace API kernel
+  unsigned long long *d_trace_counts = nullptr;
+};
+
+// Kernels' host-side launchers (trace.cu, render.cu, kdbuild.cu).
+int trace_api_launch(SceneImpl &s, const float *rays, int n, float *hits, cudaStream_t st,
+                     xyzgpu_trace_counters *counters);
+int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp,
+                  float *film, cudaStream_t st);
+void render_workspace_free(RenderWorkspace &ws);
+int render_collect(SceneImpl &s);
+int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig &cfg,
+                    cudaStream_t st);
+int sm_count(int device);
+
+}  // namespace xyzgpu

@@ -1,0 +1,139 @@
+// kd-tree closest-hit traversal for one ray (device).
+//
+// Semantics of the reference (xyz/geom/kdtree.cpp:82-150, 366-372):
+//   * at an interior node, the plane distance e splits [t_min, t_max]; the near
+//     child is the side holding the origin; e > t_max or e < 0 -> near only,
+//     e < t_min -> far only, otherwise near on [t_min, e] then far on
+//     [e, t_max];
+//   * a leaf tests all its triangles with the double-faced Moller-Trumbore test
+//     (xyz/geom/triangle.cpp:127-165): |det| < 1e-6 rejects, t must lie in the
+//     interval (inclusive), barycentrics f, g >= 0 and f + g <= 1; an accepted
+//     hit shrinks t_max, so among equal t the later triangle of a leaf wins;
+//   * traversal stops at the first leaf (front to back) that produced a hit.
+// Differences, all of which leave the closest hit unchanged: the ray is first
+// clipped to the scene box, and triangles are tested against the ray's whole
+// remaining interval [t_min, best_t] rather than the node's clipped interval,
+// stopping once best_t <= the leaf's exit distance (robust to a hit that
+// rounds across a split plane).  The plane distance uses a precomputed
+// reciprocal of the direction.
+#pragma once
+
+#include "common.cuh"
+
+namespace xyzgpu {
+
+struct TraceCount {
+  uint32_t nodes, leaves, tris;
+};
+
+struct RayHit {
+  float t, f, g;
+  int32_t id;    // triangle id, -1 = miss
+  int32_t back;  // 1 = hit from the back side (det > 0)
+};
+
+// FindIntersectionDF on a packed triangle; updates best_t on acceptance.
+XYZ_DEV bool hit_triangle(const float4 *__restrict__ tri, int32_t i, f3 o, f3 d, float tmin,
+                          RayHit &h) {
+  float4 const a = __ldg(&tri[3 * i + 0]);
+  float4 const b = __ldg(&tri[3 * i + 1]);
+  float4 const c = __ldg(&tri[3 * i + 2]);
+  f3 const e2xe1 = mk3(a.w, b.w, c.w);
+  float const det = dot3(d, e2xe1);
+  if (fabsf(det) < kEpsilon) return false;
+  float const inv_det = __frcp_rn(det);
+  f3 const vmo = sub3(xyz3(a), o);
+  float const t = inv_det * dot3(vmo, e2xe1);
+  if ((t < tmin) || (h.t < t)) return false;
+  f3 const dxvmo = cross3(d, vmo);
+  float const f = inv_det * dot3(xyz3(c), dxvmo);
+  if ((f < 0.0f) || (f > 1.0f)) return false;
+  float const g = inv_det * -dot3(xyz3(b), dxvmo);
+  if ((g < 0.0f) || ((f + g) > 1.0f)) return false;
+  h.t = t;
+  h.f = f;
+  h.g = g;
+  h.id = i;
+  h.back = det > 0.0f;
+  return true;
+}
+
+struct StackEntry {
+  uint32_t node;
+  float tn, tf;
+};
+
+// Closest hit in [tmin, tmax].  h.id = -1 on a miss.  Counts work if cnt != 0.
+template <bool kCount>
+XYZ_DEV void trace_closest(const DevScene &S, f3 o, f3 d, float tmin, float tmax, RayHit &h,
+                           TraceCount *cnt) {
+  h.t = tmax;
+  h.id = -1;
+  h.f = h.g = 0.0f;
+  h.back = 0;
+  float const inv[3] = {__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z)};
+  float const org[3] = {o.x, o.y, o.z};
+  float const lo[3] = {S.bmin.x, S.bmin.y, S.bmin.z};
+  float const hi[3] = {S.bmax.x, S.bmax.y, S.bmax.z};
+  float t0 = tmin, t1 = tmax;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float const ta = (lo[k] - org[k]) * inv[k];
+    float const tb = (hi[k] - org[k]) * inv[k];
+    t0 = fmaxf(t0, fminf(ta, tb));
+    t1 = fminf(t1, fmaxf(ta, tb));
+  }
+  if (!(t0 <= t1)) return;
+
+  StackEntry stack[kKdMaxDepthLimit];
+  int sp = 0;
+  uint32_t node = 0;
+  float tn = t0, tf = t1;
+  for (;;) {
+    uint2 nd = __ldg(&S.nodes[node]);
+    if (kCount) cnt->nodes++;
+    while ((nd.y & 3u) != kKdLeafTag) {
+      uint32_t const ax = nd.y & 3u;
+      float const split = __uint_as_float(nd.x);
+      uint32_t const child = nd.y >> 2;
+      float const oa = ax == 0 ? org[0] : (ax == 1 ? org[1] : org[2]);
+      float const ia = ax == 0 ? inv[0] : (ax == 1 ? inv[1] : inv[2]);
+      float const tp = (split - oa) * ia;
+      uint32_t const below = oa < split ? 0u : 1u;
+      uint32_t const first = child + below;
+      uint32_t const second = child + (below ^ 1u);
+      if ((tp > tf) || (tp < 0.0f)) {
+        node = first;
+      } else if (tp < tn) {
+        node = second;
+      } else {
+        stack[sp].node = second;
+        stack[sp].tn = tp;
+        stack[sp].tf = tf;
+        ++sp;
+        node = first;
+        tf = tp;
+      }
+      nd = __ldg(&S.nodes[node]);
+      if (kCount) cnt->nodes++;
+    }
+    uint32_t const n = nd.y >> 2;
+    if (kCount) {
+      cnt->leaves++;
+      cnt->tris += n;
+    }
+    for (uint32_t j = 0; j < n; ++j) {
+      int32_t const i = __ldg(&S.refs[nd.x + j]);
+      hit_triangle(S.tri, i, o, d, tmin, h);
+    }
+    if (h.id >= 0 && h.t <= tf) break;
+    if (sp == 0) break;
+    --sp;
+    node = stack[sp].node;
+    tn = stack[sp].tn;
+    tf = stack[sp].tf;
+    if (h.id >= 0 && h.t < tn) break;
+  }
+}
+
+}  // namespace xyzgpu
