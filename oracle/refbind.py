@@ -209,6 +209,22 @@ class PortLib(_Common):
         self._keep = (pos, tris, mat, alb, lit, nrm, pw)
         return r
 
+    def eval_path_record(self, px: int, py: int, s: int, seed: int, cap: int = 64):
+        """One path with its traced segments: (xyz, dims, rays (n,6), tri, t, kind)."""
+        out = np.zeros(3, np.float32)
+        rays = np.zeros((cap, 6), np.float32)
+        tri = np.zeros(cap, np.int32)
+        t = np.zeros(cap, np.float32)
+        kind = np.zeros(cap, np.int32)
+        n = C.c_int(0)
+        f = self.lib.xyzo_eval_path_record
+        f.restype = C.c_int
+        dims = f(px, py, s, C.c_uint64(seed), out.ctypes.data_as(C.c_void_p), cap,
+                 rays.ctypes.data_as(C.c_void_p), tri.ctypes.data_as(C.c_void_p),
+                 t.ctypes.data_as(C.c_void_p), kind.ctypes.data_as(C.c_void_p), C.byref(n))
+        k = n.value
+        return out, dims, rays[:k], tri[:k], t[:k], kind[:k]
+
     def philox_u01(self, seed, pixel, sample, dim):
         return self.lib.xyzo_philox_u01(C.c_uint64(seed), pixel, sample, dim)
 

@@ -391,6 +391,30 @@ static inline void acc_d(f3 *c, double x, double y, double z) {
   c->z += (float)z;
 }
 
+/* Optional per-path recorder for debugging: every traced segment's ray, hit
+ * triangle and kind (0 extension, 1 shadow). */
+typedef struct {
+  int n, cap;
+  float *rays;  /* 6 per segment: origin, direction */
+  int *tri, *kind;
+  float *t;
+} recorder_t;
+static __thread recorder_t *REC = NULL;
+
+static inline void rec_seg(f3 o, f3 d, int tri, float t, int kind) {
+  if (!REC || REC->n >= REC->cap) return;
+  int const i = REC->n++;
+  REC->rays[6 * i + 0] = o.x;
+  REC->rays[6 * i + 1] = o.y;
+  REC->rays[6 * i + 2] = o.z;
+  REC->rays[6 * i + 3] = d.x;
+  REC->rays[6 * i + 4] = d.y;
+  REC->rays[6 * i + 5] = d.z;
+  REC->tri[i] = tri;
+  REC->t[i] = t;
+  REC->kind[i] = kind;
+}
+
 static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
   xyzo_stream st;
   xyzo_stream_init(&st, seed, (uint32_t)(py * CAM.W + px), (uint32_t)s, 0u);
@@ -456,6 +480,7 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
   for (size_t k = 1;;) {
     isect_t p;
     int const tri = find_intersection(pos, dir, &p);
+    rec_seg(pos, dir, tri, tri >= 0 ? p.tmax : 0.0f, 0);
     if (tri < 0) break;
     frame_t fr;
     shading_basis(tri, p.f, p.g, p.back, &fr);
@@ -492,7 +517,9 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
         float const nk2 = -dot3(vin, fr.sn);
         if (!((nk2 <= 0) || (-dot3(vin, fr.gn) <= 0))) {
           isect_t q;
-          if (find_intersection(lpos, vin, &q) == tri) {
+          int const sh = find_intersection(lpos, vin, &q);
+          rec_seg(lpos, vin, sh, sh >= 0 ? q.tmax : 0.0f, 1);
+          if (sh == tri) {
             float const G = nk2 * nk3 / (q.tmax * q.tmax);
             float const dimp = (float)(XYZO_M_1_PI * (double)G);
             float const dexp = 1.0f / A;
@@ -770,6 +797,21 @@ int xyzo_eval_path(int px, int py, int s, uint64_t seed, float *out) {
   out[0] = c.x;
   out[1] = c.y;
   out[2] = c.z;
+  return dims;
+}
+
+/* eval_path with every traced segment recorded (debugging aid). */
+int xyzo_eval_path_record(int px, int py, int s, uint64_t seed, float *out, int cap, float *rays,
+                          int *tri, float *t, int *kind, int *n_seg) {
+  recorder_t r = {0, cap, rays, tri, kind, t};
+  REC = &r;
+  f3 c;
+  int const dims = eval_path(px, py, s, seed, &c);
+  REC = NULL;
+  out[0] = c.x;
+  out[1] = c.y;
+  out[2] = c.z;
+  *n_seg = r.n;
   return dims;
 }
 

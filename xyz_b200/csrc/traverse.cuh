@@ -15,7 +15,8 @@
 // remaining interval [t_min, best_t] rather than the node's clipped interval,
 // stopping once best_t <= the leaf's exit distance (robust to a hit that
 // rounds across a split plane).  The plane distance uses a precomputed
-// reciprocal of the direction.
+// reciprocal of the direction.  A ray that starts exactly on a split plane
+// continues on the side its direction points to.
 #pragma once
 
 #include "common.cuh"
@@ -98,11 +99,15 @@ XYZ_DEV void trace_closest(const DevScene &S, f3 o, f3 d, float tmin, float tmax
       uint32_t const child = nd.y >> 2;
       float const oa = ax == 0 ? org[0] : (ax == 1 ? org[1] : org[2]);
       float const ia = ax == 0 ? inv[0] : (ax == 1 ? inv[1] : inv[2]);
+      float const da = ax == 0 ? d.x : (ax == 1 ? d.y : d.z);
       float const tp = (split - oa) * ia;
-      uint32_t const below = oa < split ? 0u : 1u;
-      uint32_t const first = child + below;
-      uint32_t const second = child + (below ^ 1u);
-      if ((tp > tf) || (tp < 0.0f)) {
+      // near side: the origin's side; an origin on the plane takes the side
+      // its direction enters (the reference would take the far child there,
+      // since its plane distance 0 is below t_min, and skip the near one).
+      uint32_t const above_first = (oa < split || (oa == split && da <= 0.0f)) ? 0u : 1u;
+      uint32_t const first = child + above_first;
+      uint32_t const second = child + (above_first ^ 1u);
+      if ((tp > tf) || (tp <= 0.0f)) {
         node = first;
       } else if (tp < tn) {
         node = second;

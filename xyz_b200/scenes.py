@@ -287,7 +287,7 @@ def spheres_scene(level: int = 7, n_spheres: int = 3, seed: int = 0,
         base += v.shape[0]
     # ground (front side up)
     g = np.array([(-20, 0, -20), (20, 0, -20), (20, 0, 20), (-20, 0, 20)], dtype=np.float64)
-    gt = np.array([(0, 2, 1), (0, 3, 2)], dtype=np.int64)
+    gt = np.array([(0, 1, 2), (0, 2, 3)], dtype=np.int64)   # front normal +y
     pos_l.append(g)
     tri_l.append(gt + base)
     norm_l.append(np.tile(np.array([[0, 1, 0]], np.float32), (4, 1)))
