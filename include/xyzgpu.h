@@ -196,6 +196,28 @@ typedef struct {
 
 int xyzgpu_render_profile_get(xyzgpu_scene scene, xyzgpu_render_profile *out);
 
+/* Rendering without allocation.  No counterpart in the reference (which
+ * renders on the CPU and never allocates GPU memory); it exists for callers
+ * that cannot allocate device memory while running - an application that
+ * gives all GPU memory to its own pool at start-up, a real-time loop that may
+ * not call the allocator mid-frame, a process with a fixed memory budget.
+ * Same image as xyzgpu_render for the same parameters, but the path state and
+ * queues live in one file-scope device array of XYZGPU_NOALLOC_SCRATCH_BYTES
+ * that every device loading the library holds until exit, so at most
+ * XYZGPU_NOALLOC_MAX_WAVE_PATHS paths are in flight at a time.
+ * Limits (else XYZGPU_E_LIMIT / XYZGPU_E_INVALID): film in device memory,
+ * max_depth <= XYZGPU_NOALLOC_MAX_DEPTH, wave_paths <= the wave maximum,
+ * profile off.  The first call on a device looks up the array's address
+ * (make that first call before any stream capture).  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised.
+ * Allocates nothing: no cudaMalloc, cudaFree or host allocation of pinned
+ * memory. */
+#define XYZGPU_NOALLOC_MAX_WAVE_PATHS 65536
+#define XYZGPU_NOALLOC_MAX_DEPTH 64
+#define XYZGPU_NOALLOC_SCRATCH_BYTES 11536896
+int xyzgpu_render_noalloc(xyzgpu_scene scene, const xyzgpu_camera *camera,
+                          const xyzgpu_render_params *rp, float *film_device, void *stream);
+
 /* Host evaluation of the random stream defined above (for tests). */
 float xyzgpu_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim);
 

@@ -1,0 +1,58 @@
+"""xyzgpu_render_noalloc: rendering for callers that cannot allocate device
+memory while they run (an application that gives all GPU memory to its own
+pool at start-up, a real-time loop that may not call the allocator mid-frame).
+Its path state lives in a fixed file-scope device array; the image must be the
+one xyzgpu_render produces.  This file is collected last on purpose."""
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_noalloc_render_equals_render_on_two_calls_in_a_row():
+    import torch
+    from xyz_b200 import api, scenes
+    sd = scenes.cornell_box(pinhole=True)
+    thin = scenes.cornell_box(pinhole=False).camera
+    # the second call is smaller and shallower, so stale queue lengths or
+    # radiance left in the shared array by the first call would show up
+    cases = [dict(cam=sd.camera, W=96, H=64, spp=5, seed=3, depth=12),
+             dict(cam=thin, W=40, H=30, spp=2, seed=9, depth=6)]
+    with api.Scene(sd) as s:
+        for c in cases:
+            ref = s.render(c["cam"], c["W"], c["H"], c["spp"], seed=c["seed"], max_depth=c["depth"])
+            film = torch.full((c["H"], c["W"], 3), float("nan"), device="cuda")
+            s.render_noalloc(c["cam"], c["W"], c["H"], c["spp"], film, seed=c["seed"],
+                             max_depth=c["depth"])
+            torch.cuda.synchronize()
+            # per-path results do not depend on the wave size: identical films
+            assert torch.equal(film, ref)
+
+
+def test_noalloc_render_rejects_sizes_beyond_its_limits():
+    import numpy as np
+    import torch
+    from xyz_b200 import api, scenes
+    sd = scenes.cornell_box()
+    film = torch.zeros((8, 8, 3), device="cuda")
+    with api.Scene(sd) as s:
+        with pytest.raises(api.XyzGpuError) as e:
+            s.render_noalloc(sd.camera, 8, 8, 1, film, max_depth=65)
+        assert e.value.code == -4 and "max_depth" in str(e.value)
+        with pytest.raises(api.XyzGpuError) as e:
+            s.render_noalloc(sd.camera, 8, 8, 1, film, wave_paths=65537)
+        assert e.value.code == -4 and "wave_paths" in str(e.value)
+        # a host film would need a device staging buffer
+        L = api.load_library()
+        cam = api.CameraDesc()
+        for k in range(3):
+            cam.eye[k], cam.at[k] = sd.camera.eye[k], sd.camera.at[k]
+        cam.film_size, cam.focal_length, cam.f_number, cam.pinhole = (
+            sd.camera.film_size, sd.camera.focal_length, sd.camera.f_number, 1)
+        rp = api.RenderParams()
+        L.xyzgpu_render_params_default(api.C.byref(rp))
+        rp.width = rp.height = 8
+        rp.film_location = api.XYZGPU_FILM_HOST
+        host = np.zeros((8, 8, 3), np.float32)
+        assert L.xyzgpu_render_noalloc(s.handle, api.C.byref(cam), api.C.byref(rp),
+                                       host.ctypes.data, None) == -1

@@ -30,7 +30,8 @@ EXPORTED = [
     "xyzgpu_build_params_default", "xyzgpu_scene_create", "xyzgpu_scene_destroy",
     "xyzgpu_scene_stats_get", "xyzgpu_scene_copy_tree", "xyzgpu_trace_closest",
     "xyzgpu_trace_closest_counted", "xyzgpu_render_params_default", "xyzgpu_render",
-    "xyzgpu_render_counters_get", "xyzgpu_render_profile_get", "xyzgpu_philox_u01", "xyzgpu_last_error", "xyzgpu_abi_version",
+    "xyzgpu_render_counters_get", "xyzgpu_render_profile_get", "xyzgpu_render_noalloc",
+    "xyzgpu_philox_u01", "xyzgpu_last_error", "xyzgpu_abi_version",
 ]
 
 
@@ -115,6 +116,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                                C.POINTER(TraceCounters)]
     L.xyzgpu_render.argtypes = [C.c_void_p, C.POINTER(CameraDesc), C.POINTER(RenderParams), C.c_void_p,
                                 C.c_void_p]
+    L.xyzgpu_render_noalloc.argtypes = [C.c_void_p, C.POINTER(CameraDesc), C.POINTER(RenderParams),
+                                        C.c_void_p, C.c_void_p]
     L.xyzgpu_render_counters_get.argtypes = [C.c_void_p, C.POINTER(RenderCounters)]
     L.xyzgpu_render_profile_get.argtypes = [C.c_void_p, C.POINTER(RenderProfile)]
     L.xyzgpu_philox_u01.restype = C.c_float
@@ -284,6 +287,33 @@ class Scene:
             rp.film_location = XYZGPU_FILM_DEVICE
             ptr = film.data_ptr()
         _check(_LIB.xyzgpu_render(self.handle, C.byref(cam), C.byref(rp), ptr, _stream_ptr(stream)))
+        return film
+
+    def render_noalloc(self, camera, width: int, height: int, spp: int, film, *, seed: int = 0,
+                       spp_offset: int = 0, max_depth: int = 15, rr_start_depth: int = 1,
+                       rr_threshold: float = 0.2, accumulate: bool = False, wave_paths: int = 0,
+                       stream=None):
+        """xyzgpu_render_noalloc: same image as render(), for callers that cannot
+        allocate device memory while rendering.  `film` must be a CUDA tensor
+        (H, W, 3) float32 that the caller owns; nothing is allocated."""
+        cam = CameraDesc()
+        for k in range(3):
+            cam.eye[k] = float(camera.eye[k])
+            cam.at[k] = float(camera.at[k])
+        cam.film_size = float(camera.film_size)
+        cam.focal_length = float(camera.focal_length)
+        cam.f_number = float(camera.f_number)
+        cam.pinhole = int(bool(camera.pinhole))
+        rp = RenderParams()
+        _LIB.xyzgpu_render_params_default(C.byref(rp))
+        rp.width, rp.height, rp.spp, rp.spp_offset = width, height, spp, spp_offset
+        rp.max_depth, rp.rr_start_depth, rp.rr_threshold = max_depth, rr_start_depth, rr_threshold
+        rp.seed = seed
+        rp.accumulate = int(bool(accumulate))
+        rp.wave_paths = wave_paths
+        rp.film_location = XYZGPU_FILM_DEVICE
+        _check(_LIB.xyzgpu_render_noalloc(self.handle, C.byref(cam), C.byref(rp), film.data_ptr(),
+                                          _stream_ptr(stream)))
         return film
 
     def render_profile(self) -> dict:

@@ -403,6 +403,31 @@ int xyzgpu_render(xyzgpu_scene scene, const xyzgpu_camera *cam, const xyzgpu_ren
                        static_cast<cudaStream_t>(stream));
 }
 
+int xyzgpu_render_noalloc(xyzgpu_scene scene, const xyzgpu_camera *cam,
+                          const xyzgpu_render_params *rp, float *film, void *stream) {
+  clear_error();
+  if (!scene || !cam || !rp || !film) return set_error(XYZGPU_E_INVALID, "render_noalloc: null argument");
+  if (rp->width <= 0 || rp->height <= 0 || rp->spp < 0 || rp->spp_offset < 0 ||
+      rp->max_depth < 1 || rp->rr_start_depth < 1 || !(rp->rr_threshold >= 0.0f) ||
+      rp->wave_paths < 0)
+    return set_error(XYZGPU_E_INVALID, "render_noalloc: parameters out of range");
+  if (static_cast<int64_t>(rp->width) * rp->height >= (1ll << 31))
+    return set_error(XYZGPU_E_LIMIT, "render_noalloc: image of %d x %d pixels exceeds 2^31",
+                     rp->width, rp->height);
+  if (static_cast<int64_t>(rp->spp_offset) + rp->spp >= (1ll << 32))
+    return set_error(XYZGPU_E_LIMIT, "render_noalloc: sample index exceeds 2^32");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(cam->eye[k]) || !std::isfinite(cam->at[k]))
+      return set_error(XYZGPU_E_INVALID, "render_noalloc: camera position is not finite");
+  if (!(cam->film_size > 0) || !(cam->focal_length > 0) || !(cam->f_number > 0))
+    return set_error(XYZGPU_E_INVALID,
+                     "render_noalloc: camera film size, focal length and F-number must be > 0");
+  if (reinterpret_cast<uintptr_t>(film) & 3u)
+    return set_error(XYZGPU_E_INVALID, "render_noalloc: film must be 4-byte aligned");
+  return render_noalloc_launch(*reinterpret_cast<SceneImpl *>(scene), *cam, *rp, film,
+                               static_cast<cudaStream_t>(stream));
+}
+
 int xyzgpu_render_counters_get(xyzgpu_scene scene, xyzgpu_render_counters *out) {
   clear_error();
   if (!scene || !out) return set_error(XYZGPU_E_INVALID, "render_counters_get: null argument");

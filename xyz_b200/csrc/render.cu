@@ -27,7 +27,9 @@
 // Every path reads its own Philox stream (include/xyzgpu.h), so the result does
 // not depend on the wave size or on the order in which queues are filled.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "scene.h"
 #include "traverse.cuh"
@@ -749,6 +751,183 @@ int render_collect(SceneImpl &s) {
     }
   }
   s.profile_pending = false;
+  return XYZGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// xyzgpu_render_noalloc: rendering for callers that cannot allocate.
+//
+// Some hosts must not allocate device memory once they are running: a
+// renderer embedded in an application that hands all GPU memory to its own
+// pool at start-up, a real-time loop that may not enter the driver's allocator
+// (and its implicit synchronisation) in the middle of a frame, or a process
+// whose memory budget is fixed when it starts.  xyzgpu_render allocates the
+// per-scene path state and queues on its first call and again whenever a
+// larger wave is asked for; this entry point instead keeps them in one
+// file-scope device array of fixed size, so it performs no allocation at all.
+// The scene (created beforehand) and the device film are the caller's.
+//
+// The array is XYZGPU_NOALLOC_SCRATCH_BYTES on every device that loads the
+// library, held until the process exits.  It holds the state of at most
+// XYZGPU_NOALLOC_MAX_WAVE_PATHS paths in flight, so large images render in
+// more, smaller waves than xyzgpu_render uses (same image, lower throughput).
+// Every call on a device shares the array and it keeps the previous call's
+// contents: calls that overlap on the GPU (different streams, threads or
+// scenes) race and must be serialised by the caller.
+namespace {
+
+constexpr int64_t kNoAllocPaths = XYZGPU_NOALLOC_MAX_WAVE_PATHS;
+constexpr int kNoAllocDepth = XYZGPU_NOALLOC_MAX_DEPTH;
+constexpr size_t kSeg = 256;
+constexpr size_t seg(size_t bytes) { return (bytes + kSeg - 1) / kSeg * kSeg; }
+constexpr size_t kNoAllocF4 = seg(kNoAllocPaths * sizeof(float4));
+constexpr size_t kNoAllocI4 = seg(kNoAllocPaths * sizeof(int32_t));
+constexpr size_t kNoAllocCounts = seg((kNoAllocDepth + 2) * kCountStride * sizeof(int32_t));
+constexpr size_t kNoAllocTally = seg(16 * sizeof(unsigned long long));
+// beta, radiance, q_o[2], q_d[2], hits, s_o, s_d, s_pb: 10 float4 arrays;
+// misc, q_slot[2], s_target: 4 int arrays.
+constexpr size_t kNoAllocBytes = 10 * kNoAllocF4 + 4 * kNoAllocI4 + kNoAllocCounts + kNoAllocTally;
+static_assert(kNoAllocBytes == XYZGPU_NOALLOC_SCRATCH_BYTES,
+              "XYZGPU_NOALLOC_SCRATCH_BYTES must match the scratch layout");
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_base[64] = {nullptr};
+
+// Device address of g_noalloc_scratch on `device` (which must be current).
+// The first call on a device looks the symbol up; later calls reuse it.
+int noalloc_scratch(int device, unsigned char **out) {
+  if (device < 0 || device >= 64)
+    return set_error(XYZGPU_E_LIMIT, "render_noalloc: device ordinal %d is beyond 63", device);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_base[device]) {
+    void *p = nullptr;
+    cudaError_t const e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return set_error(XYZGPU_E_CUDA, "render_noalloc: cudaGetSymbolAddress failed: %s",
+                       cudaGetErrorString(e));
+    g_noalloc_base[device] = p;
+  }
+  *out = static_cast<unsigned char *>(g_noalloc_base[device]);
+  return XYZGPU_OK;
+}
+
+CamDev noalloc_camera(const xyzgpu_camera &cam, int width, int height) {
+  // ThinLensCamera::Reset (thinlenscamera.cpp:71-90), as in render_launch.
+  CamDev C;
+  C.eye = mk3(cam.eye[0], cam.eye[1], cam.eye[2]);
+  f3 const at = mk3(cam.at[0], cam.at[1], cam.at[2]);
+  f3 const view = sub3(C.eye, at);
+  C.L = std::sqrt(dot3(view, view));
+  C.V = C.L * cam.focal_length / (C.L - cam.focal_length);
+  C.R = cam.focal_length / (2 * cam.f_number);
+  float const r = 1.0f / std::sqrt(dot3(view, view));
+  C.back = scl3(view, r);
+  f3 const rr = cross3(mk3(0.0f, 1.0f, 0.0f), C.back);
+  float const r2 = 1.0f / std::sqrt(dot3(rr, rr));
+  C.right = scl3(rr, r2);
+  C.up = cross3(C.back, C.right);
+  C.film = cam.film_size;
+  C.aspect = static_cast<float>(width) / static_cast<float>(height);
+  C.pinhole = cam.pinhole ? 1 : 0;
+  return C;
+}
+
+}  // namespace
+
+int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp,
+                          float *film, cudaStream_t st) {
+  if (rp.film_location != XYZGPU_FILM_DEVICE)
+    return set_error(XYZGPU_E_INVALID, "render_noalloc: the film must be device memory");
+  if (rp.profile != XYZGPU_PROFILE_OFF)
+    return set_error(XYZGPU_E_INVALID, "render_noalloc: profiling is not available");
+  if (rp.wave_paths > kNoAllocPaths)
+    return set_error(XYZGPU_E_LIMIT, "render_noalloc: wave_paths %d exceeds the maximum of %lld",
+                     rp.wave_paths, static_cast<long long>(kNoAllocPaths));
+  if (rp.max_depth > kNoAllocDepth)
+    return set_error(XYZGPU_E_LIMIT, "render_noalloc: max_depth %d exceeds the maximum of %d",
+                     rp.max_depth, kNoAllocDepth);
+  XYZ_CUDA_TRY(cudaSetDevice(s.device));
+  unsigned char *base = nullptr;
+  int rc = noalloc_scratch(s.device, &base);
+  if (rc) return rc;
+
+  WaveArgs A;
+  std::memset(&A, 0, sizeof(A));
+  unsigned char *p = base;
+  auto take = [&p](size_t bytes) {
+    unsigned char *q = p;
+    p += bytes;
+    return q;
+  };
+  A.beta = reinterpret_cast<float4 *>(take(kNoAllocF4));
+  A.radiance = reinterpret_cast<float4 *>(take(kNoAllocF4));
+  for (int q = 0; q < 2; ++q) {
+    A.q_o[q] = reinterpret_cast<float4 *>(take(kNoAllocF4));
+    A.q_d[q] = reinterpret_cast<float4 *>(take(kNoAllocF4));
+  }
+  A.hits = reinterpret_cast<float4 *>(take(kNoAllocF4));
+  A.s_o = reinterpret_cast<float4 *>(take(kNoAllocF4));
+  A.s_d = reinterpret_cast<float4 *>(take(kNoAllocF4));
+  A.s_pb = reinterpret_cast<float4 *>(take(kNoAllocF4));
+  A.misc = reinterpret_cast<uint32_t *>(take(kNoAllocI4));
+  for (int q = 0; q < 2; ++q) A.q_slot[q] = reinterpret_cast<int32_t *>(take(kNoAllocI4));
+  A.s_target = reinterpret_cast<int32_t *>(take(kNoAllocI4));
+  A.counts = reinterpret_cast<int32_t *>(take(kNoAllocCounts));
+  unsigned long long *tally = reinterpret_cast<unsigned long long *>(take(kNoAllocTally));
+
+  A.S = s.dev;
+  A.cam = noalloc_camera(cam, rp.width, rp.height);
+  A.W = rp.width;
+  A.H = rp.height;
+  A.kmax = rp.max_depth + 1;
+  A.rr_start = rp.rr_start_depth;
+  A.rr_threshold = rp.rr_threshold;
+  A.seed = rp.seed;
+
+  static int g_raygen = 0, g_trace_e = 0, g_trace_s = 0, g_shade = 0, g_film = 0;
+  if (!g_raygen) {
+    g_raygen = occupancy_grid(k_raygen, s.device);
+    g_trace_e = occupancy_grid(k_trace_queue<false, false>, s.device);
+    g_trace_s = occupancy_grid(k_trace_queue<true, false>, s.device);
+    g_shade = occupancy_grid(k_shade, s.device);
+    g_film = occupancy_grid(k_film, s.device);
+  }
+  int64_t const npix_total = static_cast<int64_t>(rp.width) * rp.height;
+  int64_t const cap = rp.wave_paths > 0 ? rp.wave_paths : kNoAllocPaths;
+  int const iters = rp.max_depth;
+  if (!rp.accumulate) XYZ_CUDA_TRY(cudaMemsetAsync(film, 0, 3 * npix_total * sizeof(float), st));
+  XYZ_CUDA_TRY(cudaMemsetAsync(tally, 0, kNoAllocTally, st));
+  int64_t const spp_per_wave =
+      std::max<int64_t>(1, std::min<int64_t>(rp.spp, cap / std::max<int64_t>(1, npix_total)));
+  int64_t const pix_per_wave = std::min<int64_t>(npix_total, cap);
+  for (int64_t s0 = 0; s0 < rp.spp; s0 += spp_per_wave) {
+    int const ns = static_cast<int>(std::min<int64_t>(spp_per_wave, rp.spp - s0));
+    for (int64_t p0 = 0; p0 < npix_total; p0 += pix_per_wave) {
+      A.p0 = p0;
+      A.npix = std::min<int64_t>(pix_per_wave, npix_total - p0);
+      A.s0 = static_cast<uint32_t>(rp.spp_offset + s0);
+      A.nsamp = ns;
+      A.npaths = A.npix * ns;
+      // queue lengths and work counters from the previous wave or call
+      XYZ_CUDA_TRY(cudaMemsetAsync(A.counts, 0, kNoAllocCounts, st));
+      int const gr = static_cast<int>(std::min<int64_t>(g_raygen, (A.npaths + kThreads - 1) / kThreads));
+      k_raygen<<<gr, kThreads, 0, st>>>(A);
+      for (int b = 0; b < iters; ++b) {
+        k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, tally + 8);
+        k_shade<<<g_shade, kThreads, 0, st>>>(A, b);
+        k_trace_queue<true, false><<<g_trace_s, kThreads, 0, st>>>(A, b, tally + 8);
+      }
+      int const gf = static_cast<int>(std::min<int64_t>(g_film, (A.npix + kThreads - 1) / kThreads));
+      k_film<<<gf, kThreads, 0, st>>>(A, film);
+      XYZ_CUDA_TRY(cudaGetLastError());
+    }
+  }
   return XYZGPU_OK;
 }
 

@@ -80,6 +80,8 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
                   float *film, cudaStream_t st);
 void render_workspace_free(RenderWorkspace &ws);
 int render_collect(SceneImpl &s);
+int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp,
+                          float *film, cudaStream_t st);
 int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig &cfg,
                     cudaStream_t st);
 int sm_count(int device);
