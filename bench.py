@@ -138,31 +138,35 @@ def cpu_setup(sd):
     return lib, kind, threads, build_s
 
 
-def cpu_rows_for(lib, threads, target_s):
-    """Row band (1 spp) that takes about target_s seconds on `threads` threads."""
-    y0 = H_PIX // 2 - 8
+def cpu_plan(lib, threads, target_s):
+    """(rows, spp): a centre band of rows and a number of samples per pixel
+    that take about target_s seconds on `threads` threads."""
+    y0 = H_PIX // 2 - 32
     t0 = time.perf_counter()
-    lib.render(1, seed=SEED + 7, y0=y0, y1=y0 + 16, nthreads=threads)
+    lib.render(1, seed=SEED + 7, y0=y0, y1=y0 + 64, nthreads=threads)
     dt = max(time.perf_counter() - t0, 1e-3)
-    rows = int(16 * target_s / dt)
-    return max(16, min(H_PIX, rows))
+    rows = int(64 * target_s / dt)
+    if rows <= H_PIX:
+        return max(16, rows), 1
+    spp = int(math.ceil(target_s / (dt * H_PIX / 64)))
+    return H_PIX, max(1, min(SPP, spp))
 
 
-def cpu_sample(lib, threads, rows, s):
+def cpu_sample(lib, threads, rows, spp, s0):
     y0 = max(0, H_PIX // 2 - rows // 2)
     t0 = time.perf_counter()
-    lib.render(1, seed=SEED, s0=s, y0=y0, y1=y0 + rows, nthreads=threads)
+    lib.render(spp, seed=SEED, s0=s0, y0=y0, y1=y0 + rows, nthreads=threads)
     dt = time.perf_counter() - t0
-    return rows * W_PIX / dt / 1e6, dt
+    return rows * W_PIX * spp / dt / 1e6, dt
 
 
 def cpu_baseline(sd, target_s=12.0):
     lib, kind, threads, build_s = cpu_setup(sd)
-    rows = cpu_rows_for(lib, threads, target_s)
-    v, dt = cpu_sample(lib, threads, rows, 0)
+    rows, spp = cpu_plan(lib, threads, target_s)
+    v, dt = cpu_sample(lib, threads, rows, spp, 0)
     return {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"1 spp over {rows} of 1024 rows (centre band) of the same scene and camera, "
-                      f"{rows * W_PIX} paths in {dt:.1f} s; tree build {build_s:.1f} s untimed"}
+            "sample": f"{spp} spp over {rows} of 1024 rows (centre band) of the same scene and "
+                      f"camera, {rows * W_PIX * spp} paths in {dt:.1f} s; tree build {build_s:.1f} s untimed"}
 
 
 def run_reference_arm(args, rank):
@@ -171,16 +175,15 @@ def run_reference_arm(args, rank):
     sd = make_scene()
     lib, kind, threads, build_s = cpu_setup(sd)
     per_step_s = max(2.0, min(15.0, 100.0 / max(1, args.steps + args.warmup)))
-    rows = cpu_rows_for(lib, threads, per_step_s)
+    rows, spp = cpu_plan(lib, threads, per_step_s)
     for w in range(args.warmup):
-        cpu_sample(lib, threads, max(16, rows // 4), 1000 + w)
-    vals, times = [], []
+        cpu_sample(lib, threads, max(16, rows // 4), 1, 1000 + w)
+    times = []
     for k in range(args.steps):
-        v, dt = cpu_sample(lib, threads, rows, k)
-        vals.append(v)
+        _, dt = cpu_sample(lib, threads, rows, spp, k * spp)
         times.append(dt)
     total = sum(times)
-    value = rows * W_PIX * args.steps / total / 1e6
+    value = rows * W_PIX * spp * args.steps / total / 1e6
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * total / args.steps, 3),
@@ -188,8 +191,8 @@ def run_reference_arm(args, rank):
         "data": "synthetic (seeded scene generator)", "config": workload_config(),
         "impl": "reference",
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": f"each step: 1 spp over {rows} of 1024 rows (centre band), "
-                                   f"{rows * W_PIX} paths; tree build {build_s:.1f} s untimed"},
+                         "sample": f"each step: {spp} spp over {rows} of 1024 rows (centre band), "
+                                   f"{rows * W_PIX * spp} paths; tree build {build_s:.1f} s untimed"},
         "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -307,7 +310,15 @@ def run_gpu_arm(args, rank, world):
         "traffic": traffic,
         "algorithmic_bytes_per_ray": round((ext_bytes + sh_bytes) / max(1, rays), 1),
         "per_ray": {"nodes": round((cp["ext_nodes"] + cp["shadow_nodes"]) / max(1, rays), 2),
-                    "tri_tests": round((cp["ext_tri_tests"] + cp["shadow_tri_tests"]) / max(1, rays), 2)},
+                    "tri_tests": round((cp["ext_tri_tests"] + cp["shadow_tri_tests"]) / max(1, rays), 2),
+                    "extension": {"rays": cp["ext_rays"],
+                                  "nodes": round(cp["ext_nodes"] / max(1, cp["ext_rays"]), 2),
+                                  "leaves": round(cp["ext_leaves"] / max(1, cp["ext_rays"]), 2),
+                                  "tri_tests": round(cp["ext_tri_tests"] / max(1, cp["ext_rays"]), 2)},
+                    "shadow": {"rays": cp["shadow_rays"],
+                               "nodes": round(cp["shadow_nodes"] / max(1, cp["shadow_rays"]), 2),
+                               "leaves": round(cp["shadow_leaves"] / max(1, cp["shadow_rays"]), 2),
+                               "tri_tests": round(cp["shadow_tri_tests"] / max(1, cp["shadow_rays"]), 2)}},
         "rays_per_step": rays,
         "trace_ms_per_step": round(trace_ms, 3),
         "kernel_ms_per_step": {c: round(ms_cls[c] / max(1, args.steps), 3) for c in api.KERNEL_CLASSES},
@@ -317,7 +328,7 @@ def run_gpu_arm(args, rank, world):
 
     # end to end through the C ABI with host buffers: upload + build + render + read back
     e2e = None
-    if rank == 0 or world > 1:
+    if not args.no_e2e:
         h2d = sum(int(a.nbytes) for a in (sd.positions, sd.tris, sd.tri_mat, sd.albedo_xyz, sd.is_light))
         if sd.normals is not None:
             h2d += int(sd.normals.nbytes)
@@ -349,7 +360,7 @@ def run_gpu_arm(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene generator)",
             "config": workload_config(stats) | {"parallelism": f"sample-parallel x{world}",
-                                                 "wave_paths": 1 << 22},
+                                                 "waves_per_step": counters["waves"]},
             "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "wall_ms_timed_region": round(wall_ms, 1),
             "render_counters": counters,
@@ -365,6 +376,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["xyz", "reference"], default="xyz")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

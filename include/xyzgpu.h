@@ -76,7 +76,7 @@ typedef struct {
   float cost_intersect;   /* SAH intersection cost (1.5) */
   float empty_bonus;      /* SAH discount for a split with an empty side (0.2) */
   int bins;               /* SAH bins per axis per node (32, max 64) */
-  int builder;            /* XYZGPU_BUILD_HOST (default) or XYZGPU_BUILD_DEVICE */
+  int builder;            /* XYZGPU_BUILD_DEVICE (default) or XYZGPU_BUILD_HOST */
   int max_refs_factor;    /* reference budget = factor * n_triangles (6) */
 } xyzgpu_build_params;
 
@@ -156,7 +156,9 @@ typedef struct {
   uint64_t seed;
   int film_location;       /* XYZGPU_FILM_DEVICE or XYZGPU_FILM_HOST */
   int accumulate;          /* nonzero: add into film; zero: overwrite */
-  int wave_paths;          /* paths in flight per wave; 0 = default (1 << 22) */
+  int wave_paths;          /* paths in flight per wave; 0 = every path of the call,
+                              at most 2^26, bounded by half of the free device memory.
+                              Wave buffers are shared by all scenes of a device. */
   int profile;             /* XYZGPU_PROFILE_*: per-kernel timing or work counters */
 } xyzgpu_render_params;
 

@@ -112,7 +112,7 @@ void xyzgpu_build_params_default(xyzgpu_build_params *bp) {
   bp->cost_intersect = 1.5f;
   bp->empty_bonus = 0.2f;
   bp->bins = 32;
-  bp->builder = XYZGPU_BUILD_HOST;
+  bp->builder = XYZGPU_BUILD_DEVICE;
   bp->max_refs_factor = 6;
 }
 

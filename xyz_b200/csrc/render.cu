@@ -166,9 +166,56 @@ __global__ void __launch_bounds__(kThreads) k_raygen(WaveArgs A) {
 }
 
 // ------------------------------------------------------------------ trace
-// Persistent warps over a device-sized queue.  kShadow: the ray starts at a
-// light point and the vertex's NEE term is added when the closest hit is the
-// vertex's own triangle.
+// Persistent warps with per-lane refill over a device-sized queue
+// (trace_persistent).  kShadow: the ray starts at a light point and the
+// vertex's NEE term is added when the closest hit is the vertex's own triangle.
+struct ExtSink {
+  const float4 *__restrict__ qo;
+  const float4 *__restrict__ qd;
+  float4 *__restrict__ hits;
+  XYZ_DEV void load(int i, f3 &o, f3 &d, float &tmin, float &tmax) const {
+    float4 const a = qo[i], b = qd[i];
+    o = xyz3(a);
+    d = xyz3(b);
+    tmin = a.w;
+    tmax = b.w;
+  }
+  XYZ_DEV void store(int i, const RayHit &h) {
+    int32_t const code = h.id >= 0 ? ((h.id << 1) | h.back) : -1;
+    hits[i] = make_float4(h.t, h.f, h.g, __int_as_float(code));
+  }
+};
+
+struct ShadowSink {
+  const WaveArgs *A;
+  uint32_t visible;
+  XYZ_DEV void load(int i, f3 &o, f3 &d, float &tmin, float &tmax) const {
+    float4 const a = A->s_o[i], b = A->s_d[i];
+    o = xyz3(a);
+    d = xyz3(b);
+    tmin = kRayTMin;
+    tmax = a.w;
+  }
+  XYZ_DEV void store(int i, const RayHit &h) {
+    if (h.id < 0 || h.id != A->s_target[i]) return;
+    // Lambert::CalculateWeightedDirectLighting, lambert.cpp:157-172
+    float const G = A->s_d[i].w / (h.t * h.t);  // nk2 * nk3 / t^2
+    float const dimp = static_cast<float>(kInvPi * static_cast<double>(G));
+    float const dexp = 1.0f / A->S.light_area;
+    float const dens = dimp / dexp;
+    double const wgt = (static_cast<double>(G) * (kInvPi * kInvPi)) *
+                       static_cast<double>(1.0f / (1.0f + dens * dens));
+    float4 const pb = A->s_pb[i];
+    int32_t const slot = __float_as_int(pb.w);
+    float4 L = A->radiance[slot];
+    L.x += static_cast<float>(static_cast<double>(pb.x) * wgt);
+    L.y += static_cast<float>(static_cast<double>(pb.y) * wgt);
+    L.z += static_cast<float>(static_cast<double>(pb.z) * wgt);
+    A->radiance[slot] = L;
+    ++visible;
+  }
+};
+
 template <bool kShadow, bool kCount>
 __global__ void __launch_bounds__(kThreads) k_trace_queue(WaveArgs A, int b,
                                                           unsigned long long *prof) {
@@ -176,45 +223,15 @@ __global__ void __launch_bounds__(kThreads) k_trace_queue(WaveArgs A, int b,
   int const n = kShadow ? cnt[kCShadow] : cnt[kCExt];
   int const lane = threadIdx.x & 31;
   int const qi = b & 1;
-  const float4 *__restrict__ qo = kShadow ? A.s_o : A.q_o[qi];
-  const float4 *__restrict__ qd = kShadow ? A.s_d : A.q_d[qi];
-  uint32_t visible = 0;
   TraceCount tc{0u, 0u, 0u};
-  for (;;) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(&cnt[kShadow ? kCFetchSh : kCFetchExt], 32);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    int const i = base + lane;
-    if (i < n) {
-      float4 const a = qo[i];
-      float4 const dd = qd[i];
-      RayHit h;
-      if (kShadow) {
-        trace_closest<kCount>(A.S, xyz3(a), xyz3(dd), kRayTMin, a.w, h, &tc);
-        if (h.id >= 0 && h.id == A.s_target[i]) {
-          // Lambert::CalculateWeightedDirectLighting, lambert.cpp:157-172
-          float const G = dd.w / (h.t * h.t);  // nk2 * nk3 / t^2
-          float const dimp = static_cast<float>(kInvPi * static_cast<double>(G));
-          float const dexp = 1.0f / A.S.light_area;
-          float const dens = dimp / dexp;
-          double const wgt = (static_cast<double>(G) * (kInvPi * kInvPi)) *
-                             static_cast<double>(1.0f / (1.0f + dens * dens));
-          float4 const pb = A.s_pb[i];
-          int32_t const slot = __float_as_int(pb.w);
-          float4 L = A.radiance[slot];
-          L.x += static_cast<float>(static_cast<double>(pb.x) * wgt);
-          L.y += static_cast<float>(static_cast<double>(pb.y) * wgt);
-          L.z += static_cast<float>(static_cast<double>(pb.z) * wgt);
-          A.radiance[slot] = L;
-          ++visible;
-        }
-      } else {
-        trace_closest<kCount>(A.S, xyz3(a), xyz3(dd), a.w, dd.w, h, &tc);
-        int32_t const code = h.id >= 0 ? ((h.id << 1) | h.back) : -1;
-        A.hits[i] = make_float4(h.t, h.f, h.g, __int_as_float(code));
-      }
-    }
+  uint32_t visible = 0;
+  if (kShadow) {
+    ShadowSink sink{&A, 0u};
+    trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
+    visible = sink.visible;
+  } else {
+    ExtSink sink{A.q_o[qi], A.q_d[qi], A.hits};
+    trace_persistent<kCount>(A.S, n, &cnt[kCFetchExt], sink, tc);
   }
   if (kShadow) {
 #pragma unroll
@@ -492,36 +509,27 @@ int occupancy_grid(K kernel, int device) {
   return per_sm * sm_count(device);
 }
 
-int ensure_workspace(SceneImpl &s, int64_t capacity, int iters) {
-  RenderWorkspace &w = s.ws;
-  if (w.capacity >= capacity && w.max_iters >= iters) return XYZGPU_OK;
-  render_workspace_free(w);
-  size_t const c = static_cast<size_t>(capacity);
-#define XYZ_ALLOC(ptr, bytes) XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&(ptr)), (bytes)))
-  XYZ_ALLOC(w.beta, c * sizeof(float4));
-  XYZ_ALLOC(w.misc, c * sizeof(uint32_t));
-  XYZ_ALLOC(w.radiance, c * sizeof(float4));
-  for (int q = 0; q < 2; ++q) {
-    XYZ_ALLOC(w.q_o[q], c * sizeof(float4));
-    XYZ_ALLOC(w.q_d[q], c * sizeof(float4));
-    XYZ_ALLOC(w.q_slot[q], c * sizeof(int32_t));
-  }
-  XYZ_ALLOC(w.hits, c * sizeof(float4));
-  XYZ_ALLOC(w.s_o, c * sizeof(float4));
-  XYZ_ALLOC(w.s_d, c * sizeof(float4));
-  XYZ_ALLOC(w.s_pb, c * sizeof(float4));
-  XYZ_ALLOC(w.s_target, c * sizeof(int32_t));
-  XYZ_ALLOC(w.counts, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t));
-  XYZ_ALLOC(w.tally, 16 * sizeof(unsigned long long));
-#undef XYZ_ALLOC
-  w.capacity = capacity;
-  w.max_iters = iters;
-  return XYZGPU_OK;
+constexpr int64_t kBytesPerPath = 3 * sizeof(float4) + sizeof(uint32_t) +  // beta, radiance, hits, misc
+                                  2 * (2 * sizeof(float4) + sizeof(int32_t)) +  // extension queues
+                                  3 * sizeof(float4) + sizeof(int32_t);          // shadow queue
+constexpr int64_t kMaxDefaultWave = int64_t{1} << 26;
+
+// Wave buffers are shared by every scene on a device: the largest wave asked
+// for so far stays allocated, and renders on different streams are ordered by
+// an event so that they never use the buffers at the same time.
+struct SharedWaves {
+  std::mutex mu;
+  RenderWorkspace ws;  // only the wave buffers (beta .. counts) are used
+  cudaEvent_t done = nullptr;
+  cudaStream_t last = nullptr;
+};
+
+SharedWaves &shared_waves(int device) {
+  static SharedWaves pool[64];
+  return pool[device & 63];
 }
 
-}  // namespace
-
-void render_workspace_free(RenderWorkspace &w) {
+void free_wave_buffers(RenderWorkspace &w) {
   cudaFree(w.beta);
   cudaFree(w.misc);
   cudaFree(w.radiance);
@@ -536,6 +544,55 @@ void render_workspace_free(RenderWorkspace &w) {
   cudaFree(w.s_pb);
   cudaFree(w.s_target);
   cudaFree(w.counts);
+  w.beta = w.radiance = w.hits = w.s_o = w.s_d = w.s_pb = nullptr;
+  w.misc = nullptr;
+  w.q_o[0] = w.q_o[1] = w.q_d[0] = w.q_d[1] = nullptr;
+  w.q_slot[0] = w.q_slot[1] = w.s_target = w.counts = nullptr;
+  w.capacity = 0;
+  w.max_iters = 0;
+}
+
+int ensure_wave_buffers(RenderWorkspace &w, int64_t capacity, int iters) {
+  if (w.capacity >= capacity && w.max_iters >= iters) return XYZGPU_OK;
+  capacity = std::max(capacity, w.capacity);
+  iters = std::max(iters, w.max_iters);
+  free_wave_buffers(w);
+  size_t const c = static_cast<size_t>(capacity);
+#define XYZ_ALLOC(ptr, bytes)                                                         \
+  do {                                                                                \
+    cudaError_t const e_ = cudaMalloc(reinterpret_cast<void **>(&(ptr)), (bytes));    \
+    if (e_ != cudaSuccess) {                                                          \
+      free_wave_buffers(w);                                                           \
+      return set_error(e_ == cudaErrorMemoryAllocation ? XYZGPU_E_NOMEM : XYZGPU_E_CUDA, \
+                       "render: allocating %zu bytes of wave buffers failed: %s",     \
+                       static_cast<size_t>(bytes), cudaGetErrorString(e_));           \
+    }                                                                                 \
+  } while (0)
+  XYZ_ALLOC(w.beta, c * sizeof(float4));
+  XYZ_ALLOC(w.misc, c * sizeof(uint32_t));
+  XYZ_ALLOC(w.radiance, c * sizeof(float4));
+  for (int q = 0; q < 2; ++q) {
+    XYZ_ALLOC(w.q_o[q], c * sizeof(float4));
+    XYZ_ALLOC(w.q_d[q], c * sizeof(float4));
+    XYZ_ALLOC(w.q_slot[q], c * sizeof(int32_t));
+  }
+  XYZ_ALLOC(w.hits, c * sizeof(float4));
+  XYZ_ALLOC(w.s_o, c * sizeof(float4));
+  XYZ_ALLOC(w.s_d, c * sizeof(float4));
+  XYZ_ALLOC(w.s_pb, c * sizeof(float4));
+  XYZ_ALLOC(w.s_target, c * sizeof(int32_t));
+  XYZ_ALLOC(w.counts, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t));
+#undef XYZ_ALLOC
+  w.capacity = capacity;
+  w.max_iters = iters;
+  return XYZGPU_OK;
+}
+
+}  // namespace
+
+// Frees a scene's own render state (profiling tally and events, host-film
+// staging); the wave buffers belong to the device.
+void render_workspace_free(RenderWorkspace &w) {
   cudaFree(w.tally);
   for (cudaEvent_t e : w.events) cudaEventDestroy(e);
   cudaFree(w.film_dev);
@@ -548,7 +605,6 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   XYZ_CUDA_TRY(cudaSetDevice(s.device));
   int64_t const npix_total = static_cast<int64_t>(rp.width) * rp.height;
   int64_t const film_elems = 3 * npix_total;
-  int64_t const cap = rp.wave_paths > 0 ? rp.wave_paths : (int64_t{1} << 22);
   int const iters = rp.max_depth;
 
   // Camera set-up as ThinLensCamera::Reset (thinlenscamera.cpp:71-90) and
@@ -574,8 +630,26 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
 
   float *film_dev = film;
   RenderWorkspace &w = s.ws;
-  int rc = ensure_workspace(s, cap, iters);
+  if (!w.tally) XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&w.tally), 16 * sizeof(unsigned long long)));
+  SharedWaves &sw = shared_waves(s.device);
+  std::lock_guard<std::mutex> lock(sw.mu);
+  // Wave size: the caller's, else every path of the call (at most 2^26),
+  // bounded by half of the free device memory.
+  int64_t cap = rp.wave_paths;
+  if (cap <= 0) {
+    cap = std::min<int64_t>(kMaxDefaultWave, std::max<int64_t>(1, npix_total * rp.spp));
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      int64_t const afford = static_cast<int64_t>((free_b / 2 + sw.ws.capacity * kBytesPerPath) / kBytesPerPath);
+      cap = std::min(cap, std::max<int64_t>(afford, int64_t{1} << 20));
+    }
+    cap = std::max(cap, sw.ws.capacity);
+  }
+  if (sw.done && sw.last != st) XYZ_CUDA_TRY(cudaStreamWaitEvent(st, sw.done, 0));
+  int rc = ensure_wave_buffers(sw.ws, cap, iters);
   if (rc) return rc;
+  if (!sw.done) XYZ_CUDA_TRY(cudaEventCreateWithFlags(&sw.done, cudaEventDisableTiming));
+  RenderWorkspace const &wv = sw.ws;
   if (rp.film_location == XYZGPU_FILM_HOST) {
     if (w.film_elems < film_elems) {
       cudaFree(w.film_dev);
@@ -634,20 +708,20 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   A.rr_start = rp.rr_start_depth;
   A.rr_threshold = rp.rr_threshold;
   A.seed = rp.seed;
-  A.beta = w.beta;
-  A.misc = w.misc;
-  A.radiance = w.radiance;
+  A.beta = wv.beta;
+  A.misc = wv.misc;
+  A.radiance = wv.radiance;
   for (int q = 0; q < 2; ++q) {
-    A.q_o[q] = w.q_o[q];
-    A.q_d[q] = w.q_d[q];
-    A.q_slot[q] = w.q_slot[q];
+    A.q_o[q] = wv.q_o[q];
+    A.q_d[q] = wv.q_d[q];
+    A.q_slot[q] = wv.q_slot[q];
   }
-  A.hits = w.hits;
-  A.s_o = w.s_o;
-  A.s_d = w.s_d;
-  A.s_pb = w.s_pb;
-  A.s_target = w.s_target;
-  A.counts = w.counts;
+  A.hits = wv.hits;
+  A.s_o = wv.s_o;
+  A.s_d = wv.s_d;
+  A.s_pb = wv.s_pb;
+  A.s_target = wv.s_target;
+  A.counts = wv.counts;
 
   xyzgpu_render_counters rc_out{};
   uint64_t launches = 0;
@@ -662,7 +736,7 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       A.s0 = static_cast<uint32_t>(rp.spp_offset + s0);
       A.nsamp = ns;
       A.npaths = A.npix * ns;
-      XYZ_CUDA_TRY(cudaMemsetAsync(w.counts, 0, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t), st));
+      XYZ_CUDA_TRY(cudaMemsetAsync(wv.counts, 0, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t), st));
       int const gr = static_cast<int>(std::min<int64_t>(g_raygen, (A.npaths + kThreads - 1) / kThreads));
 #define XYZ_MARK(cls, start)              \
   do {                                    \
@@ -703,6 +777,8 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       rc_out.waves += 1;
     }
   }
+  XYZ_CUDA_TRY(cudaEventRecord(sw.done, st));
+  sw.last = st;
   if (rp.film_location == XYZGPU_FILM_HOST) {
     XYZ_CUDA_TRY(cudaMemcpyAsync(w.film_pinned, film_dev, film_elems * sizeof(float), cudaMemcpyDeviceToHost, st));
     XYZ_CUDA_TRY(cudaStreamSynchronize(st));

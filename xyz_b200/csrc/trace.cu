@@ -1,12 +1,10 @@
 // Closest-hit entry point (xyzgpu_trace_closest): the batch form of
 // Scene::FindIntersection (xyz/core/scene.hpp:277-295).
 //
-// Persistent warps: each warp takes 32 consecutive rays from a global counter
-// (one atomicAdd by lane 0, broadcast with a shuffle), traces them to
-// completion and takes the next 32, so long and short rays balance across the
-// SMs without a tail of idle blocks.  Rays are read as two 16-byte vectors and
-// hits written as one, so a warp moves 1 KB of rays and 512 B of hits per
-// batch in full 128-byte lines.
+// Persistent warps with per-lane refill (trace_persistent in traverse.cuh):
+// rays are taken from a global counter as lanes free up, so long and short
+// rays balance across lanes and SMs.  Rays are read as two 16-byte vectors and
+// hits written as one.
 #include "scene.h"
 #include "traverse.cuh"
 
@@ -15,32 +13,36 @@ namespace {
 
 constexpr int kTraceThreads = 128;
 
+// Rays as 8 floats (o, tmin, d, tmax); hits as (t, f, g, id << 1 | back).
+struct ApiSink {
+  const float4 *__restrict__ rays;
+  float4 *__restrict__ hits;
+  uint32_t n_rays, n_hits;
+  XYZ_DEV void load(int i, f3 &o, f3 &d, float &tmin, float &tmax) const {
+    float4 const a = __ldg(&rays[2 * i + 0]);
+    float4 const b = __ldg(&rays[2 * i + 1]);
+    o = xyz3(a);
+    d = xyz3(b);
+    tmin = a.w;
+    tmax = b.w;
+  }
+  XYZ_DEV void store(int i, const RayHit &h) {
+    int32_t const code = h.id >= 0 ? ((h.id << 1) | h.back) : -1;
+    hits[i] = make_float4(h.id >= 0 ? h.t : 0.0f, h.f, h.g, __int_as_float(code));
+    ++n_rays;
+    n_hits += h.id >= 0;
+  }
+};
+
 template <bool kCount>
 __global__ void __launch_bounds__(kTraceThreads)
     k_trace_api(DevScene S, const float4 *__restrict__ rays, int n, float4 *__restrict__ hits,
                 int *__restrict__ fetch, unsigned long long *__restrict__ counts) {
   int const lane = threadIdx.x & 31;
   TraceCount c{0u, 0u, 0u};
-  uint32_t n_rays = 0, n_hits = 0;
-  for (;;) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(fetch, 32);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    int const i = base + lane;
-    if (i < n) {
-      float4 const a = __ldg(&rays[2 * i + 0]);
-      float4 const b = __ldg(&rays[2 * i + 1]);
-      RayHit h;
-      trace_closest<kCount>(S, xyz3(a), xyz3(b), a.w, b.w, h, &c);
-      int32_t const code = h.id >= 0 ? ((h.id << 1) | h.back) : -1;
-      hits[i] = make_float4(h.id >= 0 ? h.t : 0.0f, h.f, h.g, __int_as_float(code));
-      if (kCount) {
-        ++n_rays;
-        n_hits += h.id >= 0;
-      }
-    }
-  }
+  ApiSink sink{rays, hits, 0u, 0u};
+  trace_persistent<kCount>(S, n, fetch, sink, c);
+  uint32_t const n_rays = sink.n_rays, n_hits = sink.n_hits;
   if (kCount) {
     unsigned long long v[5] = {n_rays, c.nodes, c.leaves, c.tris, n_hits};
 #pragma unroll

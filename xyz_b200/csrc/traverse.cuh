@@ -141,4 +141,130 @@ XYZ_DEV void trace_closest(const DevScene &S, f3 o, f3 d, float tmin, float tmax
   }
 }
 
+// Persistent closest-hit loop over rays [0, n) taken from a shared work
+// counter, with per-lane refill: after every leaf visit the lanes whose ray
+// has finished are counted with a ballot, one atomicAdd by the first of them
+// fetches that many new rays, and each takes its index from a popcount of the
+// lanes below it.  A lane therefore never idles while its warp finishes long
+// rays, which keeps the warp's lanes busy on incoherent secondary and shadow
+// rays (the warp-per-batch scheme leaves most lanes waiting for the slowest
+// ray of the batch).  Every lane of the warp must call this.
+//   Sink::load(i, o, d, tmin, tmax)   ray i
+//   Sink::store(i, hit)               result of ray i
+template <bool kCount, class Sink>
+XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, TraceCount &tc) {
+  int const lane = threadIdx.x & 31;
+  unsigned const lanes_below = (1u << lane) - 1u;
+  int ray = -1;
+  bool exhausted = false;
+  f3 o{}, d{};
+  float inv[3] = {0.0f, 0.0f, 0.0f};
+  float tmin = 0.0f;
+  RayHit h{};
+  uint32_t node = 0;
+  float tn = 0.0f, tf = 0.0f;
+  int sp = 0;
+  StackEntry stack[kKdMaxDepthLimit];
+  for (;;) {
+    bool const need = ray < 0 && !exhausted;
+    unsigned const want = __ballot_sync(0xffffffffu, need);
+    if (want) {
+      int const leader = __ffs(want) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(fetch, __popc(want));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        int const i = base + __popc(want & lanes_below);
+        if (i >= n) {
+          exhausted = true;
+        } else {
+          float tmax;
+          sink.load(i, o, d, tmin, tmax);
+          h.t = tmax;
+          h.id = -1;
+          h.f = h.g = 0.0f;
+          h.back = 0;
+          inv[0] = __frcp_rn(d.x);
+          inv[1] = __frcp_rn(d.y);
+          inv[2] = __frcp_rn(d.z);
+          float const org[3] = {o.x, o.y, o.z};
+          float const lo[3] = {S.bmin.x, S.bmin.y, S.bmin.z};
+          float const hi[3] = {S.bmax.x, S.bmax.y, S.bmax.z};
+          float t0 = tmin, t1 = tmax;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            float const ta = (lo[k] - org[k]) * inv[k];
+            float const tb = (hi[k] - org[k]) * inv[k];
+            t0 = fmaxf(t0, fminf(ta, tb));
+            t1 = fminf(t1, fmaxf(ta, tb));
+          }
+          if (!(t0 <= t1)) {
+            sink.store(i, h);  // misses the scene box
+          } else {
+            ray = i;
+            node = 0;
+            tn = t0;
+            tf = t1;
+            sp = 0;
+          }
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, exhausted && ray < 0)) break;
+    if (ray < 0) continue;
+    // descend to a leaf
+    uint2 nd = __ldg(&S.nodes[node]);
+    if (kCount) tc.nodes++;
+    while ((nd.y & 3u) != kKdLeafTag) {
+      uint32_t const ax = nd.y & 3u;
+      float const split = __uint_as_float(nd.x);
+      uint32_t const child = nd.y >> 2;
+      float const oa = ax == 0 ? o.x : (ax == 1 ? o.y : o.z);
+      float const ia = ax == 0 ? inv[0] : (ax == 1 ? inv[1] : inv[2]);
+      float const da = ax == 0 ? d.x : (ax == 1 ? d.y : d.z);
+      float const tp = (split - oa) * ia;
+      uint32_t const above_first = (oa < split || (oa == split && da <= 0.0f)) ? 0u : 1u;
+      uint32_t const first = child + above_first;
+      uint32_t const second = child + (above_first ^ 1u);
+      if ((tp > tf) || (tp <= 0.0f)) {
+        node = first;
+      } else if (tp < tn) {
+        node = second;
+      } else {
+        stack[sp].node = second;
+        stack[sp].tn = tp;
+        stack[sp].tf = tf;
+        ++sp;
+        node = first;
+        tf = tp;
+      }
+      nd = __ldg(&S.nodes[node]);
+      if (kCount) tc.nodes++;
+    }
+    // test the leaf
+    uint32_t const cnt = nd.y >> 2;
+    if (kCount) {
+      tc.leaves++;
+      tc.tris += cnt;
+    }
+    for (uint32_t j = 0; j < cnt; ++j) {
+      int32_t const t = __ldg(&S.refs[nd.x + j]);
+      hit_triangle(S.tri, t, o, d, tmin, h);
+    }
+    // next leaf, or done
+    bool done = (h.id >= 0 && h.t <= tf) || sp == 0;
+    if (!done) {
+      --sp;
+      node = stack[sp].node;
+      tn = stack[sp].tn;
+      tf = stack[sp].tf;
+      done = h.id >= 0 && h.t < tn;
+    }
+    if (done) {
+      sink.store(ray, h);
+      ray = -1;
+    }
+  }
+}
+
 }  // namespace xyzgpu
