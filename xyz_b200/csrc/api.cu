@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "scene.h"
@@ -41,13 +42,36 @@ int sm_count(int device) {
 
 namespace {
 
+// Scene and builder memory comes from the device's stream-ordered pool, which
+// keeps freed blocks for reuse: building and destroying scenes repeatedly
+// (batches, end-to-end loops) then costs no driver allocation or device-wide
+// synchronisation after the first time.
+void configure_pool(int device) {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0 || device >= 64 || done[device]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = ~uint64_t{0};
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done[device] = true;
+}
+
 template <class T>
-int dev_upload(T **dst, const std::vector<T> &src, int64_t *bytes) {
-  size_t const n = src.empty() ? 1 : src.size();
-  XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(dst), n * sizeof(T)));
-  if (!src.empty())
-    XYZ_CUDA_TRY(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+int dev_alloc(T **dst, size_t n, int64_t *bytes, cudaStream_t st) {
+  n = n ? n : 1;
+  XYZ_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(dst), n * sizeof(T), st));
   *bytes += static_cast<int64_t>(n * sizeof(T));
+  return XYZGPU_OK;
+}
+
+template <class T>
+int dev_upload(T **dst, const T *src, size_t n, int64_t *bytes, cudaStream_t st) {
+  int const rc = dev_alloc(dst, n, bytes, st);
+  if (rc) return rc;
+  if (n) XYZ_CUDA_TRY(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
   return XYZGPU_OK;
 }
 
@@ -56,19 +80,81 @@ void free_scene(SceneImpl *s) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(s->device);
+  // work queued on any stream that still reads the scene finishes first
+  cudaDeviceSynchronize();
   render_workspace_free(s->ws);
-  cudaFree(s->d_tri);
-  cudaFree(s->d_ng);
-  cudaFree(s->d_sn);
-  cudaFree(s->d_mat);
-  cudaFree(s->d_lights);
-  cudaFree(s->d_cdf);
-  cudaFree(s->d_nodes);
-  cudaFree(s->d_refs);
-  cudaFree(s->d_fetch);
-  cudaFree(s->d_trace_counts);
+  void *bufs[] = {s->d_tri, s->d_ng, s->d_sn, s->d_mat, s->d_lights, s->d_cdf,
+                  s->d_nodes, s->d_refs, s->d_fetch, s->d_trace_counts};
+  for (void *b : bufs)
+    if (b) cudaFreeAsync(b, nullptr);
+  cudaStreamSynchronize(nullptr);
   cudaSetDevice(prev);
   delete s;
+}
+
+// Triangle records from the uploaded vertex and index arrays (the Triangle
+// constructor, xyz/geom/triangle.cpp:35-60): v0, e1 = v1 - v0, e2 = v2 - v0,
+// n = cross(e2, e1), ng = n / |n|, shading normals n0, s1 = n1 - n0,
+// s2 = n2 - n0.  Same float operations as the host (--fmad=false).
+__global__ void k_prepare_triangles(const float *__restrict__ pos, const float *__restrict__ nrm,
+                                    const int32_t *__restrict__ idx, const int32_t *__restrict__ tmat,
+                                    int nt, float4 *__restrict__ tri, float4 *__restrict__ ng,
+                                    float4 *__restrict__ sn, float *__restrict__ box_min,
+                                    float *__restrict__ box_max) {
+  int const i = blockIdx.x * blockDim.x + threadIdx.x;
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  if (i < nt) {
+    int const a = idx[3 * i], b = idx[3 * i + 1], c = idx[3 * i + 2];
+    f3 const p0 = mk3(pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]);
+    f3 const p1 = mk3(pos[3 * b], pos[3 * b + 1], pos[3 * b + 2]);
+    f3 const p2 = mk3(pos[3 * c], pos[3 * c + 1], pos[3 * c + 2]);
+    f3 const e1 = sub3(p1, p0), e2 = sub3(p2, p0);
+    f3 const n = cross3(e2, e1);
+    float const r = 1.0f / sqrtf(dot3(n, n));
+    tri[3 * i + 0] = make_float4(p0.x, p0.y, p0.z, n.x);
+    tri[3 * i + 1] = make_float4(e1.x, e1.y, e1.z, n.y);
+    tri[3 * i + 2] = make_float4(e2.x, e2.y, e2.z, n.z);
+    ng[i] = make_float4(n.x * r, n.y * r, n.z * r, __int_as_float(tmat[i]));
+    if (sn) {
+      f3 const n0 = mk3(nrm[3 * a], nrm[3 * a + 1], nrm[3 * a + 2]);
+      f3 const n1 = mk3(nrm[3 * b], nrm[3 * b + 1], nrm[3 * b + 2]);
+      f3 const n2 = mk3(nrm[3 * c], nrm[3 * c + 1], nrm[3 * c + 2]);
+      f3 const s1 = sub3(n1, n0), s2 = sub3(n2, n0);
+      sn[3 * i + 0] = make_float4(n0.x, n0.y, n0.z, 0.0f);
+      sn[3 * i + 1] = make_float4(s1.x, s1.y, s1.z, 0.0f);
+      sn[3 * i + 2] = make_float4(s2.x, s2.y, s2.z, 0.0f);
+    }
+    // the vertices as the intersection test sees them: v0, v0 + e1, v0 + e2
+    f3 const q1 = add3(p0, e1), q2 = add3(p0, e2);
+    float const v[3][3] = {{p0.x, p0.y, p0.z}, {q1.x, q1.y, q1.z}, {q2.x, q2.y, q2.z}};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = fminf(fminf(v[0][k], v[1][k]), v[2][k]);
+      hi[k] = fmaxf(fmaxf(v[0][k], v[1][k]), v[2][k]);
+    }
+  }
+  // scene bounds: block reduction, then one ordered-integer atomic per block
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float l = lo[k], h = hi[k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      l = fminf(l, __shfl_xor_sync(0xffffffffu, l, off));
+      h = fmaxf(h, __shfl_xor_sync(0xffffffffu, h, off));
+    }
+    if ((threadIdx.x & 31) == 0 && l <= h) {
+      // IEEE order = signed-integer order for non-negative floats, reversed for negative
+      int const li = __float_as_int(l), hv = __float_as_int(h);
+      if (li >= 0)
+        atomicMin(reinterpret_cast<int *>(&box_min[k]), li);
+      else
+        atomicMax(reinterpret_cast<unsigned *>(&box_min[k]), static_cast<unsigned>(li));
+      if (hv >= 0)
+        atomicMax(reinterpret_cast<int *>(&box_max[k]), hv);
+      else
+        atomicMin(reinterpret_cast<unsigned *>(&box_max[k]), static_cast<unsigned>(hv));
+    }
+  }
 }
 
 int check_device(int *dev) {
@@ -169,13 +255,10 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
     if (!std::isfinite(d->positions[i]))
       return set_error(XYZGPU_E_INVALID, "scene_create: vertex coordinate %lld is not finite",
                        static_cast<long long>(i));
-  std::vector<float4> tri(3 * static_cast<size_t>(nt)), ng(nt), sn;
   std::vector<float4> mat(nm > 0 ? nm : 1);
-  std::vector<float> trv(9 * static_cast<size_t>(nt));
   std::vector<int32_t> lights;
   std::vector<float> cdf(1, 0.0f);
   bool const smooth = d->normals != nullptr;
-  if (smooth) sn.resize(3 * static_cast<size_t>(nt));
   for (int m = 0; m < nm; ++m) {
     mat[m] = make_float4(d->albedo_xyz[3 * m], d->albedo_xyz[3 * m + 1], d->albedo_xyz[3 * m + 2],
                          d->is_light[m] ? 1.0f : 0.0f);
@@ -187,37 +270,13 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
       return set_error(XYZGPU_E_INVALID, "scene_create: triangle %d has a vertex index out of range", i);
     if (m < 0 || m >= nm)
       return set_error(XYZGPU_E_INVALID, "scene_create: triangle %d has material %d out of range", i, m);
-    f3 const p0 = mk3(d->positions[3 * a], d->positions[3 * a + 1], d->positions[3 * a + 2]);
-    f3 const p1 = mk3(d->positions[3 * b], d->positions[3 * b + 1], d->positions[3 * b + 2]);
-    f3 const p2 = mk3(d->positions[3 * c], d->positions[3 * c + 1], d->positions[3 * c + 2]);
-    // Triangle constructor (xyz/geom/triangle.cpp:35-60)
-    f3 const e1 = sub3(p1, p0), e2 = sub3(p2, p0);
-    f3 const n = cross3(e2, e1);
-    float const r = 1.0f / std::sqrt(dot3(n, n));
-    f3 const g = scl3(n, r);
-    tri[3 * i + 0] = make_float4(p0.x, p0.y, p0.z, n.x);
-    tri[3 * i + 1] = make_float4(e1.x, e1.y, e1.z, n.y);
-    tri[3 * i + 2] = make_float4(e2.x, e2.y, e2.z, n.z);
-    int32_t mbits = m;
-    float mf;
-    std::memcpy(&mf, &mbits, 4);
-    ng[i] = make_float4(g.x, g.y, g.z, mf);
-    f3 const q1 = add3(p0, e1), q2 = add3(p0, e2);
-    float *tv = &trv[9 * static_cast<size_t>(i)];
-    tv[0] = p0.x, tv[1] = p0.y, tv[2] = p0.z;
-    tv[3] = q1.x, tv[4] = q1.y, tv[5] = q1.z;
-    tv[6] = q2.x, tv[7] = q2.y, tv[8] = q2.z;
-    if (smooth) {
-      f3 const n0 = mk3(d->normals[3 * a], d->normals[3 * a + 1], d->normals[3 * a + 2]);
-      f3 const n1 = mk3(d->normals[3 * b], d->normals[3 * b + 1], d->normals[3 * b + 2]);
-      f3 const n2 = mk3(d->normals[3 * c], d->normals[3 * c + 1], d->normals[3 * c + 2]);
-      f3 const s1 = sub3(n1, n0), s2 = sub3(n2, n0);
-      sn[3 * i + 0] = make_float4(n0.x, n0.y, n0.z, 0.0f);
-      sn[3 * i + 1] = make_float4(s1.x, s1.y, s1.z, 0.0f);
-      sn[3 * i + 2] = make_float4(s2.x, s2.y, s2.z, 0.0f);
-    }
     if (d->is_light[m]) {
-      // light CDF in triangle order (xyz/core/scene_mqo.cpp:512-519)
+      // light CDF in triangle order (xyz/core/scene_mqo.cpp:512-519), with the
+      // area of Triangle::area (xyz/geom/triangle.hpp:57-59)
+      f3 const p0 = mk3(d->positions[3 * a], d->positions[3 * a + 1], d->positions[3 * a + 2]);
+      f3 const p1 = mk3(d->positions[3 * b], d->positions[3 * b + 1], d->positions[3 * b + 2]);
+      f3 const p2 = mk3(d->positions[3 * c], d->positions[3 * c + 1], d->positions[3 * c + 2]);
+      f3 const n = cross3(sub3(p2, p0), sub3(p1, p0));
       float const area = std::sqrt(dot3(n, n)) * 0.5f;
       lights.push_back(i);
       cdf.push_back(cdf.back() + area);
@@ -231,27 +290,69 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   s->n_lights = static_cast<int>(lights.size());
   s->n_materials = nm;
   s->smooth = smooth;
-  int64_t bytes = 0;
-#define XYZ_TRY_UP(dst, src)                 \
-  do {                                       \
-    int const r_ = dev_upload(dst, src, &bytes); \
-    if (r_) {                                \
-      free_scene(s);                         \
-      return r_;                             \
-    }                                        \
-  } while (0)
-  XYZ_TRY_UP(&s->d_tri, tri);
-  XYZ_TRY_UP(&s->d_ng, ng);
-  if (smooth) XYZ_TRY_UP(&s->d_sn, sn);
-  XYZ_TRY_UP(&s->d_mat, mat);
-  XYZ_TRY_UP(&s->d_lights, lights);
-  XYZ_TRY_UP(&s->d_cdf, cdf);
-#undef XYZ_TRY_UP
-  if (cudaMalloc(&s->d_fetch, 64 * sizeof(int32_t)) != cudaSuccess ||
-      cudaMalloc(&s->d_trace_counts, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+  configure_pool(dev);
+  cudaStream_t const st = nullptr;
+  int64_t bytes = 0, scratch = 0;
+  float *d_pos = nullptr, *d_nrm = nullptr, *d_box = nullptr;
+  int32_t *d_idx = nullptr, *d_tmat = nullptr;
+  auto fail = [&](int r) {
+    cudaFreeAsync(d_pos, st);
+    cudaFreeAsync(d_nrm, st);
+    cudaFreeAsync(d_idx, st);
+    cudaFreeAsync(d_tmat, st);
+    cudaFreeAsync(d_box, st);
     free_scene(s);
-    return set_error(XYZGPU_E_NOMEM, "scene_create: device allocation failed");
+    return r;
+  };
+#define XYZ_TRY(expr)      \
+  do {                     \
+    int const r_ = (expr); \
+    if (r_) return fail(r_); \
+  } while (0)
+  XYZ_TRY(dev_upload(&d_pos, d->positions, 3 * static_cast<size_t>(nv), &scratch, st));
+  if (smooth) XYZ_TRY(dev_upload(&d_nrm, d->normals, 3 * static_cast<size_t>(nv), &scratch, st));
+  XYZ_TRY(dev_upload(&d_idx, d->triangles, 3 * static_cast<size_t>(nt), &scratch, st));
+  XYZ_TRY(dev_upload(&d_tmat, d->tri_material, static_cast<size_t>(nt), &scratch, st));
+  XYZ_TRY(dev_alloc(&s->d_tri, 3 * static_cast<size_t>(nt), &bytes, st));
+  XYZ_TRY(dev_alloc(&s->d_ng, static_cast<size_t>(nt), &bytes, st));
+  if (smooth) XYZ_TRY(dev_alloc(&s->d_sn, 3 * static_cast<size_t>(nt), &bytes, st));
+  XYZ_TRY(dev_upload(&s->d_mat, mat.data(), mat.size(), &bytes, st));
+  XYZ_TRY(dev_upload(&s->d_lights, lights.data(), lights.size(), &bytes, st));
+  XYZ_TRY(dev_upload(&s->d_cdf, cdf.data(), cdf.size(), &bytes, st));
+  XYZ_TRY(dev_alloc(&s->d_fetch, 64, &bytes, st));
+  XYZ_TRY(dev_alloc(&s->d_trace_counts, 8, &bytes, st));
+  XYZ_TRY(dev_alloc(&d_box, 6, &scratch, st));
+  float const box_init[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  if (cudaMemcpyAsync(d_box, box_init, sizeof(box_init), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return fail(set_error(XYZGPU_E_CUDA, "scene_create: copy failed"));
+  if (nt > 0) {
+    k_prepare_triangles<<<(nt + 255) / 256, 256, 0, st>>>(d_pos, d_nrm, d_idx, d_tmat, nt, s->d_tri, s->d_ng,
+                                                           s->d_sn, d_box, d_box + 3);
+    cudaError_t const e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(set_error(XYZGPU_E_CUDA, "scene_create: %s", cudaGetErrorString(e)));
   }
+  float box[6];
+  if (cudaMemcpyAsync(box, d_box, sizeof(box), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return fail(set_error(XYZGPU_E_CUDA, "scene_create: triangle preparation failed"));
+  cudaFreeAsync(d_pos, st);
+  cudaFreeAsync(d_nrm, st);
+  cudaFreeAsync(d_idx, st);
+  cudaFreeAsync(d_tmat, st);
+  cudaFreeAsync(d_box, st);
+  d_pos = d_nrm = d_box = nullptr;
+  d_idx = d_tmat = nullptr;
+#undef XYZ_TRY
+  // root box: the bounds grown by 1e-5 of the extent plus 1e-6 (kd_root_bounds)
+  for (int k = 0; k < 3; ++k) {
+    float lo = box[k], hi = box[3 + k];
+    if (nt == 0) lo = hi = 0.0f;
+    float const pad = (hi - lo) * 1e-5f + 1e-6f;
+    box[k] = lo - pad;
+    box[3 + k] = hi + pad;
+  }
+  s->dev.bmin = mk3(box[0], box[1], box[2]);
+  s->dev.bmax = mk3(box[3], box[4], box[5]);
 
   BuildConfig cfg;
   cfg.leaf_max_tris = bp.leaf_max_tris;
@@ -263,6 +364,21 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   cfg.max_refs = static_cast<int64_t>(bp.max_refs_factor) * nt + 1024;
   auto const t0 = std::chrono::steady_clock::now();
   if (bp.builder == XYZGPU_BUILD_HOST) {
+    // the host builder reads the triangles' vertices back from the device
+    std::vector<float4> tri(3 * static_cast<size_t>(nt));
+    if (nt && cudaMemcpy(tri.data(), s->d_tri, tri.size() * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      free_scene(s);
+      return set_error(XYZGPU_E_CUDA, "scene_create: reading triangles back failed");
+    }
+    std::vector<float> trv(9 * static_cast<size_t>(nt));
+    for (int i = 0; i < nt; ++i) {
+      f3 const p0 = xyz3(tri[3 * i]), e1 = xyz3(tri[3 * i + 1]), e2 = xyz3(tri[3 * i + 2]);
+      f3 const q1 = add3(p0, e1), q2 = add3(p0, e2);
+      float *tv = &trv[9 * static_cast<size_t>(i)];
+      tv[0] = p0.x, tv[1] = p0.y, tv[2] = p0.z;
+      tv[3] = q1.x, tv[4] = q1.y, tv[5] = q1.z;
+      tv[6] = q2.x, tv[7] = q2.y, tv[8] = q2.z;
+    }
     KdTreeHost tree;
     std::string err;
     if (!kd_build_host(trv.data(), nt, cfg, &tree, &err)) {
@@ -276,20 +392,14 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
     s->depth = tree.depth;
     std::vector<uint2> nodes(s->n_nodes);
     for (int64_t j = 0; j < s->n_nodes; ++j) nodes[j] = make_uint2(tree.nodes[2 * j], tree.nodes[2 * j + 1]);
-    int r2 = dev_upload(&s->d_nodes, nodes, &bytes);
-    if (!r2) r2 = dev_upload(&s->d_refs, tree.refs, &bytes);
+    int r2 = dev_upload(&s->d_nodes, nodes.data(), nodes.size(), &bytes, st);
+    if (!r2) r2 = dev_upload(&s->d_refs, tree.refs.data(), tree.refs.size(), &bytes, st);
     if (r2) {
       free_scene(s);
       return r2;
     }
-    s->dev.bmin = mk3(tree.bmin[0], tree.bmin[1], tree.bmin[2]);
-    s->dev.bmax = mk3(tree.bmax[0], tree.bmax[1], tree.bmax[2]);
   } else if (bp.builder == XYZGPU_BUILD_DEVICE) {
-    float bmin[3], bmax[3];
-    kd_root_bounds(trv.data(), nt, bmin, bmax);
-    s->dev.bmin = mk3(bmin[0], bmin[1], bmin[2]);
-    s->dev.bmax = mk3(bmax[0], bmax[1], bmax[2]);
-    int r2 = kd_build_device(*s, s->d_tri, nt, cfg, nullptr);
+    int r2 = kd_build_device(*s, s->d_tri, nt, cfg, st);
     if (r2) {
       free_scene(s);
       return r2;
@@ -316,7 +426,7 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   v.n_lights = cdf.back() > 0.0f ? s->n_lights : 0;
   v.light_area = cdf.back();
   v.power = mk3(d->light_power_xyz[0], d->light_power_xyz[1], d->light_power_xyz[2]);
-  cudaError_t const e = cudaDeviceSynchronize();
+  cudaError_t const e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     free_scene(s);
     return set_error(XYZGPU_E_CUDA, "scene_create: %s", cudaGetErrorString(e));

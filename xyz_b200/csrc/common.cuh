@@ -42,7 +42,7 @@ XYZ_DEV f3 normalize3(f3 a) {
   float const r = 1.0f / sqrtf(dot3(a, a));
   return scl3(a, r);
 }
-XYZ_DEV f3 xyz3(float4 v) { return f3{v.x, v.y, v.z}; }
+XYZ_HD f3 xyz3(float4 v) { return f3{v.x, v.y, v.z}; }
 
 // ---------------------------------------------------------------- random
 // Philox4x32-10 (Salmon et al., SC'11).  Stream layout in include/xyzgpu.h.

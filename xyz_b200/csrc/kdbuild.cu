@@ -574,26 +574,30 @@ __global__ void __launch_bounds__(kBigThreads)
 }
 
 // ---- device buffers
+// Device buffer from the stream-ordered pool (the scene's build stream).
 template <class T>
 struct DevBuf {
   T *p = nullptr;
   int64_t cap = 0;
-  ~DevBuf() { cudaFree(p); }
+  cudaStream_t st = nullptr;
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
   // Grows to at least n elements, keeping the first `keep` elements.
   cudaError_t reserve(int64_t n, int64_t keep = 0) {
     if (n <= cap) return cudaSuccess;
     int64_t const nc = std::max<int64_t>(n, cap + cap / 2);
     T *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, nc * sizeof(T));
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&q), nc * sizeof(T), st);
     if (e != cudaSuccess) return e;
     if (keep > 0 && p) {
-      e = cudaMemcpy(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice);
+      e = cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, st);
       if (e != cudaSuccess) {
-        cudaFree(q);
+        cudaFreeAsync(q, st);
         return e;
       }
     }
-    cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = q;
     cap = nc;
     return cudaSuccess;
@@ -683,6 +687,18 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
   DevBuf<int32_t> leaf_refs;
   DevBuf<int32_t> big_list, small_i32;
   DevBuf<uint4> block_sums, grand;
+  for (int q = 0; q < 2; ++q) {
+    refs[q].tri.st = st;
+    for (auto &c : refs[q].c) c.st = st;
+    for (auto *b : {&lv[q].begin, &lv[q].count, &lv[q].axis, &lv[q].nl, &lv[q].nr}) b->st = st;
+    lv[q].blo.st = lv[q].bhi.st = st;
+    lv[q].plane.st = st;
+    lv[q].scan.st = st;
+  }
+  nodes.st = st;
+  leaf_refs.st = st;
+  big_list.st = small_i32.st = st;
+  block_sums.st = grand.st = st;
   XYZ_BUILD_TRY(refs[0].reserve(std::max(1, n)));
   XYZ_BUILD_TRY(lv[0].reserve(1));
   XYZ_BUILD_TRY(nodes.reserve(std::max<int64_t>(64, 2 * static_cast<int64_t>(n) / std::max(1, cfg.leaf_max_tris))));
