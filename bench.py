@@ -238,13 +238,13 @@ def run_gpu_arm(args, rank, world):
     cam = sd.camera
     film = torch.zeros((H_PIX, W_PIX, 3), dtype=torch.float32, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    offset = rank * SPP
+    from xyz_b200.distributed import render_and_reduce, weak_range
+    offset, _ = weak_range(SPP, rank)
 
     def step(s_off, profile=0):
-        scene.render(cam, W_PIX, H_PIX, SPP, seed=SEED, spp_offset=s_off, max_depth=MAX_DEPTH,
-                     film=film, profile=profile)
-        if dist is not None:
-            dist.reduce(film, dst=0)
+        render_and_reduce(lambda first, count: scene.render(
+            cam, W_PIX, H_PIX, count, seed=SEED, spp_offset=first, max_depth=MAX_DEPTH,
+            film=film, profile=profile), s_off, SPP)
         flush.zero_()
 
     for _ in range(args.warmup):

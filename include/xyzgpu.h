@@ -189,11 +189,15 @@ int xyzgpu_render_counters_get(xyzgpu_scene scene, xyzgpu_render_counters *out);
  * 3 shadow trace, 4 film.  ms: summed CUDA-event time (TIMING); the traversal
  * counters are filled by a COUNTERS render. */
 #define XYZGPU_KERNEL_CLASSES 5
+#define XYZGPU_PROFILE_MAX_ITERS 64
 typedef struct {
   uint64_t launches[XYZGPU_KERNEL_CLASSES];
   double ms[XYZGPU_KERNEL_CLASSES];
   uint64_t ext_rays, ext_nodes, ext_leaves, ext_tri_tests;
   uint64_t shadow_rays, shadow_nodes, shadow_leaves, shadow_tri_tests, shadow_visible;
+  uint32_t iterations;          /* bounce iterations per wave (max_depth) */
+  uint64_t ext_rays_by_iter[XYZGPU_PROFILE_MAX_ITERS];     /* summed over waves */
+  uint64_t shadow_rays_by_iter[XYZGPU_PROFILE_MAX_ITERS];
 } xyzgpu_render_profile;
 
 int xyzgpu_render_profile_get(xyzgpu_scene scene, xyzgpu_render_profile *out);

@@ -82,7 +82,9 @@ class RenderProfile(C.Structure):
     _fields_ = [("launches", C.c_uint64 * 5), ("ms", C.c_double * 5), ("ext_rays", C.c_uint64),
                 ("ext_nodes", C.c_uint64), ("ext_leaves", C.c_uint64), ("ext_tri_tests", C.c_uint64),
                 ("shadow_rays", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_leaves", C.c_uint64),
-                ("shadow_tri_tests", C.c_uint64), ("shadow_visible", C.c_uint64)]
+                ("shadow_tri_tests", C.c_uint64), ("shadow_visible", C.c_uint64),
+                ("iterations", C.c_uint32), ("ext_rays_by_iter", C.c_uint64 * 64),
+                ("shadow_rays_by_iter", C.c_uint64 * 64)]
 
 
 KERNEL_CLASSES = ["raygen", "trace_extension", "shade", "trace_shadow", "film"]
@@ -319,7 +321,10 @@ class Scene:
     def render_profile(self) -> dict:
         p = RenderProfile()
         _check(_LIB.xyzgpu_render_profile_get(self.handle, C.byref(p)))
-        out = {f: getattr(p, f) for f, _ in RenderProfile._fields_ if f not in ("launches", "ms")}
+        skip = ("launches", "ms", "ext_rays_by_iter", "shadow_rays_by_iter")
+        out = {f: getattr(p, f) for f, _ in RenderProfile._fields_ if f not in skip}
+        out["ext_rays_by_iter"] = list(p.ext_rays_by_iter)[: p.iterations]
+        out["shadow_rays_by_iter"] = list(p.shadow_rays_by_iter)[: p.iterations]
         out["launches"] = dict(zip(KERNEL_CLASSES, list(p.launches)))
         out["ms"] = dict(zip(KERNEL_CLASSES, list(p.ms)))
         return out

@@ -251,13 +251,22 @@ __global__ void __launch_bounds__(kThreads) k_trace_queue(WaveArgs A, int b,
 }
 
 // Adds the wave's queue lengths to the render's running totals.
+constexpr int kTallyIterBase = 16;
+constexpr int kTallyWords = kTallyIterBase + 2 * XYZGPU_PROFILE_MAX_ITERS;
+
 __global__ void k_tally(WaveArgs A, int iters, unsigned long long *tally) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   unsigned long long e = 0, sh = 0, vis = 0;
   for (int b = 0; b < iters; ++b) {
-    e += A.counts[b * kCountStride + kCExt];
-    sh += A.counts[b * kCountStride + kCShadow];
+    unsigned long long const eb = A.counts[b * kCountStride + kCExt];
+    unsigned long long const sb = A.counts[b * kCountStride + kCShadow];
+    e += eb;
+    sh += sb;
     vis += A.counts[b * kCountStride + kCVisible];
+    if (b < XYZGPU_PROFILE_MAX_ITERS) {
+      tally[kTallyIterBase + b] += eb;
+      tally[kTallyIterBase + XYZGPU_PROFILE_MAX_ITERS + b] += sb;
+    }
   }
   tally[0] += e;
   tally[1] += sh;
@@ -630,7 +639,7 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
 
   float *film_dev = film;
   RenderWorkspace &w = s.ws;
-  if (!w.tally) XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&w.tally), 16 * sizeof(unsigned long long)));
+  if (!w.tally) XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&w.tally), kTallyWords * sizeof(unsigned long long)));
   SharedWaves &sw = shared_waves(s.device);
   std::lock_guard<std::mutex> lock(sw.mu);
   // Wave size: the caller's, else every path of the call (at most 2^26),
@@ -681,7 +690,8 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   int const prof = rp.profile;
   bool const timing = prof == XYZGPU_PROFILE_TIMING;
   bool const counting = prof == XYZGPU_PROFILE_COUNTERS;
-  XYZ_CUDA_TRY(cudaMemsetAsync(w.tally, 0, 16 * sizeof(unsigned long long), st));
+  XYZ_CUDA_TRY(cudaMemsetAsync(w.tally, 0, kTallyWords * sizeof(unsigned long long), st));
+  w.profile_iters = iters;
   s.event_class.clear();
   size_t n_ev = 0;
   // Records the start or end event of a launch of `cls` (TIMING renders).
@@ -797,7 +807,7 @@ int render_collect(SceneImpl &s) {
   XYZ_CUDA_TRY(cudaSetDevice(s.device));
   RenderWorkspace &w = s.ws;
   XYZ_CUDA_TRY(cudaDeviceSynchronize());
-  unsigned long long t[16];
+  unsigned long long t[kTallyWords];
   XYZ_CUDA_TRY(cudaMemcpy(t, w.tally, sizeof(t), cudaMemcpyDeviceToHost));
   s.counters.extension_rays = t[0];
   s.counters.shadow_rays = t[1];
@@ -808,6 +818,11 @@ int render_collect(SceneImpl &s) {
     p.ext_rays = t[0];
     p.shadow_rays = t[1];
     p.shadow_visible = t[2];
+    p.iterations = static_cast<uint32_t>(std::min(w.profile_iters, XYZGPU_PROFILE_MAX_ITERS));
+    for (int b = 0; b < XYZGPU_PROFILE_MAX_ITERS; ++b) {
+      p.ext_rays_by_iter[b] = t[kTallyIterBase + b];
+      p.shadow_rays_by_iter[b] = t[kTallyIterBase + XYZGPU_PROFILE_MAX_ITERS + b];
+    }
     if (s.profile_mode == XYZGPU_PROFILE_COUNTERS) {
       p.ext_nodes = t[8];
       p.ext_leaves = t[9];

@@ -40,8 +40,10 @@ struct RenderWorkspace {
   float4 *s_o = nullptr, *s_d = nullptr, *s_pb = nullptr;
   int32_t *s_target = nullptr;
   int32_t *counts = nullptr;  // per iteration counters (see render.cu)
-  unsigned long long *tally = nullptr;  // [0] ext rays [1] shadow rays [2] visible, then
-                                        // [8..] traversal counters of COUNTERS renders
+  unsigned long long *tally = nullptr;  // [0] ext rays [1] shadow rays [2] visible,
+                                        // [8..13] traversal counters of COUNTERS renders,
+                                        // [16..] extension / shadow rays per iteration
+  int profile_iters = 0;
   std::vector<cudaEvent_t> events;      // timing pairs of TIMING renders
   float *film_dev = nullptr;  // staging film for host-film renders
   float *film_pinned = nullptr;
