@@ -64,6 +64,11 @@ typedef struct {
   const int32_t *is_light;      /* n_materials flags */
   int n_materials;
   float light_power_xyz[3];     /* Phi shared by all light triangles */
+  /* Spectral data for the spectral film modes (else NULL / unused):
+   * 31 albedo bins per material at 400, 410, ..., 700 nm and the light's
+   * power spectrum (the reference's basic_spectrum, libhi/hi/image/spectrum.hpp:14). */
+  const float *albedo_spd;      /* 31 * n_materials, or NULL */
+  float light_power_spd[31];
 } xyzgpu_scene_desc;
 
 /* kd-tree construction parameters (the reference: KDTree(max_bucket = 16,
@@ -160,7 +165,26 @@ typedef struct {
                               at most 2^26, bounded by half of the free device memory.
                               Wave buffers are shared by all scenes of a device. */
   int profile;             /* XYZGPU_PROFILE_*: per-kernel timing or work counters */
+  int spectral;            /* XYZGPU_SPECTRAL_*: XYZ tristimulus paths (the xyz renderer,
+                              default) or hero-wavelength spectral paths */
+  int hero_wavelengths;    /* 1..4 wavelengths per path in the spectral modes */
 } xyzgpu_render_params;
+
+/* Film modes.  OFF: throughput and albedo are CIE XYZ triples, the estimator of
+ * xyz::Scene::EvalutePathTracing.  BINNED: the estimator of the reference's
+ * spectral renderer, tgir::Scene::EvaluteRussianRoulette
+ * (renderer/core/SceneStrategy.cpp:11-149): one of 31 equal-probability bins
+ * over 400..700 nm per wavelength, next-event estimation before the depth cap,
+ * Russian roulette on the first wavelength's throughput, XYZ = L * 31 * CMF[bin]
+ * (libhi/hi/image/spectrum.cpp:561-567); hero_wavelengths = 1 is that
+ * estimator exactly.  CONTINUOUS: the same estimator with wavelengths uniform in
+ * 380..720 nm and spectra interpolated as basic_spectrum::Sample does
+ * (spectrum.cpp:148-165, clamped to the end bins outside 400..700).  Hero
+ * wavelength j of a path is frac(u + j / H), u the path's wavelength draw
+ * (the dimension after the camera's). */
+#define XYZGPU_SPECTRAL_OFF 0
+#define XYZGPU_SPECTRAL_BINNED 1
+#define XYZGPU_SPECTRAL_CONTINUOUS 2
 
 #define XYZGPU_PROFILE_OFF 0
 #define XYZGPU_PROFILE_TIMING 1   /* CUDA events around every kernel launch */
@@ -221,6 +245,7 @@ int xyzgpu_render_profile_get(xyzgpu_scene scene, xyzgpu_render_profile *out);
 #define XYZGPU_NOALLOC_MAX_WAVE_PATHS 65536
 #define XYZGPU_NOALLOC_MAX_DEPTH 64
 #define XYZGPU_NOALLOC_SCRATCH_BYTES 11536896
+/* (XYZ film mode only.) */
 int xyzgpu_render_noalloc(xyzgpu_scene scene, const xyzgpu_camera *camera,
                           const xyzgpu_render_params *rp, float *film_device, void *stream);
 

@@ -4,3 +4,13 @@
 #include <hi/math.hpp>
 #include <hi/image/spectrum.hpp>
 #include <hi/image/color_space.hpp>
+namespace hi {
+// renderer/core/config.hpp:91 passes a double XYZ vector to the float
+// overload of spd2xyz (MSVC binds a temporary there); this overload lets the
+// spectral renderer compile.  Its path tracer does not use the result.
+inline void spd2xyz(basic_spectrum const &spd, basic_vector3<double> &xyz) {
+  basic_vector3<float> f;
+  spd2xyz(spd, f);
+  xyz = f;
+}
+}  // namespace hi

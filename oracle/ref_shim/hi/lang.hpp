@@ -100,6 +100,10 @@ struct xyzref_mt19937_64 : public std::mersenne_twister_engine<
                                0xb5026f5aa96619e9ULL, 29, 0x5555555555555555ULL,
                                17, 0x71d67fffeda60000ULL, 37,
                                0xfff7eee000000000ULL, 43, 6364136223846793005ULL> {
+  using std::mersenne_twister_engine<std::uint_fast64_t, 64, 312, 156, 31, 0xb5026f5aa96619e9ULL,
+                                     29, 0x5555555555555555ULL, 17, 0x71d67fffeda60000ULL, 37,
+                                     0xfff7eee000000000ULL, 43,
+                                     6364136223846793005ULL>::mersenne_twister_engine;
   template <typename T>
   T next() {
     return T((*this)() >> 11) * T(1.0 / 9007199254740992.0);

@@ -179,6 +179,8 @@ class PortLib(_Common):
         L.xyzo_philox_u01.restype = C.c_float
         L.xyzo_philox_u01.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
         L.xyzo_kdtree_stats.argtypes = [C.c_void_p]
+        L.xyzo_scene_set_spectra.argtypes = [C.c_void_p, C.c_void_p]
+        L.xyzo_set_spectral.argtypes = [C.c_int, C.c_int]
         self.kind = "port"
         self.light_scale = np.ones(3)
 
@@ -225,6 +227,16 @@ class PortLib(_Common):
         k = n.value
         return out, dims, rays[:k], tri[:k], t[:k], kind[:k]
 
+    def set_spectra(self, albedo_spd, light_spd):
+        a, l = _f(albedo_spd), _f(light_spd)
+        self.lib.xyzo_scene_set_spectra(a.ctypes.data_as(C.c_void_p), l.ctypes.data_as(C.c_void_p))
+        self._spectra = (a, l)
+
+    def set_spectral(self, mode: int, hero: int = 1):
+        """0: XYZ estimator; 1: binned (the reference's spectral estimator);
+        2: continuous 380..720 nm; `hero` wavelengths per path."""
+        self.lib.xyzo_set_spectral(int(mode), int(hero))
+
     def philox_u01(self, seed, pixel, sample, dim):
         return self.lib.xyzo_philox_u01(C.c_uint64(seed), pixel, sample, dim)
 
@@ -236,3 +248,63 @@ class PortLib(_Common):
 
     def max_threads(self):
         return self.lib.xyzo_max_threads()
+
+
+def twin_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libxyztwin_thinlens.so"))
+
+
+class TwinLib:
+    """The reference's spectral renderer (renderer/, tgir) built from its
+    sources (thin-lens camera; its pinhole branch does not compile).  Each row
+    of a sample pass uses its own std::mt19937_64, so comparisons with it are
+    statistical."""
+
+    def __init__(self):
+        path = os.path.join(REF_DIR, "libxyztwin_thinlens.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"spectral reference oracle not built: {path}")
+        self.lib = C.CDLL(path)
+        L = self.lib
+        L.xyztwin_scene_create.restype = C.c_int
+        L.xyztwin_scene_create.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                           C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.xyztwin_set_camera.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float,
+                                         C.c_int, C.c_int]
+        L.xyztwin_set_path_params.argtypes = [C.c_int, C.c_double]
+        L.xyztwin_render.argtypes = [C.c_int, C.c_int, C.c_ulonglong, C.c_void_p, C.c_int]
+        L.xyztwin_light_spd.argtypes = [C.c_void_p]
+
+    def light_spd(self):
+        out = np.zeros(31, np.float32)
+        self.lib.xyztwin_light_spd(out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def scene_create(self, sd):
+        pos, tris, mat = _f(sd.positions), _i(sd.tris), _i(sd.tri_mat)
+        spd, lit = _f(sd.albedo_spd), _i(sd.is_light)
+        nrm = _f(sd.normals) if sd.normals is not None else None
+        r = self.lib.xyztwin_scene_create(pos.shape[0], pos.ctypes.data_as(C.c_void_p),
+                                          None if nrm is None else nrm.ctypes.data_as(C.c_void_p),
+                                          tris.shape[0], tris.ctypes.data_as(C.c_void_p),
+                                          mat.ctypes.data_as(C.c_void_p), spd.shape[0],
+                                          spd.ctypes.data_as(C.c_void_p), lit.ctypes.data_as(C.c_void_p))
+        if r < 0:
+            raise ValueError("spectral reference rejected the scene")
+        self._keep = (pos, tris, mat, spd, lit, nrm)
+        return r
+
+    def set_camera(self, cam, width, height):
+        eye, at = _f(cam.eye), _f(cam.at)
+        self.lib.xyztwin_set_camera(eye.ctypes.data_as(C.c_void_p), at.ctypes.data_as(C.c_void_p),
+                                    C.c_float(cam.film_size), C.c_float(cam.focal_length),
+                                    C.c_float(cam.f_number), width, height)
+        self.width, self.height = width, height
+
+    def set_path_params(self, max_depth: int, rr_threshold: float = 0.2):
+        self.lib.xyztwin_set_path_params(max_depth + 1, rr_threshold)
+
+    def render(self, spp, seed, s0=0, nthreads=0):
+        film = np.zeros((self.height, self.width, 3), np.float32)
+        self.lib.xyztwin_render(s0, spp, C.c_ulonglong(seed), film.ctypes.data_as(C.c_void_p), nthreads)
+        return film

@@ -83,6 +83,8 @@ typedef struct {
   int *lights;   /* light triangle ids in triangle order */
   float *cdf;    /* nl + 1 entries, cdf[0] = 0 */
   f3 power;      /* Phi, XYZ */
+  float *spd;    /* 31 albedo bins per material (spectral estimator), or NULL */
+  float light_spd[31];
   /* kd-tree (reference structure: interior / leaf / null nodes) */
   int nnodes, cap_nodes;
   int *kaxis;    /* 0..2 interior, -1 leaf, -2 null */
@@ -563,11 +565,197 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
   return (int)st.dim;
 }
 
+/* ------------------------------------------------- spectral estimator */
+/* The reference's spectral estimator, tgir::Scene::EvaluteRussianRoulette
+ * (renderer/core/SceneStrategy.cpp:11-149), with H hero wavelengths and the
+ * Philox stream; same geometry as eval_path.  Differences from the xyz
+ * estimator, as in that source: next-event estimation (renderer/bsdf/
+ * Lambert.cpp:98-137) comes before the depth cap; Russian roulette tests the
+ * first wavelength's throughput; the film gets XYZ = L * 31 * CMF[bin]
+ * (libhi/hi/image/spectrum.cpp:561-567).  Wavelength draw: the dimension after
+ * the camera's.  mode 1: 31 equal-probability bins over 400..700 nm;
+ * mode 2: 380..720 nm with basic_spectrum::Sample interpolation
+ * (spectrum.cpp:148-165). */
+static const double CMF_RAW[3][31] = {
+    {0.014, 0.044, 0.134, 0.284, 0.348, 0.336, 0.291, 0.195, 0.096, 0.032, 0.005, 0.009, 0.063, 0.166,
+     0.290, 0.433, 0.595, 0.762, 0.916, 1.026, 1.062, 1.003, 0.854, 0.642, 0.448, 0.284, 0.165, 0.087,
+     0.047, 0.023, 0.011},
+    {0.000, 0.001, 0.004, 0.012, 0.023, 0.038, 0.060, 0.091, 0.139, 0.208, 0.323, 0.503, 0.710, 0.862,
+     0.954, 0.995, 0.995, 0.952, 0.870, 0.757, 0.631, 0.503, 0.381, 0.265, 0.175, 0.107, 0.061, 0.032,
+     0.017, 0.008, 0.004},
+    {0.068, 0.207, 0.646, 1.386, 1.747, 1.772, 1.669, 1.288, 0.813, 0.465, 0.272, 0.158, 0.078, 0.042,
+     0.020, 0.009, 0.004, 0.002, 0.002, 0.001, 0.001, 0.000, 0.000, 0.000, 0.000, 0.000, 0.000, 0.000,
+     0.000, 0.000, 0.000}};
+
+static float cmf(int c, int i) { return (float)(CMF_RAW[c][i] / 9.80328); }
+
+static float spd_sample(const float *t, float p) {
+  p *= 31.0f;
+  p -= 0.5f;
+  if (p <= 0.0f) return t[0];
+  if (p >= 30.0f) return t[30];
+  int const k = (int)p;
+  p -= (float)k;
+  return t[k] + (t[k + 1] - t[k]) * p;
+}
+
+static float cmf_sample(int c, float p) {
+  float t[31];
+  for (int i = 0; i < 31; ++i) t[i] = cmf(c, i);
+  return spd_sample(t, p);
+}
+
+typedef struct {
+  int bin[4];
+  float p[4];
+} hero_t;
+
+static float spd_at(const float *t, const hero_t *hs, int k, int mode) {
+  return mode == 1 ? t[hs->bin[k]] : spd_sample(t, hs->p[k]);
+}
+
+static int eval_path_spectral(int px, int py, int s, uint64_t seed, int mode, int H, f3 *color) {
+  xyzo_stream st;
+  xyzo_stream_init(&st, seed, (uint32_t)(py * CAM.W + px), (uint32_t)s, 0u);
+  float const jx = xyzo_stream_next(&st);
+  float const jy = xyzo_stream_next(&st);
+  float const x = ((float)px + jx) / (float)CAM.W;
+  float const y = ((float)py + jy) / (float)CAM.H;
+  *color = mk(0, 0, 0);
+  float const lt = xyzo_stream_next(&st);
+  float const ls = xyzo_stream_next(&st);
+  int has_light = S.nl > 0 && S.cdf[S.nl] > 0;
+  f3 lpos = mk(0, 0, 0), lsn = mk(0, 0, 0), lgn = mk(0, 0, 0);
+  if (has_light) {
+    float const u = ls * S.cdf[S.nl];
+    int lo = 0, hi = S.nl + 1;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (!(u < S.cdf[mid])) lo = mid + 1; else hi = mid;
+    }
+    int n = lo - 1;
+    if (n < 0) n = 0;
+    if (n > S.nl - 1) n = S.nl - 1;
+    float const v = (u - S.cdf[n]) / (S.cdf[n + 1] - S.cdf[n]);
+    int const li = S.lights[n];
+    float const ss = sqrtf(v), uu = ss * (1 - lt), vv = ss * lt;
+    lpos = add3(add3(S.v0[li], scale3(S.e1[li], uu)), scale3(S.e2[li], vv));
+    lsn = normalize3(add3(add3(S.n0[li], scale3(S.s1[li], uu)), scale3(S.s2[li], vv)));
+    lgn = S.ng[li];
+  }
+  f3 pos, dir;
+  if (CAM.pinhole) {
+    pos = CAM.eye;
+    float const lx = (float)(((double)x - 0.5) * (double)CAM.film * (double)CAM.aspect);
+    float const ly = (float)(((double)y - 0.5) * (double)CAM.film);
+    dir = normalize3(add3(add3(scale3(CAM.right, lx), scale3(CAM.up, ly)), scale3(CAM.back, -CAM.V)));
+  } else {
+    float const ct = xyzo_stream_next(&st);
+    float const cs = xyzo_stream_next(&st);
+    float const radius = CAM.R * sqrtf(cs);
+    float const ang = (float)((2 * XYZO_M_PI) * (double)ct);
+    float const lensx = radius * cosf(ang), lensy = radius * sinf(ang);
+    pos = add3(add3(CAM.eye, scale3(CAM.right, lensx)), scale3(CAM.up, lensy));
+    float const fps = CAM.film * CAM.L / CAM.V;
+    float const lx = (float)(((double)x - 0.5) * (double)fps * (double)CAM.aspect - (double)lensx);
+    float const ly = (float)(((double)y - 0.5) * (double)fps - (double)lensy);
+    dir = normalize3(add3(add3(scale3(CAM.right, lx), scale3(CAM.up, ly)), scale3(CAM.back, -CAM.L)));
+  }
+  /* hero wavelengths */
+  float const uh = xyzo_stream_next(&st);
+  hero_t hs;
+  for (int k = 0; k < 4; ++k) {
+    float u = uh + (float)k / (float)H;
+    if (u >= 1.0f) u -= 1.0f;
+    int b = (int)(u * 31.0f);
+    hs.bin[k] = b > 30 ? 30 : b;
+    float const lambda = 380.0f + 340.0f * u;
+    hs.p[k] = (lambda - 395.0f) / 310.0f;
+  }
+  float phi[4] = {0, 0, 0, 0}, beta[4] = {1, 1, 1, 1}, L[4] = {0, 0, 0, 0};
+  for (int k = 0; k < H; ++k) phi[k] = spd_at(S.light_spd, &hs, k, mode);
+  int specular = 1;
+  float fsn = 0;
+  float const A = light_area();
+  for (size_t k = 1;;) {
+    isect_t p;
+    int const tri = find_intersection(pos, dir, &p);
+    if (tri < 0) break;
+    frame_t fr;
+    shading_basis(tri, p.f, p.g, p.back, &fr);
+    if (-dot3(dir, fr.sn) <= 0) break;
+    pos = add3(pos, scale3(dir, p.tmax));
+    int const m = S.mat[tri];
+    if (S.is_light[m] && !p.back) {
+      double const wl = XYZO_M_1_PI / (double)A;
+      double mis = 1.0;
+      if (!specular) {
+        float const cosv = fabsf(dot3(dir, fr.sn));
+        float const dimp = fsn * cosv / (p.tmax * p.tmax);
+        float const dens = (1.0f / A) / dimp;
+        mis = (double)(1.0f / (1 + dens * dens));
+      }
+      for (int j = 0; j < 4; ++j) L[j] += (float)((double)(phi[j] * beta[j]) * wl * mis);
+      break;
+    }
+    if (!S.is_light[m]) {
+      for (int j = 0; j < 4; ++j) beta[j] *= j < H ? spd_at(S.spd + 31 * m, &hs, j, mode) : 0.0f;
+      if (has_light) {
+        f3 const vin = normalize3(sub3(pos, lpos));
+        float const nk3 = dot3(vin, lgn);
+        if (!((nk3 <= 0) || (dot3(vin, lsn) <= 0))) {
+          float const nk2 = -dot3(vin, fr.sn);
+          if (!((nk2 <= 0) || (-dot3(vin, fr.gn) <= 0))) {
+            isect_t q;
+            if (find_intersection(lpos, vin, &q) == tri) {
+              float const G = (nk2 * nk3) / (q.tmax * q.tmax);
+              float const dimp = (float)(XYZO_M_1_PI * (double)G);
+              float const dens = dimp / (1.0f / A);
+              double const w = ((double)G * (XYZO_M_1_PI * XYZO_M_1_PI)) * (double)(1.0f / (1 + dens * dens));
+              for (int j = 0; j < 4; ++j) L[j] += (float)((double)(phi[j] * beta[j]) * w);
+            }
+          }
+        }
+      }
+    }
+    if (++k >= KMAX) break;
+    if ((int)k - 1 >= RR_START) {
+      float const t = beta[0];
+      if (t < RR_THRESHOLD) {
+        float const q = t / RR_THRESHOLD;
+        if (xyzo_stream_next(&st) >= q) break;
+        float const r = 1.0f / q;
+        for (int j = 0; j < 4; ++j) beta[j] *= r;
+      }
+    }
+    if (S.is_light[m]) break;
+    float const mu_phi = xyzo_stream_next(&st);
+    float const mu_theta = xyzo_stream_next(&st);
+    specular = 0;
+    float const ph = (float)(2 * XYZO_M_PI) * mu_phi;
+    float const cos_t = sqrtf(mu_theta), sin_t = sqrtf(1 - mu_theta);
+    dir = add3(add3(scale3(fr.tan, sin_t * cosf(ph)), scale3(fr.bin, sin_t * sinf(ph))), scale3(fr.sn, cos_t));
+    fsn = (float)(XYZO_M_1_PI * (double)cos_t);
+    if (!(dot3(dir, fr.gn) > 0)) break;
+  }
+  float const scale = mode == 1 ? 31.0f : 34.0f;
+  float acc[3] = {0, 0, 0};
+  for (int j = 0; j < H; ++j) {
+    float const v = L[j] * scale;
+    for (int c = 0; c < 3; ++c) acc[c] += v * (mode == 1 ? cmf(c, hs.bin[j]) : cmf_sample(c, hs.p[j]));
+  }
+  color->x = acc[0] / (float)H;
+  color->y = acc[1] / (float)H;
+  color->z = acc[2] / (float)H;
+  return (int)st.dim;
+}
+
 /* --------------------------------------------------------------- C API */
 static void free_scene(void) {
   free(S.v0); free(S.e1); free(S.e2); free(S.ng); free(S.n0); free(S.s1); free(S.s2);
   free(S.mat); free(S.albedo); free(S.is_light); free(S.lights); free(S.cdf);
   free(S.kaxis); free(S.kvalue); free(S.kchild); free(S.kbegin); free(S.kcount); free(S.refs);
+  free(S.spd);
   memset(&S, 0, sizeof(S));
 }
 
@@ -638,6 +826,20 @@ int xyzo_scene_create(int nv, const float *pos, const float *nrm, int nt, const 
 }
 
 void xyzo_scene_destroy(void) { free_scene(); }
+
+/* Spectral data of the current scene: 31 albedo bins per material, light SPD. */
+void xyzo_scene_set_spectra(const float *albedo_spd, const float *light_spd) {
+  free(S.spd);
+  S.spd = (float *)malloc(sizeof(float) * 31 * (size_t)(S.nm > 0 ? S.nm : 1));
+  memcpy(S.spd, albedo_spd, sizeof(float) * 31 * (size_t)S.nm);
+  memcpy(S.light_spd, light_spd, sizeof(float) * 31);
+}
+
+static int SPEC_MODE = 0, SPEC_H = 1;
+void xyzo_set_spectral(int mode, int hero) {
+  SPEC_MODE = mode;
+  SPEC_H = hero;
+}
 
 float xyzo_light_area(void) { return S.nl ? S.cdf[S.nl] : 0.0f; }
 
@@ -740,7 +942,10 @@ static void *job_worker(void *arg) {
         int const y = i;
         for (int x = 0; x < CAM.W; ++x) {
           f3 c;
-          eval_path(x, y, j->s, j->seed, &c);
+          if (SPEC_MODE)
+            eval_path_spectral(x, y, j->s, j->seed, SPEC_MODE, SPEC_H, &c);
+          else
+            eval_path(x, y, j->s, j->seed, &c);
           float *fp = j->film + 3 * ((size_t)y * CAM.W + x);
           fp[0] += c.x;
           fp[1] += c.y;
@@ -793,7 +998,8 @@ void xyzo_trace(int n, const float *org, const float *dir, int *tri, float *t, f
 
 int xyzo_eval_path(int px, int py, int s, uint64_t seed, float *out) {
   f3 c;
-  int const dims = eval_path(px, py, s, seed, &c);
+  int const dims = SPEC_MODE ? eval_path_spectral(px, py, s, seed, SPEC_MODE, SPEC_H, &c)
+                             : eval_path(px, py, s, seed, &c);
   out[0] = c.x;
   out[1] = c.y;
   out[2] = c.z;

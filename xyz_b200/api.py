@@ -45,7 +45,8 @@ class SceneDesc(C.Structure):
     _fields_ = [("positions", C.c_void_p), ("normals", C.c_void_p), ("n_vertices", C.c_int),
                 ("triangles", C.c_void_p), ("tri_material", C.c_void_p), ("n_triangles", C.c_int),
                 ("albedo_xyz", C.c_void_p), ("is_light", C.c_void_p), ("n_materials", C.c_int),
-                ("light_power_xyz", C.c_float * 3)]
+                ("light_power_xyz", C.c_float * 3), ("albedo_spd", C.c_void_p),
+                ("light_power_spd", C.c_float * 31)]
 
 
 class BuildParams(C.Structure):
@@ -75,7 +76,10 @@ class RenderParams(C.Structure):
     _fields_ = [("width", C.c_int), ("height", C.c_int), ("spp", C.c_int), ("spp_offset", C.c_int),
                 ("max_depth", C.c_int), ("rr_start_depth", C.c_int), ("rr_threshold", C.c_float),
                 ("seed", C.c_uint64), ("film_location", C.c_int), ("accumulate", C.c_int),
-                ("wave_paths", C.c_int), ("profile", C.c_int)]
+                ("wave_paths", C.c_int), ("profile", C.c_int), ("spectral", C.c_int),
+                ("hero_wavelengths", C.c_int)]
+
+SPECTRAL_MODES = {"off": 0, "xyz": 0, "binned": 1, "continuous": 2}
 
 
 class RenderProfile(C.Structure):
@@ -179,6 +183,10 @@ class Scene:
         d.n_materials = int(sd.albedo_xyz.shape[0])
         for k in range(3):
             d.light_power_xyz[k] = float(sd.light_power_xyz[k])
+        if getattr(sd, "albedo_spd", None) is not None:
+            d.albedo_spd = keep(sd.albedo_spd, np.float32)
+            for k in range(31):
+                d.light_power_spd[k] = float(sd.light_power_spd[k])
         bp = default_build_params(**build_kw)
         h = C.c_void_p()
         _check(L.xyzgpu_scene_create(C.byref(d), C.byref(bp), C.byref(h)))
@@ -257,7 +265,8 @@ class Scene:
     def render(self, camera, width: int, height: int, spp: int, *, seed: int = 0,
                spp_offset: int = 0, max_depth: int = 15, rr_start_depth: int = 1,
                rr_threshold: float = 0.2, film=None, accumulate: bool = False,
-               wave_paths: int = 0, profile: int = 0, stream=None):
+               wave_paths: int = 0, profile: int = 0, spectral="off", hero_wavelengths: int = 4,
+               stream=None):
         """Renders into `film`: a CUDA tensor (H, W, 3) (device film) or a numpy
         float32 array (host film).  Allocates a CUDA tensor if film is None.
         Returns the film (sums over samples, not means)."""
@@ -277,6 +286,8 @@ class Scene:
         rp.accumulate = int(bool(accumulate))
         rp.wave_paths = wave_paths
         rp.profile = profile
+        rp.spectral = SPECTRAL_MODES[spectral] if isinstance(spectral, str) else int(spectral)
+        rp.hero_wavelengths = hero_wavelengths
         if film is None:
             import torch
             film = torch.zeros((height, width, 3), dtype=torch.float32, device="cuda")

@@ -83,7 +83,7 @@ void free_scene(SceneImpl *s) {
   // work queued on any stream that still reads the scene finishes first
   cudaDeviceSynchronize();
   render_workspace_free(s->ws);
-  void *bufs[] = {s->d_tri, s->d_ng, s->d_sn, s->d_mat, s->d_lights, s->d_cdf,
+  void *bufs[] = {s->d_tri, s->d_ng, s->d_sn, s->d_mat, s->d_lights, s->d_cdf, s->d_spd,
                   s->d_nodes, s->d_refs, s->d_fetch, s->d_trace_counts};
   for (void *b : bufs)
     if (b) cudaFreeAsync(b, nullptr);
@@ -217,6 +217,8 @@ void xyzgpu_render_params_default(xyzgpu_render_params *rp) {
   rp->accumulate = 0;
   rp->wave_paths = 0;
   rp->profile = XYZGPU_PROFILE_OFF;
+  rp->spectral = XYZGPU_SPECTRAL_OFF;
+  rp->hero_wavelengths = 4;
 }
 
 int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *bp_in,
@@ -319,6 +321,7 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   XYZ_TRY(dev_upload(&s->d_mat, mat.data(), mat.size(), &bytes, st));
   XYZ_TRY(dev_upload(&s->d_lights, lights.data(), lights.size(), &bytes, st));
   XYZ_TRY(dev_upload(&s->d_cdf, cdf.data(), cdf.size(), &bytes, st));
+  if (d->albedo_spd) XYZ_TRY(dev_upload(&s->d_spd, d->albedo_spd, 31 * static_cast<size_t>(nm), &bytes, st));
   XYZ_TRY(dev_alloc(&s->d_fetch, 64, &bytes, st));
   XYZ_TRY(dev_alloc(&s->d_trace_counts, 8, &bytes, st));
   XYZ_TRY(dev_alloc(&d_box, 6, &scratch, st));
@@ -426,6 +429,8 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   v.n_lights = cdf.back() > 0.0f ? s->n_lights : 0;
   v.light_area = cdf.back();
   v.power = mk3(d->light_power_xyz[0], d->light_power_xyz[1], d->light_power_xyz[2]);
+  v.spd_albedo = s->d_spd;
+  for (int i = 0; i < 31; ++i) v.spd_light[i] = d->albedo_spd ? d->light_power_spd[i] : 0.0f;
   cudaError_t const e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     free_scene(s);
@@ -497,6 +502,8 @@ int xyzgpu_render(xyzgpu_scene scene, const xyzgpu_camera *cam, const xyzgpu_ren
   if (rp->width <= 0 || rp->height <= 0 || rp->spp < 0 || rp->spp_offset < 0 ||
       rp->max_depth < 1 || rp->max_depth > 1000 || rp->rr_start_depth < 1 ||
       !(rp->rr_threshold >= 0.0f) || rp->wave_paths < 0 || rp->profile < 0 || rp->profile > 2 ||
+      rp->spectral < 0 || rp->spectral > 2 ||
+      (rp->spectral && (rp->hero_wavelengths < 1 || rp->hero_wavelengths > 4)) ||
       (rp->film_location != XYZGPU_FILM_DEVICE && rp->film_location != XYZGPU_FILM_HOST))
     return set_error(XYZGPU_E_INVALID, "render: parameters out of range");
   if (static_cast<int64_t>(rp->width) * rp->height >= (1ll << 31))
@@ -509,6 +516,8 @@ int xyzgpu_render(xyzgpu_scene scene, const xyzgpu_camera *cam, const xyzgpu_ren
       return set_error(XYZGPU_E_INVALID, "render: camera position is not finite");
   if (!(cam->film_size > 0) || !(cam->focal_length > 0) || !(cam->f_number > 0))
     return set_error(XYZGPU_E_INVALID, "render: camera film size, focal length and F-number must be > 0");
+  if (rp->spectral && !reinterpret_cast<SceneImpl *>(scene)->d_spd)
+    return set_error(XYZGPU_E_INVALID, "render: the spectral film modes need albedo spectra in the scene");
   return render_launch(*reinterpret_cast<SceneImpl *>(scene), *cam, *rp, film,
                        static_cast<cudaStream_t>(stream));
 }

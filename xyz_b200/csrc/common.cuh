@@ -118,6 +118,8 @@ struct DevScene {
   float light_area;
   f3 power;
   f3 bmin, bmax;
+  const float *spd_albedo;  // 31 bins per material, or null (spectral modes need it)
+  float spd_light[31];      // light power spectrum (spectral modes)
 };
 
 }  // namespace xyzgpu

@@ -32,6 +32,7 @@
 #include <mutex>
 
 #include "scene.h"
+#include "spectral.h"
 #include "traverse.cuh"
 
 namespace xyzgpu {
@@ -75,6 +76,12 @@ struct WaveArgs {
   float4 *s_o, *s_d, *s_pb;
   int32_t *s_target;
   int32_t *counts;
+  // spectral modes (XYZGPU_SPECTRAL_*): beta and radiance hold one channel per
+  // hero wavelength, fSamplingNext moves to `fsn` and the shadow slot to `s_slot`
+  int spectral, hero;
+  uint32_t wl_dim;  // dimension of the hero wavelength draw
+  float *fsn;
+  int32_t *s_slot;
 };
 
 XYZ_DEV uint32_t pack_misc(uint32_t dim, uint32_t k, uint32_t specular) {
@@ -158,7 +165,13 @@ __global__ void __launch_bounds__(kThreads) k_raygen(WaveArgs A) {
     A.q_o[0][slot] = make_float4(o.x, o.y, o.z, kRayTMin);
     A.q_d[0][slot] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
     A.q_slot[0][slot] = static_cast<int32_t>(slot);
-    A.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    if (A.spectral) {
+      A.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+      A.fsn[slot] = 0.0f;
+      dim += 1;  // the hero wavelength draw follows the camera's
+    } else {
+      A.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    }
     A.misc[slot] = pack_misc(dim, 1u, 1u);
     A.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   }
@@ -186,6 +199,7 @@ struct ExtSink {
   }
 };
 
+template <bool kSpec>
 struct ShadowSink {
   const WaveArgs *A;
   uint32_t visible;
@@ -206,11 +220,12 @@ struct ShadowSink {
     double const wgt = (static_cast<double>(G) * (kInvPi * kInvPi)) *
                        static_cast<double>(1.0f / (1.0f + dens * dens));
     float4 const pb = A->s_pb[i];
-    int32_t const slot = __float_as_int(pb.w);
+    int32_t const slot = kSpec ? A->s_slot[i] : __float_as_int(pb.w);
     float4 L = A->radiance[slot];
     L.x += static_cast<float>(static_cast<double>(pb.x) * wgt);
     L.y += static_cast<float>(static_cast<double>(pb.y) * wgt);
     L.z += static_cast<float>(static_cast<double>(pb.z) * wgt);
+    if (kSpec) L.w += static_cast<float>(static_cast<double>(pb.w) * wgt);
     A->radiance[slot] = L;
     ++visible;
   }
@@ -225,8 +240,12 @@ __global__ void __launch_bounds__(kThreads) k_trace_queue(WaveArgs A, int b,
   int const qi = b & 1;
   TraceCount tc{0u, 0u, 0u};
   uint32_t visible = 0;
-  if (kShadow) {
-    ShadowSink sink{&A, 0u};
+  if (kShadow && A.spectral) {
+    ShadowSink<true> sink{&A, 0u};
+    trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
+    visible = sink.visible;
+  } else if (kShadow) {
+    ShadowSink<false> sink{&A, 0u};
     trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
     visible = sink.visible;
   } else {
@@ -489,6 +508,249 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
   }
 }
 
+
+// ------------------------------------------------------------ spectral shade
+// One vertex of the reference's spectral estimator, tgir::Scene::
+// EvaluteRussianRoulette (renderer/core/SceneStrategy.cpp:60-145), for H hero
+// wavelengths: the geometry is the XYZ kernel's; the throughput, emitted power
+// and albedo are per wavelength; next-event estimation comes before the depth
+// cap and Russian roulette looks at the first wavelength's throughput, as in
+// that estimator.
+struct HeroSet {
+  int bin[kMaxHero];
+  float p[kMaxHero];
+};
+
+XYZ_DEV HeroSet hero_set(const WaveArgs &A, uint32_t pixel, uint32_t sample) {
+  uint32_t w[4];
+  philox4x32_10(pixel, sample, A.wl_dim >> 2, 0u, static_cast<uint32_t>(A.seed),
+                static_cast<uint32_t>(A.seed >> 32), w);
+  uint32_t const j = A.wl_dim & 3u;
+  float const uh = u01_from_bits(j == 0 ? w[0] : (j == 1 ? w[1] : (j == 2 ? w[2] : w[3])));
+  HeroSet hs;
+#pragma unroll
+  for (int k = 0; k < kMaxHero; ++k) {
+    float const u = hero_u(uh, k, A.hero);
+    hs.bin[k] = hero_bin(u);
+    hs.p[k] = hero_sample_param(u);
+  }
+  return hs;
+}
+
+// Value of a 31-bin spectrum at hero wavelength k.
+XYZ_DEV float spd_value(const WaveArgs &A, const float *spd, const HeroSet &hs, int k) {
+  if (A.spectral == XYZGPU_SPECTRAL_BINNED) return spd[hs.bin[k]];
+  return spectrum_sample(hs.p[k], [&](int i) { return spd[i]; });
+}
+
+XYZ_DEV float4 spd_values(const WaveArgs &A, const float *spd, const HeroSet &hs) {
+  float v[kMaxHero] = {0.0f, 0.0f, 0.0f, 0.0f};
+  for (int k = 0; k < A.hero; ++k) v[k] = spd_value(A, spd, hs, k);
+  return make_float4(v[0], v[1], v[2], v[3]);
+}
+
+XYZ_DEV float4 mul4(float4 a, float4 b) { return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+
+__global__ void __launch_bounds__(kThreads) k_shade_spectral(WaveArgs A, int b) {
+  int32_t *const cnt = A.counts + b * kCountStride;
+  int32_t *const cnt_next = A.counts + (b + 1) * kCountStride;
+  int const n = cnt[kCExt];
+  int const lane = threadIdx.x & 31;
+  int const qi = b & 1, qo = qi ^ 1;
+  int const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int const nwarps = (gridDim.x * blockDim.x) >> 5;
+  DevScene const &S = A.S;
+  for (int base = warp * 32; base < n; base += nwarps * 32) {
+    int const i = base + lane;
+    bool push_ext = false, push_sh = false;
+    int32_t slot = 0, tri = 0;
+    f3 pos{}, dir{}, lpos{}, vin{};
+    float4 pb4{}, beta{};
+    float nk2nk3 = 0.0f, fsn_out = 0.0f;
+    uint32_t misc = 0;
+    if (i < n) {
+      slot = A.q_slot[qi][i];
+      float4 const h = A.hits[i];
+      int32_t const code = __float_as_int(h.w);
+      if (code >= 0) {
+        tri = code >> 1;
+        int const back = code & 1;
+        float4 const o4 = A.q_o[qi][i], d4 = A.q_d[qi][i];
+        f3 const d = xyz3(d4);
+        float4 const g4 = __ldg(&S.tri_ng[tri]);
+        f3 gn = xyz3(g4);
+        int32_t const m = __float_as_int(g4.w);
+        f3 sn;
+        if (S.tri_sn) {
+          f3 const n0 = xyz3(__ldg(&S.tri_sn[3 * tri])), s1 = xyz3(__ldg(&S.tri_sn[3 * tri + 1])),
+                   s2 = xyz3(__ldg(&S.tri_sn[3 * tri + 2]));
+          sn = normalize3(add3(add3(n0, scl3(s1, h.y)), scl3(s2, h.z)));
+        } else {
+          f3 const z = mk3(0.0f, 0.0f, 0.0f);
+          sn = normalize3(add3(add3(gn, scl3(z, h.y)), scl3(z, h.z)));
+        }
+        if (back) {
+          gn = neg3(gn);
+          sn = neg3(sn);
+        }
+        f3 tan = mk3(-sn.z, 0.0f, sn.x), bin;
+        float const l2 = dot3(tan, tan);
+        if (l2 > 0.0f) {
+          tan = scl3(tan, 1.0f / sqrtf(l2));
+          bin = cross3(tan, sn);
+        } else {
+          bin = mk3(0.0f, 0.0f, (sn.y > 0.0f) ? 1.0f : -1.0f);
+          tan = cross3(sn, bin);
+        }
+        if (!(-dot3(d, sn) <= 0.0f)) {
+          pos = add3(xyz3(o4), scl3(d, h.x));
+          bool const is_light = __ldg(&S.mat[m]).w != 0.0f;
+          beta = A.beta[slot];
+          float const fsn_in = A.fsn[slot];
+          misc = A.misc[slot];
+          uint32_t dim = misc & 0xffffu;
+          uint32_t k = (misc >> 16) & 0x7fffu;
+          uint32_t const specular = misc >> 31;
+          uint32_t pixel = 0, sample = 0;
+          slot_to_pixel_sample(A, slot, &pixel, &sample);
+          HeroSet const hs = hero_set(A, pixel, sample);
+          float4 const phi = spd_values(A, S.spd_light, hs);
+          bool alive = true;
+          if (is_light && !back) {
+            // SceneStrategy.cpp:100-120
+            float4 const pb = mul4(phi, beta);
+            double const wl = kInvPi / static_cast<double>(S.light_area);
+            double mis = 1.0;
+            if (!specular) {
+              float const cosv = fabsf(dot3(d, sn));
+              float const dimp = fsn_in * cosv / (h.x * h.x);
+              float const dens = (1.0f / S.light_area) / dimp;
+              mis = static_cast<double>(1.0f / (1.0f + dens * dens));
+            }
+            float4 L = A.radiance[slot];
+            L.x += static_cast<float>(static_cast<double>(pb.x) * wl * mis);
+            L.y += static_cast<float>(static_cast<double>(pb.y) * wl * mis);
+            L.z += static_cast<float>(static_cast<double>(pb.z) * wl * mis);
+            L.w += static_cast<float>(static_cast<double>(pb.w) * wl * mis);
+            A.radiance[slot] = L;
+            alive = false;
+          }
+          if (alive) {
+            if (!is_light) {
+              // next-event estimation before the depth cap (SceneStrategy.cpp:122-123,
+              // renderer/bsdf/Lambert.cpp:98-137)
+              float4 const alb = spd_values(A, S.spd_albedo + kSpecBins * m, hs);
+              beta = mul4(beta, alb);
+              if (S.n_lights > 0) {
+                LightSample const ls = sample_light(S, A.seed, pixel, sample);
+                f3 const v = normalize3(sub3(pos, ls.pos));
+                float const nk3 = dot3(v, ls.gn);
+                if (!((nk3 <= 0.0f) || (dot3(v, ls.sn) <= 0.0f))) {
+                  float const nk2 = -dot3(v, sn);
+                  if (!((nk2 <= 0.0f) || (-dot3(v, gn) <= 0.0f))) {
+                    push_sh = true;
+                    lpos = ls.pos;
+                    vin = v;
+                    nk2nk3 = nk2 * nk3;
+                    pb4 = mul4(phi, beta);
+                  }
+                }
+              }
+            }
+            ++k;
+            if (static_cast<int>(k) >= A.kmax) alive = false;
+          }
+          if (alive) {
+            PathRng rng;
+            rng.init(A.seed, pixel, sample, dim);
+            // Russian roulette on the first wavelength's throughput (SceneStrategy.cpp:131-140)
+            if (static_cast<int>(k) - 1 >= A.rr_start) {
+              float const t = beta.x;
+              if (t < A.rr_threshold) {
+                float const q = t / A.rr_threshold;
+                if (rng.next() >= q) {
+                  alive = false;
+                } else {
+                  float const r = 1.0f / q;
+                  beta = make_float4(beta.x * r, beta.y * r, beta.z * r, beta.w * r);
+                }
+              }
+            }
+            if (alive && is_light) alive = false;
+            if (alive) {
+              float const mu_phi = rng.next();
+              float const mu_theta = rng.next();
+              float const ph = static_cast<float>(2.0 * kPi) * mu_phi;
+              float const cos_t = sqrtf(mu_theta);
+              float const sin_t = sqrtf(1.0f - mu_theta);
+              dir = add3(add3(scl3(tan, sin_t * cosf(ph)), scl3(bin, sin_t * sinf(ph))), scl3(sn, cos_t));
+              fsn_out = static_cast<float>(kInvPi * static_cast<double>(cos_t));
+              if (dot3(dir, gn) > 0.0f) {
+                push_ext = true;
+                misc = pack_misc(rng.dim, k, 0u);
+              }
+            }
+          }
+        }
+      }
+    }
+    int32_t const js = warp_append(&cnt[kCShadow], push_sh);
+    if (push_sh) {
+      A.s_o[js] = make_float4(lpos.x, lpos.y, lpos.z, __int_as_float(0x7f800000));
+      A.s_d[js] = make_float4(vin.x, vin.y, vin.z, nk2nk3);
+      A.s_pb[js] = pb4;
+      A.s_slot[js] = slot;
+      A.s_target[js] = tri;
+    }
+    int32_t const je = warp_append(&cnt_next[kCExt], push_ext);
+    if (push_ext) {
+      A.q_o[qo][je] = make_float4(pos.x, pos.y, pos.z, kRayTMin);
+      A.q_d[qo][je] = make_float4(dir.x, dir.y, dir.z, __int_as_float(0x7f800000));
+      A.q_slot[qo][je] = slot;
+      A.beta[slot] = beta;
+      A.fsn[slot] = fsn_out;
+      A.misc[slot] = misc;
+    }
+  }
+}
+
+// Spectral film: XYZ of each path from its hero wavelengths, added in sample
+// order.  Binned: (L_j * 31) * CMF[bin_j] as hi::spd2xyz(i, L) (spectrum.cpp:
+// 561-567); continuous: (L_j * 34) * CMF(lambda_j); summed over j, then / H.
+__global__ void __launch_bounds__(kThreads) k_film_spectral(WaveArgs A, float *__restrict__ film) {
+  int64_t const stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  float const scale = A.spectral == XYZGPU_SPECTRAL_BINNED ? static_cast<float>(kSpecBins) : 34.0f;
+  for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < A.npix; p += stride) {
+    float *f = film + 3 * (A.p0 + p);
+    float fx = f[0], fy = f[1], fz = f[2];
+    for (int s = 0; s < A.nsamp; ++s) {
+      int64_t const slot = static_cast<int64_t>(s) * A.npix + p;
+      float4 const L4 = A.radiance[slot];
+      float const L[kMaxHero] = {L4.x, L4.y, L4.z, L4.w};
+      uint32_t pixel, sample;
+      slot_to_pixel_sample(A, slot, &pixel, &sample);
+      HeroSet const hs = hero_set(A, pixel, sample);
+      float acc[3] = {0.0f, 0.0f, 0.0f};
+      for (int k = 0; k < A.hero; ++k) {
+        float const v = L[k] * scale;
+        for (int c = 0; c < 3; ++c) {
+          float const cmf = A.spectral == XYZGPU_SPECTRAL_BINNED
+                                ? c_cmf[c][hs.bin[k]]
+                                : spectrum_sample(hs.p[k], [&](int i) { return c_cmf[c][i]; });
+          acc[c] += v * cmf;
+        }
+      }
+      float const inv_h = static_cast<float>(A.hero);
+      fx += acc[0] / inv_h;
+      fy += acc[1] / inv_h;
+      fz += acc[2] / inv_h;
+    }
+    f[0] = fx;
+    f[1] = fy;
+    f[2] = fz;
+  }
+}
+
 // ------------------------------------------------------------------ film
 // film[p] += color for each sample in increasing sample order
 // (PathTracer::run, integrator.cpp:119-127).
@@ -520,7 +782,8 @@ int occupancy_grid(K kernel, int device) {
 
 constexpr int64_t kBytesPerPath = 3 * sizeof(float4) + sizeof(uint32_t) +  // beta, radiance, hits, misc
                                   2 * (2 * sizeof(float4) + sizeof(int32_t)) +  // extension queues
-                                  3 * sizeof(float4) + sizeof(int32_t);          // shadow queue
+                                  3 * sizeof(float4) + sizeof(int32_t) +         // shadow queue
+                                  sizeof(float) + sizeof(int32_t);               // spectral fsn, slot
 constexpr int64_t kMaxDefaultWave = int64_t{1} << 26;
 
 // Wave buffers are shared by every scene on a device: the largest wave asked
@@ -552,7 +815,11 @@ void free_wave_buffers(RenderWorkspace &w) {
   cudaFree(w.s_d);
   cudaFree(w.s_pb);
   cudaFree(w.s_target);
+  cudaFree(w.fsn);
+  cudaFree(w.s_slot);
   cudaFree(w.counts);
+  w.fsn = nullptr;
+  w.s_slot = nullptr;
   w.beta = w.radiance = w.hits = w.s_o = w.s_d = w.s_pb = nullptr;
   w.misc = nullptr;
   w.q_o[0] = w.q_o[1] = w.q_d[0] = w.q_d[1] = nullptr;
@@ -590,6 +857,8 @@ int ensure_wave_buffers(RenderWorkspace &w, int64_t capacity, int iters) {
   XYZ_ALLOC(w.s_d, c * sizeof(float4));
   XYZ_ALLOC(w.s_pb, c * sizeof(float4));
   XYZ_ALLOC(w.s_target, c * sizeof(int32_t));
+  XYZ_ALLOC(w.fsn, c * sizeof(float));
+  XYZ_ALLOC(w.s_slot, c * sizeof(int32_t));
   XYZ_ALLOC(w.counts, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t));
 #undef XYZ_ALLOC
   w.capacity = capacity;
@@ -679,15 +948,17 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   }
   if (!rp.accumulate) XYZ_CUDA_TRY(cudaMemsetAsync(film_dev, 0, film_elems * sizeof(float), st));
 
-  static int g_raygen = 0, g_trace_e = 0, g_trace_s = 0, g_shade = 0, g_film = 0;
+  static int g_raygen = 0, g_trace_e = 0, g_trace_s = 0, g_shade = 0, g_film = 0, g_shade_sp = 0;
   if (!g_raygen) {
     g_raygen = occupancy_grid(k_raygen, s.device);
     g_trace_e = occupancy_grid(k_trace_queue<false, false>, s.device);
     g_trace_s = occupancy_grid(k_trace_queue<true, false>, s.device);
     g_shade = occupancy_grid(k_shade, s.device);
+    g_shade_sp = occupancy_grid(k_shade_spectral, s.device);
     g_film = occupancy_grid(k_film, s.device);
   }
   int const prof = rp.profile;
+  bool const spectral = rp.spectral != XYZGPU_SPECTRAL_OFF;
   bool const timing = prof == XYZGPU_PROFILE_TIMING;
   bool const counting = prof == XYZGPU_PROFILE_COUNTERS;
   XYZ_CUDA_TRY(cudaMemsetAsync(w.tally, 0, kTallyWords * sizeof(unsigned long long), st));
@@ -732,6 +1003,11 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   A.s_pb = wv.s_pb;
   A.s_target = wv.s_target;
   A.counts = wv.counts;
+  A.spectral = rp.spectral;
+  A.hero = spectral ? rp.hero_wavelengths : 1;
+  A.wl_dim = cam.pinhole ? 4u : 6u;
+  A.fsn = wv.fsn;
+  A.s_slot = wv.s_slot;
 
   xyzgpu_render_counters rc_out{};
   uint64_t launches = 0;
@@ -765,7 +1041,10 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
           k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, pc);
         XYZ_MARK(1, false);
         XYZ_MARK(2, true);
-        k_shade<<<g_shade, kThreads, 0, st>>>(A, b);
+        if (spectral)
+          k_shade_spectral<<<g_shade_sp, kThreads, 0, st>>>(A, b);
+        else
+          k_shade<<<g_shade, kThreads, 0, st>>>(A, b);
         XYZ_MARK(2, false);
         XYZ_MARK(3, true);
         if (counting)
@@ -777,7 +1056,10 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       }
       int const gf = static_cast<int>(std::min<int64_t>(g_film, (A.npix + kThreads - 1) / kThreads));
       XYZ_MARK(4, true);
-      k_film<<<gf, kThreads, 0, st>>>(A, film_dev);
+      if (spectral)
+        k_film_spectral<<<gf, kThreads, 0, st>>>(A, film_dev);
+      else
+        k_film<<<gf, kThreads, 0, st>>>(A, film_dev);
       XYZ_MARK(4, false);
 #undef XYZ_MARK
       k_tally<<<1, 32, 0, st>>>(A, iters, w.tally);
@@ -937,6 +1219,8 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
     return set_error(XYZGPU_E_INVALID, "render_noalloc: the film must be device memory");
   if (rp.profile != XYZGPU_PROFILE_OFF)
     return set_error(XYZGPU_E_INVALID, "render_noalloc: profiling is not available");
+  if (rp.spectral != XYZGPU_SPECTRAL_OFF)
+    return set_error(XYZGPU_E_INVALID, "render_noalloc: only the XYZ film mode is available");
   if (rp.wave_paths > kNoAllocPaths)
     return set_error(XYZGPU_E_LIMIT, "render_noalloc: wave_paths %d exceeds the maximum of %lld",
                      rp.wave_paths, static_cast<long long>(kNoAllocPaths));

@@ -39,6 +39,8 @@ struct RenderWorkspace {
   float4 *hits = nullptr;
   float4 *s_o = nullptr, *s_d = nullptr, *s_pb = nullptr;
   int32_t *s_target = nullptr;
+  float *fsn = nullptr;         // spectral modes: fSamplingNext per path
+  int32_t *s_slot = nullptr;    // spectral modes: path slot of each shadow ray
   int32_t *counts = nullptr;  // per iteration counters (see render.cu)
   unsigned long long *tally = nullptr;  // [0] ext rays [1] shadow rays [2] visible,
                                         // [8..13] traversal counters of COUNTERS renders,
@@ -59,6 +61,7 @@ struct SceneImpl {
   float4 *d_tri = nullptr, *d_ng = nullptr, *d_sn = nullptr, *d_mat = nullptr;
   int32_t *d_lights = nullptr;
   float *d_cdf = nullptr;
+  float *d_spd = nullptr;  // 31-bin albedo spectra (spectral modes)
   uint2 *d_nodes = nullptr;
   int32_t *d_refs = nullptr;
   int64_t n_nodes = 0, n_refs = 0, n_leaves = 0, n_empty = 0;

@@ -21,7 +21,7 @@ from typing import Optional
 
 import numpy as np
 
-from .spectrum import ccir601_rgb_to_xyz, flat_spd_xyz
+from .spectrum import N_BINS, ccir601_rgb_to_xyz, flat_spd_xyz, rgb_to_spd
 
 
 @dataclass
@@ -61,6 +61,8 @@ class SceneData:
     normals: Optional[np.ndarray] = None  # (nv, 3) float32 shading normals
     camera: Camera = field(default_factory=Camera)
     name: str = ""
+    albedo_spd: Optional[np.ndarray] = None       # (nm, 31) float32 spectra (spectral modes)
+    light_power_spd: Optional[np.ndarray] = None  # (31,) float32, Phi per bin
 
     @property
     def n_tris(self) -> int:
@@ -83,6 +85,11 @@ def triangle_areas(pos: np.ndarray, tris: np.ndarray) -> np.ndarray:
     e2 = (p[tris[:, 2]] - v0).astype(np.float32)
     c = np.cross(e2, e1).astype(np.float32)
     return (np.sqrt((c * c).sum(axis=1, dtype=np.float32)) * np.float32(0.5)).astype(np.float32)
+
+
+def flat_emitter_power_spd(radiance: float, light_area: float) -> np.ndarray:
+    """Phi per 10 nm bin of a flat emitter of `radiance` W/m^2/sr: pi * A * L."""
+    return np.full(N_BINS, np.float32(math.pi * light_area) * np.float32(radiance), np.float32)
 
 
 def flat_emitter_power(radiance: float, light_area: float) -> np.ndarray:
@@ -168,6 +175,9 @@ def cornell_box(res_fov: float = 40.0, pinhole: bool = True,
                                           pinhole=pinhole),
                    name="cornell")
     sd.light_power_xyz = flat_emitter_power(radiance, sd.light_area())
+    sd.albedo_spd = np.stack([rgb_to_spd((0.8, 0.8, 0.8)), rgb_to_spd((0.63, 0.06, 0.05)),
+                              rgb_to_spd((0.14, 0.45, 0.09)), np.zeros(N_BINS, np.float32)])
+    sd.light_power_spd = flat_emitter_power_spd(radiance, sd.light_area())
     return sd
 
 
@@ -315,6 +325,10 @@ def spheres_scene(level: int = 7, n_spheres: int = 3, seed: int = 0,
                    camera=Camera.with_fov((0.0, 1.6, 4.8), (0.0, 0.6, 0.0), fov, pinhole=True),
                    name=f"spheres-l{level}x{n_spheres}")
     sd.light_power_xyz = flat_emitter_power(radiance, sd.light_area())
+    # grey materials have flat spectra
+    sd.albedo_spd = np.concatenate([np.repeat(grey[:, None], N_BINS, axis=1).astype(np.float32),
+                                    np.zeros((1, N_BINS), np.float32)])
+    sd.light_power_spd = flat_emitter_power_spd(radiance, sd.light_area())
     return sd
 
 

@@ -73,3 +73,35 @@ def ccir601_rgb_to_xyz(rgb) -> np.ndarray:
     y = np.float32(np.float32(0.2989) * r + np.float32(0.5866) * g + np.float32(0.1145) * b)
     z = np.float32(np.float32(0.0000) * r + np.float32(0.0661) * g + np.float32(1.1162) * b)
     return np.clip(np.array([x, y, z], dtype=np.float32), 0.0, 1.0)
+
+
+def rgb_to_spd(rgb) -> np.ndarray:
+    """31-bin spectrum of a linear RGB colour by the reference's Gaussian-basis
+    fit (libhi/hi/image/spectrum.cpp:574-626): three Gaussians centred at
+    641, 508 and 426 nm whose widths narrow from 150 to 80 nm with the colour's
+    saturation, weighted so that the spectrum's XYZ (through the CMF) equals
+    the colour's CCIR 601-1 XYZ (float32 arithmetic)."""
+    f32 = np.float32
+    r, g, b = (f32(c) for c in rgb)
+    lam_c = np.array([641, 508, 426], dtype=np.float32)
+    smin, smax = f32(80), f32(150)
+    int12 = f32(0) if (r + g) == 0 else f32(abs(r - g) / (r + g))
+    int23 = f32(0) if (b + g) == 0 else f32(abs(b - g) / (b + g))
+    sigma = np.zeros(3, np.float32)
+    sigma[0] = smax + (smin - smax) * int12
+    sigma[1] = smax + (smin - smax) * int23
+    sigma[2] = min(sigma[0], sigma[1])
+    inv_sigma = (f32(1) / np.sqrt(f32(2 * np.pi) * sigma)).astype(np.float32)
+    lam = (400 + 10 * np.arange(N_BINS)).astype(np.float32)
+    f = np.zeros((3, N_BINS), np.float32)
+    for i in range(3):
+        x = ((lam - lam_c[i]) / sigma[i]).astype(np.float32)
+        f[i] = (np.exp((x * x) / f32(-2)) * inv_sigma[i]).astype(np.float32)
+    a = np.array([[float(np.dot(f[i].astype(np.float64), XYZ_CMF[c].astype(np.float64))) for c in range(3)]
+                  for i in range(3)])
+    xyz = np.array([0.6069 * r + 0.1735 * g + 0.2003 * b,
+                    0.2989 * r + 0.5866 * g + 0.1145 * b,
+                    0.0000 * r + 0.0661 * g + 1.1162 * b], dtype=np.float64)
+    # SolveLinearSystem (libhi/hi/math/vector3.hpp:221-240): xyz = sum_i w_i a_i
+    w = np.linalg.solve(a.T, xyz)
+    return (w[:, None] * f.astype(np.float64)).sum(axis=0).astype(np.float32)
