@@ -320,6 +320,7 @@ def run_gpu_arm(args, rank, world):
                                "leaves": round(cp["shadow_leaves"] / max(1, cp["shadow_rays"]), 2),
                                "tri_tests": round(cp["shadow_tri_tests"] / max(1, cp["shadow_rays"]), 2)}},
         "rays_per_step": rays,
+        "rays_by_iteration": {"extension": cp["ext_rays_by_iter"], "shadow": cp["shadow_rays_by_iter"]},
         "trace_ms_per_step": round(trace_ms, 3),
         "kernel_ms_per_step": {c: round(ms_cls[c] / max(1, args.steps), 3) for c in api.KERNEL_CLASSES},
         "kernel_share": {c: round(ms_cls[c] / max(1e-9, sum(ms_cls.values())), 4) for c in api.KERNEL_CLASSES},
