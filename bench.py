@@ -208,6 +208,53 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def adjoint_bench(steps: int, warmup: int):
+    """Differentiable-rendering iteration on the 19,392-triangle room: render
+    512 x 512 x 32 spp, L2 loss gradient to a target, 32 spp path-replay adjoint
+    on the next 32 samples, max depth 6, Russian roulette off.  Returns
+    ms per iteration (primal + adjoint, CUDA events) and its split."""
+    import torch
+    from xyz_b200 import api, diff, scenes
+    W = H = 512
+    spp = 32
+    ds = scenes.diff_scene()
+    with api.Scene(ds.scene) as s:
+        R = diff.Renderer(s, ds.scene.camera, W, H, spp, adjoint_spp=spp, adjoint_offset=spp,
+                          max_depth=6, rr_threshold=0.0)
+        s.set_materials(ds.target_albedo, ds.target_emission)
+        target = R.render()
+        s.set_materials(ds.albedo, ds.emission)
+
+        def iteration():
+            img = R.render()
+            d_img = 2.0 * (img - target)
+            return R.gradient(d_img)
+
+        for _ in range(warmup):
+            iteration()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        prim = adj = 0.0
+        for _ in range(steps):
+            ev[0].record()
+            img = R.render()
+            d_img = 2.0 * (img - target)
+            ev[1].record()
+            R.gradient(d_img)
+            ev[2].record()
+            torch.cuda.synchronize()
+            prim += ev[0].elapsed_time(ev[1])
+            adj += ev[1].elapsed_time(ev[2])
+        samples = W * H * spp
+        return {"ms_per_iter": round((prim + adj) / steps, 3), "primal_ms": round(prim / steps, 3),
+                "adjoint_ms": round(adj / steps, 3),
+                "adjoint_msamples_per_s": round(samples / (adj / steps / 1000.0) / 1e6, 1),
+                "config": "room + 3 displaced level-4 spheres, 19,392 triangles (one material each), "
+                          "512x512, 32 spp primal + 32 spp replay adjoint (next 32 samples), "
+                          "max depth 6, Russian roulette off, gradients of albedo (3 per triangle) "
+                          "and emission (32 light triangles)"}
+
+
 def profiled_traffic():
     """DRAM bytes per traced ray of the trace kernel from the committed ncu
     summary (profiles/trace_queue_spheres1m.txt), if present."""
@@ -353,6 +400,9 @@ def run_gpu_arm(args, rank, world):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(sd)
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        adjoint = adjoint_bench(args.steps, args.warmup)
 
     if rank == 0:
         line = {
@@ -363,6 +413,7 @@ def run_gpu_arm(args, rank, world):
             "config": workload_config(stats) | {"parallelism": f"sample-parallel x{world}",
                                                  "waves_per_step": counters["waves"]},
             "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
+            "adjoint": adjoint,
             "clocks": clk, "wall_ms_timed_region": round(wall_ms, 1),
             "render_counters": counters,
         }
@@ -378,6 +429,8 @@ def main():
     ap.add_argument("--impl", choices=["xyz", "reference"], default="xyz")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the differentiable-rendering measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -249,6 +249,44 @@ int xyzgpu_render_profile_get(xyzgpu_scene scene, xyzgpu_render_profile *out);
 int xyzgpu_render_noalloc(xyzgpu_scene scene, const xyzgpu_camera *camera,
                           const xyzgpu_render_params *rp, float *film_device, void *stream);
 
+/* Material parameters after creation (the differentiable-rendering inputs).
+ * albedo_xyz: 3 per material (the XYZ triple the throughput is multiplied by;
+ * ignored for lights); emission: 1 per material, a scale of the light power
+ * emitted by that material's light triangles (1 at creation, so the emitted
+ * radiance is the reference's Phi / (pi * light area) until it is set; an
+ * extension: the reference has one power for all lights).  Either pointer may
+ * be NULL (left unchanged).  location: XYZGPU_FILM_HOST (values checked and
+ * copied before return) or XYZGPU_FILM_DEVICE (device arrays read on
+ * `stream`, not checked). */
+int xyzgpu_scene_set_materials(xyzgpu_scene scene, const float *albedo_xyz, const float *emission,
+                               int location, void *stream);
+
+/* Copies the current material parameters to host arrays (either may be NULL). */
+int xyzgpu_scene_get_materials(xyzgpu_scene scene, float *albedo_xyz, float *emission);
+
+/* Path-replay adjoint of xyzgpu_render (Vicini, Speierer and Jakob, "Path
+ * Replay Backpropagation", 2021).  With film = the W*H*3 sums xyzgpu_render
+ * produces for the same scene, camera and parameters, adds
+ *   d_albedo[3m + c] += sum_p d_film[p] . d film[p] / d albedo[m][c]
+ *   d_emission[m]    += sum_p d_film[p] . d film[p] / d emission[m]
+ * for the same sample paths (same seed and sample indices): each wave is traced
+ * twice, a primal pass that keeps every path's radiance and a replay pass that
+ * regenerates the same paths and, at each vertex, scatters
+ * d_film . (radiance collected from that vertex on) / albedo into the vertex's
+ * material and d_film . (emitted contribution at unit scale) into the light's.
+ * The path sampling (Lambert cosine lobe, light choice by area, MIS weights) does
+ * not depend on albedo or emission, so with Russian roulette off
+ * (rr_threshold = 0) the result is the exact derivative of the rendered film;
+ * with it on, the roulette's survival scale is held constant.  An albedo channel
+ * that is exactly 0 gets no gradient from vertices of that material.
+ * d_film, d_albedo (3 * n_materials) and d_emission (n_materials) are device
+ * arrays; gradients are accumulated with float atomics (summation order varies
+ * between calls).  XYZ film mode only, profile off; film_location and
+ * accumulate are ignored. */
+int xyzgpu_adjoint(xyzgpu_scene scene, const xyzgpu_camera *camera,
+                   const xyzgpu_render_params *rp, const float *d_film, float *d_albedo,
+                   float *d_emission, void *stream);
+
 /* Host evaluation of the random stream defined above (for tests). */
 float xyzgpu_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim);
 

@@ -181,6 +181,9 @@ class PortLib(_Common):
         L.xyzo_kdtree_stats.argtypes = [C.c_void_p]
         L.xyzo_scene_set_spectra.argtypes = [C.c_void_p, C.c_void_p]
         L.xyzo_set_spectral.argtypes = [C.c_int, C.c_int]
+        L.xyzo_set_materials.argtypes = [C.c_void_p, C.c_void_p]
+        L.xyzo_adjoint.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_int]
         self.kind = "port"
         self.light_scale = np.ones(3)
 
@@ -236,6 +239,26 @@ class PortLib(_Common):
         """0: XYZ estimator; 1: binned (the reference's spectral estimator);
         2: continuous 380..720 nm; `hero` wavelengths per path."""
         self.lib.xyzo_set_spectral(int(mode), int(hero))
+
+    def set_materials(self, albedo_xyz=None, emission=None):
+        """Replaces the albedos (n_materials, 3) and / or sets the per-material
+        emission scale (n_materials,); None leaves a table unchanged."""
+        a = None if albedo_xyz is None else _f(albedo_xyz)
+        e = None if emission is None else _f(emission)
+        self.lib.xyzo_set_materials(None if a is None else a.ctypes.data_as(C.c_void_p),
+                                    None if e is None else e.ctypes.data_as(C.c_void_p))
+
+    def adjoint(self, dfilm, spp: int, seed: int, n_materials: int, s0: int = 0, nthreads: int = 0):
+        """Gradient of sum(dfilm * film) over samples [s0, s0 + spp) with
+        respect to albedo (n_materials, 3) and emission scale (n_materials,),
+        float64 (per-contribution derivatives, XYZ estimator)."""
+        df = _f(dfilm)
+        assert df.shape == (self.height, self.width, 3)
+        ga = np.zeros((n_materials, 3), np.float64)
+        ge = np.zeros(n_materials, np.float64)
+        self.lib.xyzo_adjoint(s0, spp, C.c_uint64(seed), df.ctypes.data_as(C.c_void_p),
+                              ga.ctypes.data_as(C.c_void_p), ge.ctypes.data_as(C.c_void_p), nthreads)
+        return ga, ge
 
     def philox_u01(self, seed, pixel, sample, dim):
         return self.lib.xyzo_philox_u01(C.c_uint64(seed), pixel, sample, dim)

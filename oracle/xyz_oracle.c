@@ -30,8 +30,16 @@
  *
  * Extensions beyond the reference (off by default, used to check the CUDA
  * path's options): `rr_start` (first vertex index that plays Russian roulette;
- * the reference plays it from vertex 1) and a run-time pinhole switch (the
- * reference selects it at compile time, CONFIG_PINHOLE_CAMERA_MODEL).
+ * the reference plays it from vertex 1), a run-time pinhole switch (the
+ * reference selects it at compile time, CONFIG_PINHOLE_CAMERA_MODEL), and a
+ * per-material emission scale of the light power (1 = the reference).
+ *
+ * Gradients (xyzo_adjoint): for the differentiable-rendering check, every
+ * contribution C = Phi * e * prod_j albedo_j * r * w of a path (r the Russian
+ * roulette scale, w the geometric / MIS weight) is differentiated directly:
+ * dC/d albedo_j = C without albedo_j's factor (product of the others), dC/de =
+ * C at e = 1.  This per-contribution form is independent of the CUDA adjoint's
+ * suffix-sum replay.
  */
 #include <math.h>
 #include <pthread.h>
@@ -84,6 +92,7 @@ typedef struct {
   float *cdf;    /* nl + 1 entries, cdf[0] = 0 */
   f3 power;      /* Phi, XYZ */
   float *spd;    /* 31 albedo bins per material (spectral estimator), or NULL */
+  float *emission; /* per-material emission scale, or NULL (all 1) */
   float light_spd[31];
   /* kd-tree (reference structure: interior / leaf / null nodes) */
   int nnodes, cap_nodes;
@@ -417,6 +426,40 @@ static inline void rec_seg(f3 o, f3 d, int tri, float t, int kind) {
   REC->kind[i] = kind;
 }
 
+/* Gradient context of one thread (xyzo_adjoint). */
+#define XYZO_MAX_VERT 1024
+typedef struct {
+  const float *dfilm;  /* 3 per pixel */
+  double *g_alb, *g_em;
+  size_t pix;
+  int nv;
+  int vm[XYZO_MAX_VERT];  /* materials of the vertices whose albedo is in beta */
+  double r[3];            /* Russian roulette scale in beta */
+} grad_t;
+static __thread grad_t *GRAD = NULL;
+
+static inline float emission_of(int m) { return S.emission ? S.emission[m] : 1.0f; }
+
+/* Adds dfilm . dC/dparams for a contribution C_c = phi_w[c] * e * r_c * prod a_c. */
+static void grad_contrib(const double phi_w[3], int light_m) {
+  grad_t *g = GRAD;
+  float const *df = g->dfilm + 3 * g->pix;
+  double const e = (double)emission_of(light_m);
+  double cu = 0;
+  for (int c = 0; c < 3; ++c) {
+    double prod = g->r[c];
+    for (int j = 0; j < g->nv; ++j) prod *= (double)at3(S.albedo[g->vm[j]], c);
+    cu += (double)df[c] * phi_w[c] * prod;
+    for (int j = 0; j < g->nv; ++j) {
+      double others = g->r[c] * e * phi_w[c];
+      for (int i = 0; i < g->nv; ++i)
+        if (i != j) others *= (double)at3(S.albedo[g->vm[i]], c);
+      g->g_alb[3 * g->vm[j] + c] += (double)df[c] * others;
+    }
+  }
+  g->g_em[light_m] += cu;
+}
+
 static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
   xyzo_stream st;
   xyzo_stream_init(&st, seed, (uint32_t)(py * CAM.W + px), (uint32_t)s, 0u);
@@ -431,6 +474,7 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
   float const ls = xyzo_stream_next(&st);
   int has_light = S.nl > 0;
   f3 lpos = mk(0, 0, 0), lsn = mk(0, 0, 0), lgn = mk(0, 0, 0);
+  int lmat = 0;
   if (has_light) {
     float const u = ls * S.cdf[S.nl];
     int lo = 0, hi = S.nl + 1; /* upper_bound over cdf[0..nl] */
@@ -448,8 +492,14 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
     lpos = add3(add3(S.v0[li], scale3(S.e1[li], uu)), scale3(S.e2[li], vv));
     lsn = normalize3(add3(add3(S.n0[li], scale3(S.s1[li], uu)), scale3(S.s2[li], vv)));
     lgn = S.ng[li];
+    lmat = S.mat[li];
   }
   f3 const lpow = S.power;
+  if (GRAD) {
+    GRAD->pix = (size_t)py * (size_t)CAM.W + (size_t)px;
+    GRAD->nv = 0;
+    GRAD->r[0] = GRAD->r[1] = GRAD->r[2] = 1.0;
+  }
 
   /* camera vertex */
   f3 pos, dir;
@@ -490,10 +540,12 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
     pos = add3(pos, scale3(dir, p.tmax));
     int const m = S.mat[tri];
     if (S.is_light[m] && !p.back) {
-      f3 const pb = mul3(lpow, beta);
+      f3 const pb = scale3(mul3(lpow, beta), emission_of(m));
+      double wt;
       if (specular) {
         double const w = XYZO_M_1_PI / (double)A;
         acc_d(color, (double)pb.x * w, (double)pb.y * w, (double)pb.z * w);
+        wt = w;
       } else {
         float const cosv = fabsf(dot3(dir, fr.sn));
         float const d2 = p.tmax * p.tmax;
@@ -504,6 +556,11 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
         float const mis = 1.0f / (1 + dens * dens);
         acc_d(color, (double)pb.x * w * (double)mis, (double)pb.y * w * (double)mis,
               (double)pb.z * w * (double)mis);
+        wt = w * (double)mis;
+      }
+      if (GRAD) {
+        double const pw[3] = {(double)lpow.x * wt, (double)lpow.y * wt, (double)lpow.z * wt};
+        grad_contrib(pw, m);
       }
       break;
     }
@@ -511,7 +568,10 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
 
     /* NEE (Lambert::CalculateWeightedDirectLighting); a light's NEE is zero
      * and leaves the throughput alone (xyz/bsdf/light.cpp:18-25). */
-    if (!S.is_light[m]) beta = mul3(beta, S.albedo[m]);
+    if (!S.is_light[m]) {
+      beta = mul3(beta, S.albedo[m]);
+      if (GRAD && GRAD->nv < XYZO_MAX_VERT) GRAD->vm[GRAD->nv++] = m;
+    }
     if (has_light && !S.is_light[m]) {
       f3 const vin = normalize3(sub3(pos, lpos));
       float const nk3 = dot3(vin, lgn);
@@ -528,10 +588,14 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
             float const dens = dimp / dexp;
             double const w =
                 ((double)G * (XYZO_M_1_PI * XYZO_M_1_PI)) * (double)(1.0f / (1 + dens * dens));
-            f3 const pb = mul3(lpow, beta);
+            f3 const pb = scale3(mul3(lpow, beta), emission_of(lmat));
             f3 const c = mk((float)((double)pb.x * w), (float)((double)pb.y * w),
                             (float)((double)pb.z * w));
             *color = add3(*color, c);
+            if (GRAD) {
+              double const pw[3] = {(double)lpow.x * w, (double)lpow.y * w, (double)lpow.z * w};
+              grad_contrib(pw, lmat);
+            }
           }
         }
       }
@@ -544,6 +608,8 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
         float const q = t / RR_THRESHOLD;
         if (xyzo_stream_next(&st) >= q) break;
         beta = scale3(beta, 1.0f / q);
+        if (GRAD)
+          for (int c = 0; c < 3; ++c) GRAD->r[c] *= (double)(1.0f / q);
       }
     }
 
@@ -626,6 +692,7 @@ static int eval_path_spectral(int px, int py, int s, uint64_t seed, int mode, in
   float const ls = xyzo_stream_next(&st);
   int has_light = S.nl > 0 && S.cdf[S.nl] > 0;
   f3 lpos = mk(0, 0, 0), lsn = mk(0, 0, 0), lgn = mk(0, 0, 0);
+  int lmat = 0;
   if (has_light) {
     float const u = ls * S.cdf[S.nl];
     int lo = 0, hi = S.nl + 1;
@@ -642,6 +709,7 @@ static int eval_path_spectral(int px, int py, int s, uint64_t seed, int mode, in
     lpos = add3(add3(S.v0[li], scale3(S.e1[li], uu)), scale3(S.e2[li], vv));
     lsn = normalize3(add3(add3(S.n0[li], scale3(S.s1[li], uu)), scale3(S.s2[li], vv)));
     lgn = S.ng[li];
+    lmat = S.mat[li];
   }
   f3 pos, dir;
   if (CAM.pinhole) {
@@ -695,7 +763,8 @@ static int eval_path_spectral(int px, int py, int s, uint64_t seed, int mode, in
         float const dens = (1.0f / A) / dimp;
         mis = (double)(1.0f / (1 + dens * dens));
       }
-      for (int j = 0; j < 4; ++j) L[j] += (float)((double)(phi[j] * beta[j]) * wl * mis);
+      float const e = emission_of(m);
+      for (int j = 0; j < 4; ++j) L[j] += (float)((double)(phi[j] * beta[j] * e) * wl * mis);
       break;
     }
     if (!S.is_light[m]) {
@@ -712,7 +781,8 @@ static int eval_path_spectral(int px, int py, int s, uint64_t seed, int mode, in
               float const dimp = (float)(XYZO_M_1_PI * (double)G);
               float const dens = dimp / (1.0f / A);
               double const w = ((double)G * (XYZO_M_1_PI * XYZO_M_1_PI)) * (double)(1.0f / (1 + dens * dens));
-              for (int j = 0; j < 4; ++j) L[j] += (float)((double)(phi[j] * beta[j]) * w);
+              float const e = emission_of(lmat);
+              for (int j = 0; j < 4; ++j) L[j] += (float)((double)(phi[j] * beta[j] * e) * w);
             }
           }
         }
@@ -756,6 +826,7 @@ static void free_scene(void) {
   free(S.mat); free(S.albedo); free(S.is_light); free(S.lights); free(S.cdf);
   free(S.kaxis); free(S.kvalue); free(S.kchild); free(S.kbegin); free(S.kcount); free(S.refs);
   free(S.spd);
+  free(S.emission);
   memset(&S, 0, sizeof(S));
 }
 
@@ -835,6 +906,17 @@ void xyzo_scene_set_spectra(const float *albedo_spd, const float *light_spd) {
   memcpy(S.light_spd, light_spd, sizeof(float) * 31);
 }
 
+/* Replaces the albedos (3 per material) and / or sets the per-material
+ * emission scale (NULL leaves a table unchanged). */
+void xyzo_set_materials(const float *albedo, const float *emission) {
+  if (albedo)
+    for (int m = 0; m < S.nm; ++m) S.albedo[m] = mk(albedo[3 * m], albedo[3 * m + 1], albedo[3 * m + 2]);
+  if (emission) {
+    if (!S.emission) S.emission = (float *)malloc(sizeof(float) * (size_t)(S.nm > 0 ? S.nm : 1));
+    memcpy(S.emission, emission, sizeof(float) * (size_t)S.nm);
+  }
+}
+
 static int SPEC_MODE = 0, SPEC_H = 1;
 void xyzo_set_spectral(int mode, int hero) {
   SPEC_MODE = mode;
@@ -910,6 +992,10 @@ typedef struct {
   int s;
   uint64_t seed;
   float *film;
+  /* adjoint: samples [s, s + spp) of rows [lo, hi), gradients summed under mu */
+  int spp;
+  const float *dfilm;
+  double *g_alb, *g_em;
 } job_t;
 
 static int job_take(job_t *j, int *b, int *e) {
@@ -923,8 +1009,35 @@ static int job_take(job_t *j, int *b, int *e) {
   return 1;
 }
 
+static void *adjoint_worker(job_t *j) {
+  size_t const na = 3 * (size_t)S.nm, ne = (size_t)S.nm;
+  grad_t *g = (grad_t *)calloc(1, sizeof(grad_t));
+  g->dfilm = j->dfilm;
+  g->g_alb = (double *)calloc(na + 1, sizeof(double));
+  g->g_em = (double *)calloc(ne + 1, sizeof(double));
+  GRAD = g;
+  int b, e;
+  while (job_take(j, &b, &e))
+    for (int y = b; y < e; ++y)
+      for (int s = j->s; s < j->s + j->spp; ++s)
+        for (int x = 0; x < CAM.W; ++x) {
+          f3 c;
+          eval_path(x, y, s, j->seed, &c);
+        }
+  GRAD = NULL;
+  pthread_mutex_lock(&j->mu);
+  for (size_t i = 0; i < na; ++i) j->g_alb[i] += g->g_alb[i];
+  for (size_t i = 0; i < ne; ++i) j->g_em[i] += g->g_em[i];
+  pthread_mutex_unlock(&j->mu);
+  free(g->g_alb);
+  free(g->g_em);
+  free(g);
+  return NULL;
+}
+
 static void *job_worker(void *arg) {
   job_t *j = (job_t *)arg;
+  if (j->mode == 2) return adjoint_worker(j);
   int b, e;
   while (job_take(j, &b, &e)) {
     for (int i = b; i < e; ++i) {
@@ -1039,3 +1152,23 @@ void xyzo_render(int s0, int spp, uint64_t seed, int y0, int y1, float *film, in
 }
 
 int xyzo_max_threads(void) { return default_threads(0); }
+
+/* Gradient of sum_p dfilm[p] . film[p] (the film of xyzo_render over samples
+ * [s0, s0 + spp)) with respect to the albedos (3 per material) and emission
+ * scales (1 per material), added to g_alb / g_em.  XYZ estimator only. */
+void xyzo_adjoint(int s0, int spp, uint64_t seed, const float *dfilm, double *g_alb, double *g_em,
+                  int nthreads) {
+  job_t j;
+  memset(&j, 0, sizeof(j));
+  j.mode = 2;
+  j.lo = 0;
+  j.hi = CAM.H;
+  j.chunk = 1;
+  j.s = s0;
+  j.spp = spp;
+  j.seed = seed;
+  j.dfilm = dfilm;
+  j.g_alb = g_alb;
+  j.g_em = g_em;
+  run_job(&j, nthreads);
+}

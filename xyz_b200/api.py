@@ -31,7 +31,8 @@ EXPORTED = [
     "xyzgpu_scene_stats_get", "xyzgpu_scene_copy_tree", "xyzgpu_trace_closest",
     "xyzgpu_trace_closest_counted", "xyzgpu_render_params_default", "xyzgpu_render",
     "xyzgpu_render_counters_get", "xyzgpu_render_profile_get", "xyzgpu_render_noalloc",
-    "xyzgpu_philox_u01", "xyzgpu_last_error", "xyzgpu_abi_version",
+    "xyzgpu_philox_u01", "xyzgpu_last_error", "xyzgpu_abi_version", "xyzgpu_adjoint",
+    "xyzgpu_scene_set_materials", "xyzgpu_scene_get_materials",
 ]
 
 
@@ -128,6 +129,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.xyzgpu_render_profile_get.argtypes = [C.c_void_p, C.POINTER(RenderProfile)]
     L.xyzgpu_philox_u01.restype = C.c_float
     L.xyzgpu_philox_u01.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+    L.xyzgpu_adjoint.argtypes = [C.c_void_p, C.POINTER(CameraDesc), C.POINTER(RenderParams), C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p]
+    L.xyzgpu_scene_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    L.xyzgpu_scene_get_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     L.xyzgpu_build_params_default.argtypes = [C.POINTER(BuildParams)]
     L.xyzgpu_render_params_default.argtypes = [C.POINTER(RenderParams)]
     _LIB = L
@@ -147,6 +152,35 @@ def default_build_params(**kw) -> BuildParams:
             v = {"device": XYZGPU_BUILD_DEVICE, "host": XYZGPU_BUILD_HOST}[v]
         setattr(bp, k, v)
     return bp
+
+
+def camera_desc(camera) -> "CameraDesc":
+    cam = CameraDesc()
+    for k in range(3):
+        cam.eye[k] = float(camera.eye[k])
+        cam.at[k] = float(camera.at[k])
+    cam.film_size = float(camera.film_size)
+    cam.focal_length = float(camera.focal_length)
+    cam.f_number = float(camera.f_number)
+    cam.pinhole = int(bool(camera.pinhole))
+    return cam
+
+
+def render_params(width: int, height: int, spp: int, *, seed: int = 0, spp_offset: int = 0,
+                  max_depth: int = 15, rr_start_depth: int = 1, rr_threshold: float = 0.2,
+                  accumulate: bool = False, wave_paths: int = 0, profile: int = 0, spectral="off",
+                  hero_wavelengths: int = 4) -> "RenderParams":
+    rp = RenderParams()
+    load_library().xyzgpu_render_params_default(C.byref(rp))
+    rp.width, rp.height, rp.spp, rp.spp_offset = width, height, spp, spp_offset
+    rp.max_depth, rp.rr_start_depth, rp.rr_threshold = max_depth, rr_start_depth, rr_threshold
+    rp.seed = seed
+    rp.accumulate = int(bool(accumulate))
+    rp.wave_paths = wave_paths
+    rp.profile = profile
+    rp.spectral = SPECTRAL_MODES[spectral] if isinstance(spectral, str) else int(spectral)
+    rp.hero_wavelengths = hero_wavelengths
+    return rp
 
 
 def _stream_ptr(stream) -> Optional[int]:
@@ -270,24 +304,11 @@ class Scene:
         """Renders into `film`: a CUDA tensor (H, W, 3) (device film) or a numpy
         float32 array (host film).  Allocates a CUDA tensor if film is None.
         Returns the film (sums over samples, not means)."""
-        cam = CameraDesc()
-        for k in range(3):
-            cam.eye[k] = float(camera.eye[k])
-            cam.at[k] = float(camera.at[k])
-        cam.film_size = float(camera.film_size)
-        cam.focal_length = float(camera.focal_length)
-        cam.f_number = float(camera.f_number)
-        cam.pinhole = int(bool(camera.pinhole))
-        rp = RenderParams()
-        _LIB.xyzgpu_render_params_default(C.byref(rp))
-        rp.width, rp.height, rp.spp, rp.spp_offset = width, height, spp, spp_offset
-        rp.max_depth, rp.rr_start_depth, rp.rr_threshold = max_depth, rr_start_depth, rr_threshold
-        rp.seed = seed
-        rp.accumulate = int(bool(accumulate))
-        rp.wave_paths = wave_paths
-        rp.profile = profile
-        rp.spectral = SPECTRAL_MODES[spectral] if isinstance(spectral, str) else int(spectral)
-        rp.hero_wavelengths = hero_wavelengths
+        cam = camera_desc(camera)
+        rp = render_params(width, height, spp, seed=seed, spp_offset=spp_offset, max_depth=max_depth,
+                           rr_start_depth=rr_start_depth, rr_threshold=rr_threshold,
+                           accumulate=accumulate, wave_paths=wave_paths, profile=profile,
+                           spectral=spectral, hero_wavelengths=hero_wavelengths)
         if film is None:
             import torch
             film = torch.zeros((height, width, 3), dtype=torch.float32, device="cuda")
@@ -309,21 +330,10 @@ class Scene:
         """xyzgpu_render_noalloc: same image as render(), for callers that cannot
         allocate device memory while rendering.  `film` must be a CUDA tensor
         (H, W, 3) float32 that the caller owns; nothing is allocated."""
-        cam = CameraDesc()
-        for k in range(3):
-            cam.eye[k] = float(camera.eye[k])
-            cam.at[k] = float(camera.at[k])
-        cam.film_size = float(camera.film_size)
-        cam.focal_length = float(camera.focal_length)
-        cam.f_number = float(camera.f_number)
-        cam.pinhole = int(bool(camera.pinhole))
-        rp = RenderParams()
-        _LIB.xyzgpu_render_params_default(C.byref(rp))
-        rp.width, rp.height, rp.spp, rp.spp_offset = width, height, spp, spp_offset
-        rp.max_depth, rp.rr_start_depth, rp.rr_threshold = max_depth, rr_start_depth, rr_threshold
-        rp.seed = seed
-        rp.accumulate = int(bool(accumulate))
-        rp.wave_paths = wave_paths
+        cam = camera_desc(camera)
+        rp = render_params(width, height, spp, seed=seed, spp_offset=spp_offset, max_depth=max_depth,
+                           rr_start_depth=rr_start_depth, rr_threshold=rr_threshold,
+                           accumulate=accumulate, wave_paths=wave_paths)
         rp.film_location = XYZGPU_FILM_DEVICE
         _check(_LIB.xyzgpu_render_noalloc(self.handle, C.byref(cam), C.byref(rp), film.data_ptr(),
                                           _stream_ptr(stream)))
@@ -345,6 +355,65 @@ class Scene:
         _check(_LIB.xyzgpu_render_counters_get(self.handle, C.byref(c)))
         return {f: getattr(c, f) for f, _ in RenderCounters._fields_}
 
+    # -- differentiable rendering ----------------------------------------
+    def set_materials(self, albedo_xyz=None, emission=None, stream=None):
+        """xyzgpu_scene_set_materials: albedo (n_materials, 3) and / or emission
+        scale (n_materials,), as numpy arrays (host) or CUDA float32 tensors
+        (device; read on `stream`)."""
+        a, e = albedo_xyz, emission
+        on_device = any(x is not None and not isinstance(x, np.ndarray) for x in (a, e))
+        if on_device:
+            for x in (a, e):
+                if x is not None:
+                    assert x.is_cuda and str(x.dtype) == "torch.float32" and x.is_contiguous()
+            _check(_LIB.xyzgpu_scene_set_materials(self.handle, None if a is None else a.data_ptr(),
+                                                   None if e is None else e.data_ptr(), XYZGPU_FILM_DEVICE,
+                                                   _stream_ptr(stream)))
+            return
+        keep = []
+        ptrs = []
+        for x in (a, e):
+            if x is None:
+                ptrs.append(None)
+            else:
+                x = np.ascontiguousarray(x, np.float32)
+                keep.append(x)
+                ptrs.append(x.ctypes.data)
+        _check(_LIB.xyzgpu_scene_set_materials(self.handle, ptrs[0], ptrs[1], XYZGPU_FILM_HOST,
+                                               _stream_ptr(stream)))
+
+    def get_materials(self):
+        """Current (albedo (n_materials, 3), emission scale (n_materials,)) as numpy."""
+        nm = int(self.data.albedo_xyz.shape[0])
+        a = np.zeros((nm, 3), np.float32)
+        e = np.zeros(nm, np.float32)
+        _check(_LIB.xyzgpu_scene_get_materials(self.handle, a.ctypes.data, e.ctypes.data))
+        return a, e
+
+    def adjoint(self, camera, width: int, height: int, spp: int, d_film, *, seed: int = 0,
+                spp_offset: int = 0, max_depth: int = 15, rr_start_depth: int = 1,
+                rr_threshold: float = 0.2, wave_paths: int = 0, d_albedo=None, d_emission=None,
+                stream=None):
+        """xyzgpu_adjoint: gradient of sum(d_film * film) with respect to the
+        materials' albedo and emission scale, for the film render() gives with the
+        same arguments.  d_film: CUDA float32 tensor (H, W, 3).  Returns
+        (d_albedo (n_materials, 3), d_emission (n_materials,)) CUDA tensors
+        (accumulated into the given ones)."""
+        import torch
+        nm = int(self.data.albedo_xyz.shape[0])
+        if d_albedo is None:
+            d_albedo = torch.zeros((nm, 3), dtype=torch.float32, device=d_film.device)
+        if d_emission is None:
+            d_emission = torch.zeros(nm, dtype=torch.float32, device=d_film.device)
+        assert d_film.is_cuda and d_film.is_contiguous() and tuple(d_film.shape) == (height, width, 3)
+        cam = camera_desc(camera)
+        rp = render_params(width, height, spp, seed=seed, spp_offset=spp_offset, max_depth=max_depth,
+                           rr_start_depth=rr_start_depth, rr_threshold=rr_threshold, wave_paths=wave_paths)
+        _check(_LIB.xyzgpu_adjoint(self.handle, C.byref(cam), C.byref(rp), d_film.data_ptr(),
+                                   d_albedo.data_ptr(), d_emission.data_ptr(), _stream_ptr(stream)))
+        return d_albedo, d_emission
+
 
 def philox_u01(seed: int, pixel: int, sample: int, dim: int) -> float:
     return load_library().xyzgpu_philox_u01(seed, pixel, sample, dim)
+

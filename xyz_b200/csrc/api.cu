@@ -83,7 +83,7 @@ void free_scene(SceneImpl *s) {
   // work queued on any stream that still reads the scene finishes first
   cudaDeviceSynchronize();
   render_workspace_free(s->ws);
-  void *bufs[] = {s->d_tri, s->d_ng, s->d_sn, s->d_mat, s->d_lights, s->d_cdf, s->d_spd,
+  void *bufs[] = {s->d_tri, s->d_ng, s->d_sn, s->d_mat, s->d_emission, s->d_lights, s->d_cdf, s->d_spd,
                   s->d_nodes, s->d_refs, s->d_fetch, s->d_trace_counts};
   for (void *b : bufs)
     if (b) cudaFreeAsync(b, nullptr);
@@ -169,6 +169,31 @@ int check_device(int *dev) {
   if (major != 10)
     return set_error(XYZGPU_E_NODEVICE, "device %d has compute capability %d.x; this library is built for sm_100a",
                      *dev, major);
+  return XYZGPU_OK;
+}
+
+// Material table update from device arrays: albedo (3 per material) into the
+// xyz of the float4 records, emission scale copied as is.
+__global__ void k_set_materials(float4 *__restrict__ mat, float *__restrict__ emission,
+                                const float *__restrict__ albedo_in, const float *__restrict__ emission_in,
+                                int nm) {
+  int const m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nm) return;
+  if (albedo_in) {
+    float4 r = mat[m];
+    r.x = albedo_in[3 * m];
+    r.y = albedo_in[3 * m + 1];
+    r.z = albedo_in[3 * m + 2];
+    mat[m] = r;
+  }
+  if (emission_in) emission[m] = emission_in[m];
+}
+
+int materials_device_update(SceneImpl &s, const float *albedo_xyz, const float *emission, cudaStream_t st) {
+  if (!albedo_xyz && !emission) return XYZGPU_OK;
+  int const nm = s.n_materials;
+  k_set_materials<<<(nm + 255) / 256, 256, 0, st>>>(s.d_mat, s.d_emission, albedo_xyz, emission, nm);
+  XYZ_CUDA_TRY(cudaGetLastError());
   return XYZGPU_OK;
 }
 
@@ -319,6 +344,11 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   XYZ_TRY(dev_alloc(&s->d_ng, static_cast<size_t>(nt), &bytes, st));
   if (smooth) XYZ_TRY(dev_alloc(&s->d_sn, 3 * static_cast<size_t>(nt), &bytes, st));
   XYZ_TRY(dev_upload(&s->d_mat, mat.data(), mat.size(), &bytes, st));
+  {
+    std::vector<float> ones(mat.size(), 1.0f);
+    XYZ_TRY(dev_upload(&s->d_emission, ones.data(), ones.size(), &bytes, st));
+    // the upload's source is pageable host memory: the copy has completed on return
+  }
   XYZ_TRY(dev_upload(&s->d_lights, lights.data(), lights.size(), &bytes, st));
   XYZ_TRY(dev_upload(&s->d_cdf, cdf.data(), cdf.size(), &bytes, st));
   if (d->albedo_spd) XYZ_TRY(dev_upload(&s->d_spd, d->albedo_spd, 31 * static_cast<size_t>(nm), &bytes, st));
@@ -420,6 +450,7 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   v.tri_ng = s->d_ng;
   v.tri_sn = s->d_sn;
   v.mat = s->d_mat;
+  v.emission = s->d_emission;
   v.lights = s->d_lights;
   v.cdf = s->d_cdf;
   v.nodes = s->d_nodes;
@@ -495,31 +526,120 @@ int xyzgpu_trace_closest_counted(xyzgpu_scene scene, const float *rays, int n, f
                           static_cast<cudaStream_t>(stream), counters);
 }
 
-int xyzgpu_render(xyzgpu_scene scene, const xyzgpu_camera *cam, const xyzgpu_render_params *rp,
-                  float *film, void *stream) {
-  clear_error();
-  if (!scene || !cam || !rp || !film) return set_error(XYZGPU_E_INVALID, "render: null argument");
+namespace {
+// Checks shared by xyzgpu_render and xyzgpu_adjoint.
+int check_render_args(const char *who, xyzgpu_scene scene, const xyzgpu_camera *cam,
+                      const xyzgpu_render_params *rp) {
   if (rp->width <= 0 || rp->height <= 0 || rp->spp < 0 || rp->spp_offset < 0 ||
       rp->max_depth < 1 || rp->max_depth > 1000 || rp->rr_start_depth < 1 ||
       !(rp->rr_threshold >= 0.0f) || rp->wave_paths < 0 || rp->profile < 0 || rp->profile > 2 ||
       rp->spectral < 0 || rp->spectral > 2 ||
       (rp->spectral && (rp->hero_wavelengths < 1 || rp->hero_wavelengths > 4)) ||
       (rp->film_location != XYZGPU_FILM_DEVICE && rp->film_location != XYZGPU_FILM_HOST))
-    return set_error(XYZGPU_E_INVALID, "render: parameters out of range");
+    return set_error(XYZGPU_E_INVALID, "%s: parameters out of range", who);
   if (static_cast<int64_t>(rp->width) * rp->height >= (1ll << 31))
-    return set_error(XYZGPU_E_LIMIT, "render: image of %d x %d pixels exceeds 2^31", rp->width,
+    return set_error(XYZGPU_E_LIMIT, "%s: image of %d x %d pixels exceeds 2^31", who, rp->width,
                      rp->height);
   if (static_cast<int64_t>(rp->spp_offset) + rp->spp >= (1ll << 32))
-    return set_error(XYZGPU_E_LIMIT, "render: sample index exceeds 2^32");
+    return set_error(XYZGPU_E_LIMIT, "%s: sample index exceeds 2^32", who);
   for (int k = 0; k < 3; ++k)
     if (!std::isfinite(cam->eye[k]) || !std::isfinite(cam->at[k]))
-      return set_error(XYZGPU_E_INVALID, "render: camera position is not finite");
+      return set_error(XYZGPU_E_INVALID, "%s: camera position is not finite", who);
   if (!(cam->film_size > 0) || !(cam->focal_length > 0) || !(cam->f_number > 0))
-    return set_error(XYZGPU_E_INVALID, "render: camera film size, focal length and F-number must be > 0");
+    return set_error(XYZGPU_E_INVALID, "%s: camera film size, focal length and F-number must be > 0", who);
   if (rp->spectral && !reinterpret_cast<SceneImpl *>(scene)->d_spd)
-    return set_error(XYZGPU_E_INVALID, "render: the spectral film modes need albedo spectra in the scene");
+    return set_error(XYZGPU_E_INVALID, "%s: the spectral film modes need albedo spectra in the scene", who);
+  return XYZGPU_OK;
+}
+}  // namespace
+
+int xyzgpu_render(xyzgpu_scene scene, const xyzgpu_camera *cam, const xyzgpu_render_params *rp,
+                  float *film, void *stream) {
+  clear_error();
+  if (!scene || !cam || !rp || !film) return set_error(XYZGPU_E_INVALID, "render: null argument");
+  int const rc = check_render_args("render", scene, cam, rp);
+  if (rc) return rc;
   return render_launch(*reinterpret_cast<SceneImpl *>(scene), *cam, *rp, film,
                        static_cast<cudaStream_t>(stream));
+}
+
+int xyzgpu_adjoint(xyzgpu_scene scene, const xyzgpu_camera *cam, const xyzgpu_render_params *rp,
+                   const float *d_film, float *d_albedo, float *d_emission, void *stream) {
+  clear_error();
+  if (!scene || !cam || !rp || !d_film || !d_albedo || !d_emission)
+    return set_error(XYZGPU_E_INVALID, "adjoint: null argument");
+  int const rc = check_render_args("adjoint", scene, cam, rp);
+  if (rc) return rc;
+  if (rp->spectral != XYZGPU_SPECTRAL_OFF)
+    return set_error(XYZGPU_E_INVALID, "adjoint: only the XYZ film mode is differentiated");
+  if (rp->profile != XYZGPU_PROFILE_OFF)
+    return set_error(XYZGPU_E_INVALID, "adjoint: profiling is not supported");
+  if ((reinterpret_cast<uintptr_t>(d_film) | reinterpret_cast<uintptr_t>(d_albedo) |
+       reinterpret_cast<uintptr_t>(d_emission)) & 3u)
+    return set_error(XYZGPU_E_INVALID, "adjoint: buffers must be 4-byte aligned");
+  AdjointArgs adj{d_film, d_albedo, d_emission};
+  return render_launch(*reinterpret_cast<SceneImpl *>(scene), *cam, *rp, nullptr,
+                       static_cast<cudaStream_t>(stream), &adj);
+}
+
+int xyzgpu_scene_set_materials(xyzgpu_scene scene, const float *albedo_xyz, const float *emission,
+                               int location, void *stream) {
+  clear_error();
+  if (!scene) return set_error(XYZGPU_E_INVALID, "scene_set_materials: null scene");
+  if (location != XYZGPU_FILM_DEVICE && location != XYZGPU_FILM_HOST)
+    return set_error(XYZGPU_E_INVALID, "scene_set_materials: unknown location %d", location);
+  SceneImpl &s = *reinterpret_cast<SceneImpl *>(scene);
+  cudaStream_t const st = static_cast<cudaStream_t>(stream);
+  XYZ_CUDA_TRY(cudaSetDevice(s.device));
+  int const nm = s.n_materials;
+  if (nm == 0) return XYZGPU_OK;
+  if (location == XYZGPU_FILM_HOST) {
+    // host values are checked and copied synchronously
+    if (albedo_xyz) {
+      std::vector<float4> mat(nm);
+      XYZ_CUDA_TRY(cudaMemcpyAsync(mat.data(), s.d_mat, nm * sizeof(float4), cudaMemcpyDeviceToHost, st));
+      XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+      for (int m = 0; m < nm; ++m) {
+        for (int c = 0; c < 3; ++c)
+          if (!std::isfinite(albedo_xyz[3 * m + c]))
+            return set_error(XYZGPU_E_INVALID, "scene_set_materials: albedo of material %d is not finite", m);
+        mat[m].x = albedo_xyz[3 * m];
+        mat[m].y = albedo_xyz[3 * m + 1];
+        mat[m].z = albedo_xyz[3 * m + 2];
+      }
+      XYZ_CUDA_TRY(cudaMemcpyAsync(s.d_mat, mat.data(), nm * sizeof(float4), cudaMemcpyHostToDevice, st));
+      XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    if (emission) {
+      for (int m = 0; m < nm; ++m)
+        if (!std::isfinite(emission[m]))
+          return set_error(XYZGPU_E_INVALID, "scene_set_materials: emission of material %d is not finite", m);
+      XYZ_CUDA_TRY(cudaMemcpyAsync(s.d_emission, emission, nm * sizeof(float), cudaMemcpyHostToDevice, st));
+      XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return XYZGPU_OK;
+  }
+  return materials_device_update(s, albedo_xyz, emission, st);
+}
+
+int xyzgpu_scene_get_materials(xyzgpu_scene scene, float *albedo_xyz, float *emission) {
+  clear_error();
+  if (!scene) return set_error(XYZGPU_E_INVALID, "scene_get_materials: null scene");
+  SceneImpl &s = *reinterpret_cast<SceneImpl *>(scene);
+  XYZ_CUDA_TRY(cudaSetDevice(s.device));
+  int const nm = s.n_materials;
+  if (nm == 0) return XYZGPU_OK;
+  if (albedo_xyz) {
+    std::vector<float4> mat(nm);
+    XYZ_CUDA_TRY(cudaMemcpy(mat.data(), s.d_mat, nm * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (int m = 0; m < nm; ++m) {
+      albedo_xyz[3 * m] = mat[m].x;
+      albedo_xyz[3 * m + 1] = mat[m].y;
+      albedo_xyz[3 * m + 2] = mat[m].z;
+    }
+  }
+  if (emission) XYZ_CUDA_TRY(cudaMemcpy(emission, s.d_emission, nm * sizeof(float), cudaMemcpyDeviceToHost));
+  return XYZGPU_OK;
 }
 
 int xyzgpu_render_noalloc(xyzgpu_scene scene, const xyzgpu_camera *cam,

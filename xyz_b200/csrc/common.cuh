@@ -110,6 +110,7 @@ struct DevScene {
   const float4 *tri_ng;   // (normalize(n), material id bits)
   const float4 *tri_sn;   // 3 per triangle: shading n0, s1 = n1 - n0, s2 = n2 - n0 (or null)
   const float4 *mat;      // (albedo xyz, 1 = light)
+  const float *emission;  // per-material scale of the light's emitted power (1 by default)
   const int32_t *lights;  // light triangle ids, triangle order
   const float *cdf;       // n_lights + 1 prefix sums of light areas, cdf[0] = 0
   const uint2 *nodes;

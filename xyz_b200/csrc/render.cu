@@ -82,6 +82,12 @@ struct WaveArgs {
   uint32_t wl_dim;  // dimension of the hero wavelength draw
   float *fsn;
   int32_t *s_slot;
+  // path-replay adjoint (xyzgpu_adjoint): each path's radiance from the primal
+  // pass, dLoss/dfilm, and the gradient accumulators
+  float4 *ltot;
+  const float *dfilm;
+  float *g_alb;
+  float *g_em;
 };
 
 XYZ_DEV uint32_t pack_misc(uint32_t dim, uint32_t k, uint32_t specular) {
@@ -199,7 +205,7 @@ struct ExtSink {
   }
 };
 
-template <bool kSpec>
+template <bool kSpec, bool kAdj>
 struct ShadowSink {
   const WaveArgs *A;
   uint32_t visible;
@@ -219,8 +225,24 @@ struct ShadowSink {
     float const dens = dimp / dexp;
     double const wgt = (static_cast<double>(G) * (kInvPi * kInvPi)) *
                        static_cast<double>(1.0f / (1.0f + dens * dens));
-    float4 const pb = A->s_pb[i];
+    float4 pb = A->s_pb[i];
     int32_t const slot = kSpec ? A->s_slot[i] : __float_as_int(pb.w);
+    if (kAdj) {
+      // replay: pb is the unit-emission power; the light's scale is applied
+      // here and the unit contribution goes to that light's emission gradient
+      int32_t const ml = A->s_slot[i];
+      float const e = __ldg(&A->S.emission[ml]);
+      uint32_t pixel, sample;
+      slot_to_pixel_sample(*A, slot, &pixel, &sample);
+      float const *df = A->dfilm + 3 * static_cast<int64_t>(pixel);
+      float const g = df[0] * static_cast<float>(static_cast<double>(pb.x) * wgt) +
+                      df[1] * static_cast<float>(static_cast<double>(pb.y) * wgt) +
+                      df[2] * static_cast<float>(static_cast<double>(pb.z) * wgt);
+      if (g != 0.0f) atomicAdd(&A->g_em[ml], g);
+      pb.x *= e;
+      pb.y *= e;
+      pb.z *= e;
+    }
     float4 L = A->radiance[slot];
     L.x += static_cast<float>(static_cast<double>(pb.x) * wgt);
     L.y += static_cast<float>(static_cast<double>(pb.y) * wgt);
@@ -231,7 +253,7 @@ struct ShadowSink {
   }
 };
 
-template <bool kShadow, bool kCount>
+template <bool kShadow, bool kCount, bool kAdj = false>
 __global__ void __launch_bounds__(kThreads) k_trace_queue(WaveArgs A, int b,
                                                           unsigned long long *prof) {
   int32_t *const cnt = A.counts + b * kCountStride;
@@ -240,12 +262,16 @@ __global__ void __launch_bounds__(kThreads) k_trace_queue(WaveArgs A, int b,
   int const qi = b & 1;
   TraceCount tc{0u, 0u, 0u};
   uint32_t visible = 0;
-  if (kShadow && A.spectral) {
-    ShadowSink<true> sink{&A, 0u};
+  if (kShadow && kAdj) {
+    ShadowSink<false, true> sink{&A, 0u};
+    trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
+    visible = sink.visible;
+  } else if (kShadow && A.spectral) {
+    ShadowSink<true, false> sink{&A, 0u};
     trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
     visible = sink.visible;
   } else if (kShadow) {
-    ShadowSink<false> sink{&A, 0u};
+    ShadowSink<false, false> sink{&A, 0u};
     trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
     visible = sink.visible;
   } else {
@@ -295,6 +321,7 @@ __global__ void k_tally(WaveArgs A, int iters, unsigned long long *tally) {
 // ------------------------------------------------------------------ shade
 struct LightSample {
   f3 pos, sn, gn;
+  int32_t mat;  // the light triangle's material
 };
 
 // Scene::SampleLightPosition + Triangle::Sample (scene.cpp:42-78,
@@ -327,6 +354,7 @@ XYZ_DEV LightSample sample_light(const DevScene &S, uint64_t seed, uint32_t pixe
   L.pos = add3(add3(xyz3(a), scl3(xyz3(b), uu)), scl3(xyz3(c), vv));
   float4 const g4 = __ldg(&S.tri_ng[li]);
   L.gn = xyz3(g4);
+  L.mat = __float_as_int(g4.w);
   if (S.tri_sn) {
     f3 const n0 = xyz3(__ldg(&S.tri_sn[3 * li])), s1 = xyz3(__ldg(&S.tri_sn[3 * li + 1])),
              s2 = xyz3(__ldg(&S.tri_sn[3 * li + 2]));
@@ -338,6 +366,8 @@ XYZ_DEV LightSample sample_light(const DevScene &S, uint64_t seed, uint32_t pixe
   return L;
 }
 
+// kAdj: the replay pass of xyzgpu_adjoint (same path, plus gradients).
+template <bool kAdj>
 __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
   int32_t *const cnt = A.counts + b * kCountStride;
   int32_t *const cnt_next = A.counts + (b + 1) * kCountStride;
@@ -355,6 +385,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
     float nk2nk3 = 0.0f;
     float4 beta4{};
     uint32_t misc = 0;
+    int32_t light_mat = 0;
     if (i < n) {
       slot = A.q_slot[qi][i];
       float4 const h = A.hits[i];
@@ -402,8 +433,12 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
           uint32_t const specular = misc >> 31;
           bool alive = true;
           if (is_light && !back) {
-            // emitter hit (scene_pathtracing.cpp:84-111)
-            f3 const pb = mul3(S.power, beta);
+            // emitter hit (scene_pathtracing.cpp:84-111); the material's
+            // emission scale multiplies the light's power (1 unless set)
+            f3 pb = mul3(S.power, beta);
+            float const e = __ldg(&S.emission[m]);
+            f3 const pb_unit = pb;
+            pb = scl3(pb, e);
             double const wl = kInvPi / static_cast<double>(S.light_area);
             double mis = 1.0;
             if (!specular) {
@@ -413,6 +448,16 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
               float const dexp = 1.0f / S.light_area;
               float const dens = dexp / dimp;
               mis = static_cast<double>(1.0f / (1.0f + dens * dens));
+            }
+            if (kAdj) {
+              double const w = specular ? wl : wl * mis;
+              uint32_t px, smp;
+              slot_to_pixel_sample(A, slot, &px, &smp);
+              float const *df = A.dfilm + 3 * static_cast<int64_t>(px);
+              float const g = df[0] * static_cast<float>(static_cast<double>(pb_unit.x) * w) +
+                              df[1] * static_cast<float>(static_cast<double>(pb_unit.y) * w) +
+                              df[2] * static_cast<float>(static_cast<double>(pb_unit.z) * w);
+              if (g != 0.0f) atomicAdd(&A.g_em[m], g);
             }
             float4 L = A.radiance[slot];
             if (specular) {
@@ -437,6 +482,17 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
             if (!is_light) {
               // next-event estimation (lambert.cpp:125-156)
               beta = mul3(beta, xyz3(m4));
+              if (kAdj) {
+                // Every contribution from here on carries this vertex's albedo
+                // once: d/d albedo_c = (L_total - L_so_far)_c / albedo_c.
+                float4 const lt = A.ltot[slot], lr = A.radiance[slot];
+                float const *df = A.dfilm + 3 * static_cast<int64_t>(pixel);
+                float const gx = df[0] * (lt.x - lr.x), gy = df[1] * (lt.y - lr.y),
+                            gz = df[2] * (lt.z - lr.z);
+                if (gx != 0.0f && m4.x != 0.0f) atomicAdd(&A.g_alb[3 * m], gx / m4.x);
+                if (gy != 0.0f && m4.y != 0.0f) atomicAdd(&A.g_alb[3 * m + 1], gy / m4.y);
+                if (gz != 0.0f && m4.z != 0.0f) atomicAdd(&A.g_alb[3 * m + 2], gz / m4.z);
+              }
               if (S.n_lights > 0) {
                 LightSample const ls = sample_light(S, A.seed, pixel, sample);
                 f3 const v = normalize3(sub3(pos, ls.pos));
@@ -449,6 +505,8 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
                     vin = v;
                     nk2nk3 = nk2 * nk3;
                     pbv = mul3(S.power, beta);
+                    light_mat = ls.mat;
+                    if (!kAdj) pbv = scl3(pbv, __ldg(&S.emission[ls.mat]));
                   }
                 }
               }
@@ -496,6 +554,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
       A.s_d[js] = make_float4(vin.x, vin.y, vin.z, nk2nk3);
       A.s_pb[js] = make_float4(pbv.x, pbv.y, pbv.z, __int_as_float(slot));
       A.s_target[js] = tri;
+      if (kAdj) A.s_slot[js] = light_mat;
     }
     int32_t const je = warp_append(&cnt_next[kCExt], push_ext);
     if (push_ext) {
@@ -618,7 +677,9 @@ __global__ void __launch_bounds__(kThreads) k_shade_spectral(WaveArgs A, int b) 
           bool alive = true;
           if (is_light && !back) {
             // SceneStrategy.cpp:100-120
-            float4 const pb = mul4(phi, beta);
+            float const e = __ldg(&S.emission[m]);
+            float4 pb = mul4(phi, beta);
+            pb = make_float4(pb.x * e, pb.y * e, pb.z * e, pb.w * e);
             double const wl = kInvPi / static_cast<double>(S.light_area);
             double mis = 1.0;
             if (!specular) {
@@ -653,6 +714,8 @@ __global__ void __launch_bounds__(kThreads) k_shade_spectral(WaveArgs A, int b) 
                     vin = v;
                     nk2nk3 = nk2 * nk3;
                     pb4 = mul4(phi, beta);
+                    float const e = __ldg(&S.emission[ls.mat]);
+                    pb4 = make_float4(pb4.x * e, pb4.y * e, pb4.z * e, pb4.w * e);
                   }
                 }
               }
@@ -771,6 +834,13 @@ __global__ void __launch_bounds__(kThreads) k_film(WaveArgs A, float *__restrict
   }
 }
 
+// Adjoint: keeps each path's primal radiance for the replay pass.
+__global__ void __launch_bounds__(kThreads) k_adj_stash(WaveArgs A) {
+  int64_t const stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < A.npaths; i += stride)
+    A.ltot[i] = A.radiance[i];
+}
+
 template <class K>
 int occupancy_grid(K kernel, int device) {
   int per_sm = 0;
@@ -879,7 +949,7 @@ void render_workspace_free(RenderWorkspace &w) {
 }
 
 int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp, float *film,
-                  cudaStream_t st) {
+                  cudaStream_t st, const AdjointArgs *adj) {
   XYZ_CUDA_TRY(cudaSetDevice(s.device));
   int64_t const npix_total = static_cast<int64_t>(rp.width) * rp.height;
   int64_t const film_elems = 3 * npix_total;
@@ -928,7 +998,7 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   if (rc) return rc;
   if (!sw.done) XYZ_CUDA_TRY(cudaEventCreateWithFlags(&sw.done, cudaEventDisableTiming));
   RenderWorkspace const &wv = sw.ws;
-  if (rp.film_location == XYZGPU_FILM_HOST) {
+  if (!adj && rp.film_location == XYZGPU_FILM_HOST) {
     if (w.film_elems < film_elems) {
       cudaFree(w.film_dev);
       cudaFreeHost(w.film_pinned);
@@ -946,14 +1016,30 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
                                    cudaMemcpyHostToDevice, st));
     }
   }
-  if (!rp.accumulate) XYZ_CUDA_TRY(cudaMemsetAsync(film_dev, 0, film_elems * sizeof(float), st));
+  if (!adj && !rp.accumulate) XYZ_CUDA_TRY(cudaMemsetAsync(film_dev, 0, film_elems * sizeof(float), st));
+  float4 *ltot = nullptr;
+  if (adj) {
+    cudaError_t const e = cudaMallocAsync(reinterpret_cast<void **>(&ltot), static_cast<size_t>(cap) * sizeof(float4), st);
+    if (e != cudaSuccess)
+      return set_error(e == cudaErrorMemoryAllocation ? XYZGPU_E_NOMEM : XYZGPU_E_CUDA,
+                       "adjoint: allocating the primal radiance of %lld paths failed: %s",
+                       static_cast<long long>(cap), cudaGetErrorString(e));
+  }
+  // frees the adjoint's buffer on every return below
+  struct FreeAsync {
+    float4 *p;
+    cudaStream_t st;
+    ~FreeAsync() {
+      if (p) cudaFreeAsync(p, st);
+    }
+  } ltot_guard{ltot, st};
 
   static int g_raygen = 0, g_trace_e = 0, g_trace_s = 0, g_shade = 0, g_film = 0, g_shade_sp = 0;
   if (!g_raygen) {
     g_raygen = occupancy_grid(k_raygen, s.device);
     g_trace_e = occupancy_grid(k_trace_queue<false, false>, s.device);
     g_trace_s = occupancy_grid(k_trace_queue<true, false>, s.device);
-    g_shade = occupancy_grid(k_shade, s.device);
+    g_shade = occupancy_grid(k_shade<false>, s.device);
     g_shade_sp = occupancy_grid(k_shade_spectral, s.device);
     g_film = occupancy_grid(k_film, s.device);
   }
@@ -1008,6 +1094,12 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   A.wl_dim = cam.pinhole ? 4u : 6u;
   A.fsn = wv.fsn;
   A.s_slot = wv.s_slot;
+  if (adj) {
+    A.ltot = ltot;
+    A.dfilm = adj->d_film;
+    A.g_alb = adj->g_albedo;
+    A.g_em = adj->g_emission;
+  }
 
   xyzgpu_render_counters rc_out{};
   uint64_t launches = 0;
@@ -1029,41 +1121,62 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
     int const m_ = mark((cls), (start));  \
     if (m_) return m_;                    \
   } while (0)
-      XYZ_MARK(0, true);
-      k_raygen<<<gr, kThreads, 0, st>>>(A);
-      XYZ_MARK(0, false);
-      ++launches;
-      for (int b = 0; b < iters; ++b) {
-        XYZ_MARK(1, true);
-        if (counting)
-          k_trace_queue<false, true><<<g_trace_e, kThreads, 0, st>>>(A, b, pc);
-        else
-          k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, pc);
-        XYZ_MARK(1, false);
-        XYZ_MARK(2, true);
-        if (spectral)
-          k_shade_spectral<<<g_shade_sp, kThreads, 0, st>>>(A, b);
-        else
-          k_shade<<<g_shade, kThreads, 0, st>>>(A, b);
-        XYZ_MARK(2, false);
-        XYZ_MARK(3, true);
-        if (counting)
-          k_trace_queue<true, true><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
-        else
-          k_trace_queue<true, false><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
-        XYZ_MARK(3, false);
-        launches += 3;
-      }
+      // One pass over the wave: camera rays, then per bounce closest hit,
+      // shading and shadow rays.  The adjoint runs it twice (primal, replay).
+      auto pass = [&](bool replay) -> int {
+        XYZ_MARK(0, true);
+        k_raygen<<<gr, kThreads, 0, st>>>(A);
+        XYZ_MARK(0, false);
+        ++launches;
+        for (int b = 0; b < iters; ++b) {
+          XYZ_MARK(1, true);
+          if (counting)
+            k_trace_queue<false, true><<<g_trace_e, kThreads, 0, st>>>(A, b, pc);
+          else
+            k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, pc);
+          XYZ_MARK(1, false);
+          XYZ_MARK(2, true);
+          if (spectral)
+            k_shade_spectral<<<g_shade_sp, kThreads, 0, st>>>(A, b);
+          else if (replay)
+            k_shade<true><<<g_shade, kThreads, 0, st>>>(A, b);
+          else
+            k_shade<false><<<g_shade, kThreads, 0, st>>>(A, b);
+          XYZ_MARK(2, false);
+          XYZ_MARK(3, true);
+          if (counting)
+            k_trace_queue<true, true><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
+          else if (replay)
+            k_trace_queue<true, false, true><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
+          else
+            k_trace_queue<true, false><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
+          XYZ_MARK(3, false);
+          launches += 3;
+        }
+        return XYZGPU_OK;
+      };
+      int const pr = pass(false);
+      if (pr) return pr;
       int const gf = static_cast<int>(std::min<int64_t>(g_film, (A.npix + kThreads - 1) / kThreads));
-      XYZ_MARK(4, true);
-      if (spectral)
-        k_film_spectral<<<gf, kThreads, 0, st>>>(A, film_dev);
-      else
-        k_film<<<gf, kThreads, 0, st>>>(A, film_dev);
-      XYZ_MARK(4, false);
+      if (adj) {
+        int const gs = static_cast<int>(std::min<int64_t>(g_film, (A.npaths + kThreads - 1) / kThreads));
+        k_adj_stash<<<gs, kThreads, 0, st>>>(A);
+        ++launches;
+        XYZ_CUDA_TRY(cudaMemsetAsync(wv.counts, 0, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t), st));
+        int const rr = pass(true);
+        if (rr) return rr;
+      } else {
+        XYZ_MARK(4, true);
+        if (spectral)
+          k_film_spectral<<<gf, kThreads, 0, st>>>(A, film_dev);
+        else
+          k_film<<<gf, kThreads, 0, st>>>(A, film_dev);
+        XYZ_MARK(4, false);
+        ++launches;
+      }
 #undef XYZ_MARK
       k_tally<<<1, 32, 0, st>>>(A, iters, w.tally);
-      launches += 2;
+      ++launches;
       XYZ_CUDA_TRY(cudaGetLastError());
       rc_out.paths += static_cast<uint64_t>(A.npaths);
       rc_out.waves += 1;
@@ -1071,7 +1184,7 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   }
   XYZ_CUDA_TRY(cudaEventRecord(sw.done, st));
   sw.last = st;
-  if (rp.film_location == XYZGPU_FILM_HOST) {
+  if (!adj && rp.film_location == XYZGPU_FILM_HOST) {
     XYZ_CUDA_TRY(cudaMemcpyAsync(w.film_pinned, film_dev, film_elems * sizeof(float), cudaMemcpyDeviceToHost, st));
     XYZ_CUDA_TRY(cudaStreamSynchronize(st));
     std::memcpy(film, w.film_pinned, film_elems * sizeof(float));
@@ -1270,7 +1383,7 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
     g_raygen = occupancy_grid(k_raygen, s.device);
     g_trace_e = occupancy_grid(k_trace_queue<false, false>, s.device);
     g_trace_s = occupancy_grid(k_trace_queue<true, false>, s.device);
-    g_shade = occupancy_grid(k_shade, s.device);
+    g_shade = occupancy_grid(k_shade<false>, s.device);
     g_film = occupancy_grid(k_film, s.device);
   }
   int64_t const npix_total = static_cast<int64_t>(rp.width) * rp.height;
@@ -1295,7 +1408,7 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
       k_raygen<<<gr, kThreads, 0, st>>>(A);
       for (int b = 0; b < iters; ++b) {
         k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, tally + 8);
-        k_shade<<<g_shade, kThreads, 0, st>>>(A, b);
+        k_shade<false><<<g_shade, kThreads, 0, st>>>(A, b);
         k_trace_queue<true, false><<<g_trace_s, kThreads, 0, st>>>(A, b, tally + 8);
       }
       int const gf = static_cast<int>(std::min<int64_t>(g_film, (A.npix + kThreads - 1) / kThreads));

@@ -59,6 +59,7 @@ struct SceneImpl {
   DevScene dev{};
   // device allocations owned here
   float4 *d_tri = nullptr, *d_ng = nullptr, *d_sn = nullptr, *d_mat = nullptr;
+  float *d_emission = nullptr;  // per-material emission scale, ones at creation
   int32_t *d_lights = nullptr;
   float *d_cdf = nullptr;
   float *d_spd = nullptr;  // 31-bin albedo spectra (spectral modes)
@@ -81,8 +82,16 @@ struct SceneImpl {
 // Kernels' host-side launchers (trace.cu, render.cu, kdbuild.cu).
 int trace_api_launch(SceneImpl &s, const float *rays, int n, float *hits, cudaStream_t st,
                      xyzgpu_trace_counters *counters);
+// Path-replay adjoint of a render (xyzgpu_adjoint): gradients are added to
+// g_albedo (3 per material) and g_emission (1 per material).
+struct AdjointArgs {
+  const float *d_film;  // W * H * 3, device
+  float *g_albedo;
+  float *g_emission;
+};
+
 int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp,
-                  float *film, cudaStream_t st);
+                  float *film, cudaStream_t st, const AdjointArgs *adj = nullptr);
 void render_workspace_free(RenderWorkspace &ws);
 int render_collect(SceneImpl &s);
 int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp,

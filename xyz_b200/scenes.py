@@ -332,6 +332,101 @@ def spheres_scene(level: int = 7, n_spheres: int = 3, seed: int = 0,
     return sd
 
 
+
+def _grid_quad(b: "_Builder", origin, u, v, n: int, m_first: int, front) -> int:
+    """n x n grid of quads spanning origin + [0,1] u + [0,1] v, one material per
+    triangle starting at m_first; returns the next free material id."""
+    o, u, v = (np.asarray(x, dtype=np.float64) for x in (origin, u, v))
+    m = m_first
+    for i in range(n):
+        for j in range(n):
+            p00 = o + u * (i / n) + v * (j / n)
+            p10 = o + u * ((i + 1) / n) + v * (j / n)
+            p11 = o + u * ((i + 1) / n) + v * ((j + 1) / n)
+            p01 = o + u * (i / n) + v * ((j + 1) / n)
+            b.add_tri(p00, p10, p11, m, front)
+            b.add_tri(p00, p11, p01, m + 1, front)
+            m += 2
+    return m
+
+
+@dataclass
+class DiffScene:
+    """A differentiable-rendering workload: the scene (one material per
+    triangle), the initial parameters and the target's parameters."""
+    scene: SceneData
+    albedo: np.ndarray          # (n_materials, 3) float32, initial
+    emission: np.ndarray        # (n_materials,) float32, initial (0 for non-lights)
+    target_albedo: np.ndarray
+    target_emission: np.ndarray
+    light_materials: np.ndarray  # ids of the emitting materials
+
+
+def diff_scene(level: int = 4, wall_n: int = 20, light_n: int = 4, seed: int = 0,
+               target_seed: int = 1, perturb: float = 0.2) -> DiffScene:
+    """Room + 3 displaced spheres with per-triangle parameters.
+
+    The room is the Cornell box's 2 x 2 x 2 m shell (floor, ceiling, back, left,
+    right; open front) with each wall an wall_n x wall_n grid of quads; a
+    0.5 x 0.5 m ceiling light (light_n x light_n quads) 1 mm below the
+    ceiling; three displaced level-`level` icospheres of radius 0.3 on the
+    floor.  Every triangle is its own material.  Albedo: 3 channels (the film's
+    XYZ channels) uniform in [0.1, 0.9]; light triangles: emission scale uniform
+    in [5, 20] on a base radiance of 1 per channel (Phi = pi * A_light).  The
+    target's parameters add uniform noise of +-`perturb` (emission: a relative
+    +-`perturb`) drawn from `target_seed`.  At level 4, wall_n 20 and light_n 4
+    this is 15,360 + 4,000 + 32 = 19,392 triangles."""
+    b = _Builder()
+    m = 0
+    m = _grid_quad(b, (-1, 0, -1), (2, 0, 0), (0, 0, 2), wall_n, m, (0, 1, 0))    # floor
+    m = _grid_quad(b, (-1, 2, -1), (2, 0, 0), (0, 0, 2), wall_n, m, (0, -1, 0))   # ceiling
+    m = _grid_quad(b, (-1, 0, -1), (2, 0, 0), (0, 2, 0), wall_n, m, (0, 0, 1))    # back
+    m = _grid_quad(b, (-1, 0, -1), (0, 2, 0), (0, 0, 2), wall_n, m, (1, 0, 0))    # left
+    m = _grid_quad(b, (1, 0, -1), (0, 2, 0), (0, 0, 2), wall_n, m, (-1, 0, 0))    # right
+    n_walls = m
+    y = 2.0 - 0.001
+    m = _grid_quad(b, (-0.25, y, -0.25), (0.5, 0, 0), (0, 0, 0.5), light_n, m, (0, -1, 0))
+    n_light = m - n_walls
+    pos_r, tris_r, mat_r = b.arrays()
+    nrm_r = np.zeros_like(pos_r)
+    for t in range(tris_r.shape[0]):
+        a, bb, c = pos_r[tris_r[t]].astype(np.float64)
+        n = np.cross(c - a, bb - a)
+        nrm_r[tris_r[t]] = (n / np.linalg.norm(n)).astype(np.float32)
+    pos_l, tri_l, nrm_l, mat_l = [pos_r], [tris_r], [nrm_r], [mat_r]
+    base = pos_r.shape[0]
+    for k, (cx, cz) in enumerate([(-0.45, -0.35), (0.15, 0.35), (0.55, -0.45)]):
+        v, f = displaced_icosphere(level, seed * 31 + k, 0.15)
+        v = v * 0.3 + np.array([cx, 0.36, cz])
+        pos_l.append(v)
+        tri_l.append(f + base)
+        nrm_l.append(vertex_normals(v, f))
+        mat_l.append(np.arange(m, m + f.shape[0], dtype=np.int32))
+        m += f.shape[0]
+        base += v.shape[0]
+    pos = np.concatenate(pos_l).astype(np.float32)
+    tris = np.concatenate(tri_l).astype(np.int32)
+    tri_mat = np.concatenate(mat_l).astype(np.int32)
+    normals = np.concatenate(nrm_l).astype(np.float32)
+    nm = m
+    is_light = np.zeros(nm, np.int32)
+    light_mats = np.arange(n_walls, n_walls + n_light, dtype=np.int32)
+    is_light[light_mats] = 1
+    rng = np.random.default_rng(seed)
+    albedo = rng.uniform(0.1, 0.9, size=(nm, 3)).astype(np.float32)
+    albedo[light_mats] = 0.0
+    emission = np.zeros(nm, np.float32)
+    emission[light_mats] = rng.uniform(5.0, 20.0, size=n_light).astype(np.float32)
+    sd = SceneData(pos, tris, tri_mat, albedo, is_light, np.zeros(3, np.float32), normals=normals,
+                   camera=Camera.with_fov((0.0, 1.0, 3.75), (0.0, 1.0, 0.0), 40.0, pinhole=True),
+                   name=f"diff-room-l{level}")
+    sd.light_power_xyz = np.full(3, np.float32(math.pi * sd.light_area()), np.float32)
+    rt = np.random.default_rng(target_seed)
+    t_alb = np.clip(albedo + rt.uniform(-perturb, perturb, size=albedo.shape), 0.0, 1.0).astype(np.float32)
+    t_alb[light_mats] = 0.0
+    t_em = (emission * (1.0 + rt.uniform(-perturb, perturb, size=nm))).astype(np.float32)
+    return DiffScene(sd, albedo, emission, t_alb, t_em, light_mats)
+
 def random_rays(scene: SceneData, n: int, seed: int = 0):
     """Seeded test rays: origins uniform in the scene box grown by 20 %,
     directions uniform on the sphere.  Returns (org, dir) float32 (n, 3)."""
