@@ -60,7 +60,7 @@ def test_adjoint_matches_oracle_with_russian_roulette_held():
     np.testing.assert_allclose(ge, ge_ref, rtol=2e-3)
 
 
-def _diff_setup(W, H):
+def _diff_setup():
     from xyz_b200 import api, scenes
     ds = scenes.diff_scene()
     s = api.Scene(ds.scene)
@@ -73,10 +73,8 @@ def test_adjoint_matches_central_differences_on_256_parameters():
     target rendered from perturbed parameters; adjoint gradient on the primal's
     own samples vs central differences h = 1e-3 of the same renders, on 256
     random parameters (albedo channels and light emissions)."""
-    import torch
-    from xyz_b200 import api
     W, H, spp, depth = 96, 96, 4, 6
-    ds, s = _diff_setup(W, H)
+    ds, s = _diff_setup()
     cam = ds.scene.camera
     kw = dict(seed=0, max_depth=depth, rr_threshold=0.0)
     try:
@@ -104,7 +102,7 @@ def test_adjoint_matches_central_differences_on_256_parameters():
         params += [("a", int(m), c) for m in mats for c in range(3)][: 256 - len(params)]
         assert len(params) == 256
         h = 1e-3
-        errs, fds, ads = [], [], []
+        fds, ads = [], []
         for kind, m, c in params:
             if kind == "a":
                 a1, a2 = alb.copy(), alb.copy()
@@ -137,7 +135,7 @@ def test_autograd_function_gives_adjoint_gradient_and_descends():
     import torch
     from xyz_b200 import diff
     W, H, spp = 64, 64, 4
-    ds, s = _diff_setup(W, H)
+    ds, s = _diff_setup()
     try:
         R = diff.Renderer(s, ds.scene.camera, W, H, spp, adjoint_offset=0)
         s.set_materials(ds.target_albedo, ds.target_emission)
