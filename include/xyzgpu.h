@@ -287,6 +287,76 @@ int xyzgpu_adjoint(xyzgpu_scene scene, const xyzgpu_camera *camera,
                    const xyzgpu_render_params *rp, const float *d_film, float *d_albedo,
                    float *d_emission, void *stream);
 
+/* Batched rendering: many scenes of different size, resolution and sample count
+ * rendered together.  No counterpart in the reference, which renders one scene
+ * per process.  Every kernel launch serves all jobs at once: one wave of paths
+ * holds runs of consecutive samples of several jobs ("blocks"), and each path
+ * carries its block, so traversal, shading and film kernels fetch the scene,
+ * camera and estimator parameters per path.  A job renders the same film as
+ * xyzgpu_render with its parameters (same paths, same per-pixel sample order).
+ * The launch sequence of the whole batch (all waves) is captured once in a
+ * CUDA graph and replayed by xyzgpu_batch_launch. */
+typedef struct {
+  xyzgpu_scene scene;            /* must outlive the batch */
+  xyzgpu_camera camera;
+  xyzgpu_render_params params;   /* XYZ film mode, profile off; film_location and
+                                    wave_paths are ignored (the film is device memory) */
+  float *film;                   /* device, width * height * 3 sums */
+} xyzgpu_batch_job;
+
+typedef struct {
+  int wave_paths;          /* paths in flight per wave (the queue capacity); 0 = default
+                              (all paths, at most 2^24); at least the largest job's
+                              pixel count */
+  int tile;                /* slot order of a job's pixels: tiles of tile x tile pixels
+                              (1 = scanlines); jobs whose size is not a multiple use 1 */
+  int trace_ctas_per_sm;   /* CTAs per SM of the persistent trace kernels; 0 = the
+                              occupancy maximum */
+  int use_graph;           /* nonzero: replay a captured CUDA graph (default 1) */
+} xyzgpu_batch_config;
+
+typedef struct xyzgpu_batch_s *xyzgpu_batch;
+
+void xyzgpu_batch_config_default(xyzgpu_batch_config *cfg);
+
+/* Plans the waves, allocates the batch's own path buffers and, with use_graph,
+ * captures the launch sequence.  cfg may be NULL (defaults). */
+int xyzgpu_batch_create(const xyzgpu_batch_job *jobs, int n_jobs, const xyzgpu_batch_config *cfg,
+                        xyzgpu_batch *out);
+
+/* Renders every job's spp samples into its film (film zeroed first unless the
+ * job's accumulate is set).  Asynchronous on `stream`. */
+int xyzgpu_batch_launch(xyzgpu_batch batch, void *stream);
+
+/* Sets each job's first sample index (progressive rendering: launch, then move
+ * the offsets by spp, launch again).  Takes effect at the next launch. */
+int xyzgpu_batch_set_sample_offsets(xyzgpu_batch batch, const uint32_t *spp_offsets);
+
+/* Autotuner: times launches of candidate configurations on this batch (tile,
+ * wave size, trace CTAs per SM; coordinate descent from the current one, each
+ * candidate timed `trials` times with CUDA events, best kept) and re-plans with
+ * the winner.  probe_spp > 0 caps every job's samples during the search.  The
+ * films are not touched (scratch films).  Synchronises `stream`. */
+int xyzgpu_batch_autotune(xyzgpu_batch batch, int trials, int probe_spp, void *stream,
+                          xyzgpu_batch_config *chosen);
+
+typedef struct {
+  uint64_t paths, waves, kernel_launches_per_launch, extension_rays, shadow_rays;
+  int64_t device_bytes;     /* path buffers, tables and scratch of the batch */
+  int graph_nodes;          /* nodes of the captured graph (0 without a graph) */
+} xyzgpu_batch_stats;
+
+/* Statistics of the batch; ray counts are those of the last launch (synchronises). */
+int xyzgpu_batch_stats_get(xyzgpu_batch batch, xyzgpu_batch_stats *out);
+
+int xyzgpu_batch_config_get(xyzgpu_batch batch, xyzgpu_batch_config *out);
+
+void xyzgpu_batch_destroy(xyzgpu_batch batch);
+
+/* One-shot form: create, launch, synchronise, destroy. */
+int xyzgpu_render_batch(const xyzgpu_batch_job *jobs, int n_jobs, const xyzgpu_batch_config *cfg,
+                        void *stream);
+
 /* Host evaluation of the random stream defined above (for tests). */
 float xyzgpu_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim);
 

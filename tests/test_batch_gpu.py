@@ -1,0 +1,132 @@
+"""Batched rendering (xyzgpu_batch_*): every job's film equals a single-scene
+xyzgpu_render of the same scene and parameters, bit for bit, whatever the
+wave size, pixel tile, trace grid or graph replay; progressive sample offsets;
+the autotuner; argument checks."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _workload(n=6):
+    from xyz_b200 import scenes
+    entries = []
+    sizes = [(64, 48, 3), (128, 128, 2), (32, 32, 5), (96, 64, 1), (128, 96, 4), (16, 16, 7)]
+    for k in range(n):
+        sd = scenes.batch_scene(k, target_tris=[1500, 4000, 12000, 2500, 30000, 1000][k % 6])
+        w, h, spp = sizes[k % len(sizes)]
+        entries.append((sd, w, h, spp))
+    return entries
+
+
+def _singles(scenes_, entries, seeds, depth=8):
+    out = []
+    for s, (sd, w, h, spp), seed in zip(scenes_, entries, seeds):
+        f = s.render(sd.camera, w, h, spp, seed=seed, max_depth=depth)
+        out.append(f.clone())
+    return out
+
+
+@pytest.mark.parametrize("cfg", [dict(), dict(tile=8), dict(wave_paths=40000),
+                                  dict(wave_paths=20000, tile=4, trace_ctas_per_sm=3),
+                                  dict(use_graph=0, tile=16)])
+def test_batch_films_equal_single_renders(cfg):
+    import torch
+    from xyz_b200 import api
+    entries = _workload()
+    scenes_ = [api.Scene(sd) for sd, *_ in entries]
+    seeds = [11 * k + 1 for k in range(len(entries))]
+    try:
+        ref = _singles(scenes_, entries, seeds)
+        jobs = [api.BatchJob(s, sd.camera, w, h, spp, seed=seed, max_depth=8)
+                for s, (sd, w, h, spp), seed in zip(scenes_, entries, seeds)]
+        with api.Batch(jobs, **cfg) as b:
+            b.launch()
+            torch.cuda.synchronize()
+            st = b.stats()
+            assert st["paths"] == sum(w * h * spp for _, w, h, spp in entries)
+            if cfg.get("wave_paths") == 20000:
+                assert st["waves"] > 3
+            if cfg.get("use_graph", 1):
+                assert st["graph_nodes"] > 0
+            for j, r in zip(jobs, ref):
+                assert torch.equal(j.film.view(torch.int32), r.view(torch.int32))
+            # a second replay gives the same films
+            b.launch()
+            torch.cuda.synchronize()
+            for j, r in zip(jobs, ref):
+                assert torch.equal(j.film.view(torch.int32), r.view(torch.int32))
+    finally:
+        for s in scenes_:
+            s.close()
+
+
+def test_batch_progressive_offsets_accumulate():
+    import torch
+    from xyz_b200 import api
+    entries = _workload(3)
+    scenes_ = [api.Scene(sd) for sd, *_ in entries]
+    try:
+        ref = []
+        for s, (sd, w, h, spp) in zip(scenes_, entries):
+            ref.append(s.render(sd.camera, w, h, 2 * spp, seed=5, max_depth=8).clone())
+        jobs = [api.BatchJob(s, sd.camera, w, h, spp, seed=5, max_depth=8, accumulate=True)
+                for s, (sd, w, h, spp) in zip(scenes_, entries)]
+        with api.Batch(jobs) as b:
+            b.launch()
+            b.set_sample_offsets([spp for _, _, _, spp in entries])
+            b.launch()
+            torch.cuda.synchronize()
+            for j, r in zip(jobs, ref):
+                assert torch.equal(j.film.view(torch.int32), r.view(torch.int32))
+    finally:
+        for s in scenes_:
+            s.close()
+
+
+def test_autotune_picks_a_configuration_and_keeps_films_exact():
+    import torch
+    from xyz_b200 import api
+    entries = _workload()
+    scenes_ = [api.Scene(sd) for sd, *_ in entries]
+    try:
+        ref = _singles(scenes_, entries, [3] * len(entries))
+        jobs = [api.BatchJob(s, sd.camera, w, h, spp, seed=3, max_depth=8)
+                for s, (sd, w, h, spp) in zip(scenes_, entries)]
+        marker = [j.film.fill_(7.0) for j in jobs]
+        with api.Batch(jobs) as b:
+            chosen = b.autotune(trials=1, probe_spp=2)
+            torch.cuda.synchronize()
+            # the search renders into scratch films
+            assert all(bool((m == 7.0).all()) for m in marker)
+            assert chosen == b.config()
+            assert chosen["tile"] in (1, 4, 8, 16) and chosen["wave_paths"] > 0
+            b.launch()
+            torch.cuda.synchronize()
+            for j, r in zip(jobs, ref):
+                assert torch.equal(j.film.view(torch.int32), r.view(torch.int32))
+    finally:
+        for s in scenes_:
+            s.close()
+
+
+def test_batch_argument_checks():
+    import torch
+    from xyz_b200 import api
+    entries = _workload(2)
+    scenes_ = [api.Scene(sd) for sd, *_ in entries]
+    try:
+        jobs = [api.BatchJob(s, sd.camera, w, h, spp) for s, (sd, w, h, spp) in zip(scenes_, entries)]
+        with pytest.raises(api.XyzGpuError) as e:
+            api.Batch(jobs, wave_paths=1000)  # smaller than the largest image
+        assert e.value.code == -4
+        d = jobs[0].desc()
+        d.params.spectral = 1
+        arr = (api.BatchJobDesc * 1)(d)
+        h = api.C.c_void_p()
+        assert api.load_library().xyzgpu_batch_create(arr, 1, None, api.C.byref(h)) == -1
+        assert api.load_library().xyzgpu_batch_create(arr, 0, None, api.C.byref(h)) == -1
+    finally:
+        for s in scenes_:
+            s.close()

@@ -33,6 +33,9 @@ EXPORTED = [
     "xyzgpu_render_counters_get", "xyzgpu_render_profile_get", "xyzgpu_render_noalloc",
     "xyzgpu_philox_u01", "xyzgpu_last_error", "xyzgpu_abi_version", "xyzgpu_adjoint",
     "xyzgpu_scene_set_materials", "xyzgpu_scene_get_materials",
+    "xyzgpu_batch_config_default", "xyzgpu_batch_create", "xyzgpu_batch_launch",
+    "xyzgpu_batch_set_sample_offsets", "xyzgpu_batch_autotune", "xyzgpu_batch_stats_get",
+    "xyzgpu_batch_config_get", "xyzgpu_batch_destroy", "xyzgpu_render_batch",
 ]
 
 
@@ -81,6 +84,22 @@ class RenderParams(C.Structure):
                 ("hero_wavelengths", C.c_int)]
 
 SPECTRAL_MODES = {"off": 0, "xyz": 0, "binned": 1, "continuous": 2}
+
+
+class BatchJobDesc(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", CameraDesc), ("params", RenderParams),
+                ("film", C.c_void_p)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("wave_paths", C.c_int), ("tile", C.c_int), ("trace_ctas_per_sm", C.c_int),
+                ("use_graph", C.c_int)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("waves", C.c_uint64), ("kernel_launches_per_launch", C.c_uint64),
+                ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("device_bytes", C.c_int64),
+                ("graph_nodes", C.c_int)]
 
 
 class RenderProfile(C.Structure):
@@ -133,6 +152,16 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                  C.c_void_p, C.c_void_p, C.c_void_p]
     L.xyzgpu_scene_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.xyzgpu_scene_get_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.xyzgpu_batch_config_default.argtypes = [C.POINTER(BatchConfig)]
+    L.xyzgpu_batch_create.argtypes = [C.POINTER(BatchJobDesc), C.c_int, C.POINTER(BatchConfig),
+                                      C.POINTER(C.c_void_p)]
+    L.xyzgpu_batch_launch.argtypes = [C.c_void_p, C.c_void_p]
+    L.xyzgpu_batch_set_sample_offsets.argtypes = [C.c_void_p, C.c_void_p]
+    L.xyzgpu_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.POINTER(BatchConfig)]
+    L.xyzgpu_batch_stats_get.argtypes = [C.c_void_p, C.POINTER(BatchStats)]
+    L.xyzgpu_batch_config_get.argtypes = [C.c_void_p, C.POINTER(BatchConfig)]
+    L.xyzgpu_batch_destroy.argtypes = [C.c_void_p]
+    L.xyzgpu_render_batch.argtypes = [C.POINTER(BatchJobDesc), C.c_int, C.POINTER(BatchConfig), C.c_void_p]
     L.xyzgpu_build_params_default.argtypes = [C.POINTER(BuildParams)]
     L.xyzgpu_render_params_default.argtypes = [C.POINTER(RenderParams)]
     _LIB = L
@@ -417,3 +446,96 @@ class Scene:
 def philox_u01(seed: int, pixel: int, sample: int, dim: int) -> float:
     return load_library().xyzgpu_philox_u01(seed, pixel, sample, dim)
 
+
+
+def batch_config(**kw) -> BatchConfig:
+    c = BatchConfig()
+    load_library().xyzgpu_batch_config_default(C.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, int(v))
+    return c
+
+
+def _config_dict(c: BatchConfig) -> dict:
+    return {f: getattr(c, f) for f, _ in BatchConfig._fields_}
+
+
+class BatchJob:
+    """One render of a batch: a scene, camera, image size, samples and a
+    device film (allocated if not given)."""
+
+    def __init__(self, scene: Scene, camera, width: int, height: int, spp: int, *, seed: int = 0,
+                 spp_offset: int = 0, max_depth: int = 15, rr_start_depth: int = 1,
+                 rr_threshold: float = 0.2, accumulate: bool = False, film=None):
+        import torch
+        self.scene, self.camera = scene, camera
+        self.width, self.height, self.spp = width, height, spp
+        self.kw = dict(seed=seed, spp_offset=spp_offset, max_depth=max_depth,
+                       rr_start_depth=rr_start_depth, rr_threshold=rr_threshold, accumulate=accumulate)
+        if film is None:
+            film = torch.zeros((height, width, 3), dtype=torch.float32, device="cuda")
+        assert film.is_cuda and film.is_contiguous() and tuple(film.shape) == (height, width, 3)
+        self.film = film
+
+    def desc(self) -> BatchJobDesc:
+        d = BatchJobDesc()
+        d.scene = self.scene.handle.value
+        d.camera = camera_desc(self.camera)
+        d.params = render_params(self.width, self.height, self.spp, **self.kw)
+        d.params.film_location = XYZGPU_FILM_DEVICE
+        d.film = self.film.data_ptr()
+        return d
+
+
+class Batch:
+    """xyzgpu_batch: many renders in every kernel launch, replayed from a CUDA
+    graph.  launch() renders every job's samples into its film."""
+
+    def __init__(self, jobs, **config):
+        L = load_library()
+        self.jobs = list(jobs)
+        arr = (BatchJobDesc * len(self.jobs))(*[j.desc() for j in self.jobs])
+        cfg = batch_config(**config)
+        h = C.c_void_p()
+        _check(L.xyzgpu_batch_create(arr, len(self.jobs), C.byref(cfg), C.byref(h)))
+        self.handle = h
+
+    def launch(self, stream=None):
+        _check(_LIB.xyzgpu_batch_launch(self.handle, _stream_ptr(stream)))
+
+    def set_sample_offsets(self, offsets):
+        a = np.ascontiguousarray(offsets, dtype=np.uint32)
+        assert a.shape == (len(self.jobs),)
+        _check(_LIB.xyzgpu_batch_set_sample_offsets(self.handle, a.ctypes.data))
+
+    def autotune(self, trials: int = 2, probe_spp: int = 4, stream=None) -> dict:
+        c = BatchConfig()
+        _check(_LIB.xyzgpu_batch_autotune(self.handle, trials, probe_spp, _stream_ptr(stream), C.byref(c)))
+        return _config_dict(c)
+
+    def config(self) -> dict:
+        c = BatchConfig()
+        _check(_LIB.xyzgpu_batch_config_get(self.handle, C.byref(c)))
+        return _config_dict(c)
+
+    def stats(self) -> dict:
+        st = BatchStats()
+        _check(_LIB.xyzgpu_batch_stats_get(self.handle, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in BatchStats._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _LIB.xyzgpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

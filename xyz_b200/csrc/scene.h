@@ -4,6 +4,7 @@
 
 #include <cstdarg>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -78,6 +79,20 @@ struct SceneImpl {
   int32_t *d_fetch = nullptr;  // work-fetch counters of the trace API kernel
   unsigned long long *d_trace_counts = nullptr;
 };
+
+// Wave buffers are shared by every scene on a device (single and batched
+// renders): the largest wave asked for so far stays allocated, and renders on
+// different streams are ordered by an event so that they never use the buffers
+// at the same time.  Hold `mu` while using them.
+struct SharedWaves {
+  std::mutex mu;
+  RenderWorkspace ws;  // only the wave buffers (beta .. counts) are used
+  cudaEvent_t done = nullptr;
+  cudaStream_t last = nullptr;
+};
+SharedWaves &shared_waves(int device);
+int ensure_wave_buffers(RenderWorkspace &w, int64_t capacity, int iters);
+extern const int64_t kBytesPerPath;  // wave buffer bytes per path
 
 // Kernels' host-side launchers (trace.cu, render.cu, kdbuild.cu).
 int trace_api_launch(SceneImpl &s, const float *rays, int n, float *hits, cudaStream_t st,

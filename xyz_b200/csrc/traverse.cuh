@@ -153,9 +153,11 @@ XYZ_DEV void trace_closest(const DevScene &S, f3 o, f3 d, float tmin, float tmax
 // ray of the batch).  Every lane of the warp must call this.
 //   Sink::load(i, o, d, tmin, tmax)   ray i
 //   Sink::store(i, hit)               result of ray i
+//   Sink::scene(i)                    (kBatch) the scene of ray i; rays of one
+//                                     queue may belong to different scenes
 constexpr int kRefillIdle = 12;
 
-template <bool kCount, class Sink>
+template <bool kCount, bool kBatch = false, class Sink>
 XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, TraceCount &tc) {
   int const lane = threadIdx.x & 31;
   unsigned const lanes_below = (1u << lane) - 1u;
@@ -169,6 +171,7 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
   float tn = 0.0f, tf = 0.0f;
   int sp = 0;
   StackEntry stack[kKdMaxDepthLimit];
+  const DevScene *lane_scene = &S;
   for (;;) {
     bool const need = ray < 0 && !exhausted;
     // refill once at least kRefillIdle lanes are idle: refilling after every
@@ -188,6 +191,8 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
         } else {
           float tmax;
           sink.load(i, o, d, tmin, tmax);
+          if constexpr (kBatch) lane_scene = sink.scene(i);
+          const DevScene &SL = kBatch ? *lane_scene : S;
           h.t = tmax;
           h.id = -1;
           h.f = h.g = 0.0f;
@@ -196,8 +201,8 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
           inv[1] = __frcp_rn(d.y);
           inv[2] = __frcp_rn(d.z);
           float const org[3] = {o.x, o.y, o.z};
-          float const lo[3] = {S.bmin.x, S.bmin.y, S.bmin.z};
-          float const hi[3] = {S.bmax.x, S.bmax.y, S.bmax.z};
+          float const lo[3] = {SL.bmin.x, SL.bmin.y, SL.bmin.z};
+          float const hi[3] = {SL.bmax.x, SL.bmax.y, SL.bmax.z};
           float t0 = tmin, t1 = tmax;
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
@@ -220,8 +225,9 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
     }
     if (__all_sync(0xffffffffu, exhausted && ray < 0)) break;
     if (ray < 0) continue;
+    const uint2 *__restrict__ nodes = kBatch ? lane_scene->nodes : S.nodes;
     // descend to a leaf
-    uint2 nd = __ldg(&S.nodes[node]);
+    uint2 nd = __ldg(&nodes[node]);
     if (kCount) tc.nodes++;
     while ((nd.y & 3u) != kKdLeafTag) {
       uint32_t const ax = nd.y & 3u;
@@ -244,7 +250,7 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
         node = first;
         tf = tp;
       }
-      nd = __ldg(&S.nodes[node]);
+      nd = __ldg(&nodes[node]);
       if (kCount) tc.nodes++;
     }
     // test the leaf
@@ -253,9 +259,11 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
       tc.leaves++;
       tc.tris += cnt;
     }
+    const int32_t *__restrict__ refs = kBatch ? lane_scene->refs : S.refs;
+    const float4 *__restrict__ tris = kBatch ? lane_scene->tri : S.tri;
     for (uint32_t j = 0; j < cnt; ++j) {
-      int32_t const t = __ldg(&S.refs[nd.x + j]);
-      hit_triangle(S.tri, t, o, d, tmin, h);
+      int32_t const t = __ldg(&refs[nd.x + j]);
+      hit_triangle(tris, t, o, d, tmin, h);
     }
     // next leaf, or done
     bool done = (h.id >= 0 && h.t <= tf) || sp == 0;

@@ -427,6 +427,130 @@ def diff_scene(level: int = 4, wall_n: int = 20, light_n: int = 4, seed: int = 0
     t_em = (emission * (1.0 + rt.uniform(-perturb, perturb, size=nm))).astype(np.float32)
     return DiffScene(sd, albedo, emission, t_alb, t_em, light_mats)
 
+
+_ICO_CACHE: dict = {}
+
+
+def _icosphere_cached(level: int):
+    if level not in _ICO_CACHE:
+        _ICO_CACHE[level] = icosphere(level)
+    return _ICO_CACHE[level]
+
+
+def _box_tris(lo: np.ndarray, hi: np.ndarray):
+    """Axis-aligned boxes (n, 3) lo / hi -> (n * 8, 3) vertices, (n * 12, 3)
+    triangles with outward front normals (cross(v2-v0, v1-v0))."""
+    n = lo.shape[0]
+    corners = np.array([(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0),
+                        (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)], dtype=np.float64)
+    v = lo[:, None, :] + corners[None, :, :] * (hi - lo)[:, None, :]
+    # quads (i, j, k, l) with outward normals; split (i, j, k), (i, k, l)
+    quads = [((0, 3, 2, 1)), ((4, 5, 6, 7)), ((0, 1, 5, 4)), ((3, 7, 6, 2)),
+             ((0, 4, 7, 3)), ((1, 2, 6, 5))]
+    t = []
+    for (i, j, k, l) in quads:
+        t.append((i, k, j))
+        t.append((i, l, k))
+    t = np.array(t, dtype=np.int64)
+    tris = (t[None, :, :] + 8 * np.arange(n)[:, None, None]).reshape(-1, 3)
+    return v.reshape(-1, 3), tris
+
+
+def batch_scene(seed: int, target_tris: Optional[int] = None, radiance: float = 15.0) -> SceneData:
+    """One scene of the batched workload.  Triangle count log-uniform in
+    [1,000, 500,000] (from the seed) unless given.  Odd seeds: displaced
+    icospheres (the level whose face count fits, as many spheres as make up
+    the count); even seeds: random stacks of boxes (12 triangles each).  All on
+    a 20 x 20 m ground under a spherical light of radius 0.25 (320 triangles);
+    8 grey / coloured Lambert materials; pinhole camera, 40 degree fov."""
+    rng = np.random.default_rng(1000 + seed)
+    if target_tris is None:
+        target_tris = int(round(math.exp(rng.uniform(math.log(1000), math.log(500000)))))
+    pos_l, tri_l = [], []
+    base = 0
+    if seed % 2 == 1:
+        level = 3
+        while level < 7 and 20 * 4 ** (level + 1) <= target_tris:
+            level += 1
+        n_sph = max(1, int(round(target_tris / (20 * 4 ** level))))
+        xs = np.linspace(-1.2, 1.2, n_sph) if n_sph > 1 else np.zeros(1)
+        r = 0.6 if n_sph <= 2 else 1.6 / n_sph
+        for k, x in enumerate(xs):
+            v, f = _icosphere_cached(level)
+            v = v * (1.0 + 0.15 * value_noise(v, seed * 13 + k))[:, None]
+            v = v * r + np.array([x, r * 1.2, 0.0])
+            pos_l.append(v)
+            tri_l.append(f + base)
+            base += v.shape[0]
+    else:
+        n_box = max(1, int(round(target_tris / 12)))
+        cols = max(1, int(math.ceil(math.sqrt(n_box / 4.0))))
+        per_col = int(math.ceil(n_box / (cols * cols)))
+        idx = np.arange(n_box)
+        c = idx // per_col
+        lvl = idx % per_col
+        cx, cz = c % cols, c // cols
+        cell = 2.4 / cols
+        h = 1.6 / per_col
+        jitter = rng.uniform(-0.1, 0.1, size=(n_box, 2)) * cell
+        size = rng.uniform(0.4, 0.9, size=(n_box, 2)) * cell
+        x0 = -1.2 + (cx + 0.5) * cell + jitter[:, 0] - size[:, 0] / 2
+        z0 = -1.2 + (cz + 0.5) * cell + jitter[:, 1] - size[:, 1] / 2
+        y0 = lvl * h
+        lo = np.stack([x0, y0, z0], 1)
+        hi = np.stack([x0 + size[:, 0], y0 + h * rng.uniform(0.6, 1.0, size=n_box), z0 + size[:, 1]], 1)
+        v, f = _box_tris(lo, hi)
+        pos_l.append(v)
+        tri_l.append(f + base)
+        base += v.shape[0]
+    n_geom = int(sum(t.shape[0] for t in tri_l))
+    g = np.array([(-10, 0, -10), (10, 0, -10), (10, 0, 10), (-10, 0, 10)], dtype=np.float64)
+    pos_l.append(g)
+    tri_l.append(np.array([(0, 1, 2), (0, 2, 3)], dtype=np.int64) + base)
+    base += 4
+    lv, lf = _icosphere_cached(2)
+    lv = lv * 0.25 + np.array([0.4, 2.8, 1.4])
+    pos_l.append(lv)
+    tri_l.append(lf + base)
+    pos = np.concatenate(pos_l).astype(np.float32)
+    tris = np.concatenate(tri_l).astype(np.int32)
+    n_mat = 8
+    tri_mat = np.concatenate([rng.integers(0, n_mat, size=n_geom), np.zeros(2, np.int64),
+                              np.full(lf.shape[0], n_mat)]).astype(np.int32)
+    rgb = rng.uniform(0.15, 0.85, size=(n_mat, 3))
+    albedo = np.concatenate([np.stack([ccir601_rgb_to_xyz(c) for c in rgb]),
+                             np.zeros((1, 3), np.float32)]).astype(np.float32)
+    is_light = np.zeros(n_mat + 1, np.int32)
+    is_light[n_mat] = 1
+    sd = SceneData(pos, tris, tri_mat, albedo, is_light, np.zeros(3, np.float32),
+                   camera=Camera.with_fov((0.0, 1.5, 4.2), (0.0, 0.7, 0.0), 40.0, pinhole=True),
+                   name=f"batch-{seed}")
+    sd.light_power_xyz = flat_emitter_power(radiance, sd.light_area())
+    return sd
+
+
+@dataclass
+class BatchEntry:
+    scene: SceneData
+    width: int
+    height: int
+    spp: int
+    max_depth: int = 8
+
+
+def batch_workload(n: int = 64, first_seed: int = 0) -> list:
+    """The batched workload: scenes of seeds first_seed .. first_seed + n - 1
+    (batch_scene), resolution drawn from {128, 256, 512, 1024} squared and
+    samples per pixel uniform in 4..64 (seeded per scene), max depth 8."""
+    out = []
+    for k in range(n):
+        seed = first_seed + k
+        rng = np.random.default_rng(2000 + seed)
+        res = int(rng.choice([128, 256, 512, 1024]))
+        spp = int(rng.integers(4, 65))
+        out.append(BatchEntry(batch_scene(seed), res, res, spp, 8))
+    return out
+
 def random_rays(scene: SceneData, n: int, seed: int = 0):
     """Seeded test rays: origins uniform in the scene box grown by 20 %,
     directions uniform on the sphere.  Returns (org, dir) float32 (n, 3)."""
