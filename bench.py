@@ -255,6 +255,55 @@ def adjoint_bench(steps: int, warmup: int):
                           "and emission (32 light triangles)"}
 
 
+def batch_bench(steps: int, warmup: int):
+    """Batched workload: 64 scenes (seeds 0-63, 1k-500k triangles, displaced
+    icospheres and box stacks), resolutions in {128,256,512,1024}^2, 4-64 spp,
+    max depth 8, in one graph launch after autotuning; against the same 64
+    renders issued one xyzgpu_render call after another.  Device time."""
+    import torch
+    from xyz_b200 import api, scenes
+    work = scenes.batch_workload(64)
+    sc = [api.Scene(e.scene) for e in work]
+    try:
+        paths = sum(e.width * e.height * e.spp for e in work)
+        jobs = [api.BatchJob(s, e.scene.camera, e.width, e.height, e.spp, seed=k, max_depth=e.max_depth)
+                for k, (s, e) in enumerate(zip(sc, work))]
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def singles():
+            for k, (s, e) in enumerate(zip(sc, work)):
+                s.render(e.scene.camera, e.width, e.height, e.spp, seed=k, max_depth=e.max_depth,
+                         film=jobs[k].film)
+
+        singles()
+        ev0.record()
+        singles()
+        ev1.record()
+        torch.cuda.synchronize()
+        single_ms = ev0.elapsed_time(ev1)
+        with api.Batch(jobs) as b:
+            chosen = b.autotune(trials=1, probe_spp=4)
+            for _ in range(warmup):
+                b.launch()
+            torch.cuda.synchronize()
+            ev0.record()
+            for _ in range(steps):
+                b.launch()
+            ev1.record()
+            torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1) / steps
+            st = b.stats()
+        return {"msamples_per_s": round(paths / ms / 1e3, 1), "ms_per_launch": round(ms, 3),
+                "sequential_renders_msamples_per_s": round(paths / single_ms / 1e3, 1),
+                "paths": paths, "triangles": int(sum(e.scene.n_tris for e in work)),
+                "waves": st["waves"], "graph_nodes": st["graph_nodes"], "autotuned": chosen,
+                "config": "64 scenes (seeds 0-63), 1k-500k triangles log-uniform, displaced icospheres "
+                          "(odd) and box stacks (even), 128^2..1024^2, 4-64 spp, max depth 8"}
+    finally:
+        for s in sc:
+            s.close()
+
+
 def profiled_traffic():
     """DRAM bytes per traced ray of the trace kernel from the committed ncu
     summary (profiles/trace_queue_spheres1m.txt), if present."""
@@ -400,9 +449,10 @@ def run_gpu_arm(args, rank, world):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(sd)
-    adjoint = None
+    adjoint = batch = None
     if rank == 0 and world == 1 and not args.no_extras:
         adjoint = adjoint_bench(args.steps, args.warmup)
+        batch = batch_bench(args.steps, args.warmup)
 
     if rank == 0:
         line = {
@@ -413,7 +463,7 @@ def run_gpu_arm(args, rank, world):
             "config": workload_config(stats) | {"parallelism": f"sample-parallel x{world}",
                                                  "waves_per_step": counters["waves"]},
             "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-            "adjoint": adjoint,
+            "adjoint": adjoint, "batch": batch,
             "clocks": clk, "wall_ms_timed_region": round(wall_ms, 1),
             "render_counters": counters,
         }
@@ -430,7 +480,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the differentiable-rendering measurement")
+                    help="skip the differentiable-rendering and batched-rendering measurements")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
