@@ -357,6 +357,49 @@ void xyzgpu_batch_destroy(xyzgpu_batch batch);
 int xyzgpu_render_batch(const xyzgpu_batch_job *jobs, int n_jobs, const xyzgpu_batch_config *cfg,
                         void *stream);
 
+/* Learned path guide: an MLP from a surface point (position, normal) to an
+ * 8-lobe von Mises-Fisher mixture over directions, trained online on the
+ * tracer's own radiance samples and combined with Lambert sampling by one-
+ * sample MIS (so the estimator stays unbiased).  No counterpart in the
+ * reference; its non-learned analogue is the importon histogram of
+ * xyz/core/photonmap.cpp:365-494.  The network: one-blob encoding (32 bins per
+ * input, 192 values), four hidden layers of 64 with ReLU, 64 outputs (0..7
+ * mixture logits, 8..15 log concentrations clamped to [-5, 8], 16..39 lobe
+ * means, 40..63 unused); bf16 weights, fp32 accumulation on tcgen05 tensor
+ * cores; Adam on fp32 master weights.  Parameters (XYZGPU_GUIDE_PARAMS floats):
+ * for each layer l = 0..4, W_l as [in][64] row-major then b_l[64]. */
+#define XYZGPU_GUIDE_PARAMS 28992
+#define XYZGPU_GUIDE_OUTPUTS 64
+
+typedef struct {
+  float alpha;           /* probability of sampling the guide in the one-sample MIS (0.5) */
+  float learning_rate;   /* Adam step size (1e-3) */
+  int batch_size;        /* training records per Adam step (65536) */
+  int steps_per_pass;    /* Adam steps after each training render (16) */
+  int train_bounces;     /* path vertices per path that give training records (2) */
+  uint64_t seed;         /* weight initialisation */
+} xyzgpu_guide_config;
+
+typedef struct xyzgpu_guide_s *xyzgpu_guide;
+
+void xyzgpu_guide_config_default(xyzgpu_guide_config *cfg);
+/* A guide for `scene` (positions are normalised by its bounds). */
+int xyzgpu_guide_create(xyzgpu_scene scene, const xyzgpu_guide_config *cfg, xyzgpu_guide *out);
+void xyzgpu_guide_destroy(xyzgpu_guide guide);
+/* fp32 master parameters, host arrays of XYZGPU_GUIDE_PARAMS (set resets Adam). */
+int xyzgpu_guide_get_params(xyzgpu_guide guide, float *params);
+int xyzgpu_guide_set_params(xyzgpu_guide guide, const float *params);
+/* Network outputs for n points: features n x 6 (position, normal), out n x 64
+ * (device arrays).  Synchronises `stream`. */
+int xyzgpu_guide_forward(xyzgpu_guide guide, const float *features, int n, float *out, void *stream);
+/* Adds scale * d/dparams sum_i -w_i log p(d_i | x_i) to grad (device,
+ * XYZGPU_GUIDE_PARAMS floats); records: n x 10 = position, normal, direction
+ * d (unit), weight w (device).  Synchronises `stream`. */
+int xyzgpu_guide_gradient(xyzgpu_guide guide, const float *records, int n, float scale, float *grad,
+                          void *stream);
+/* One Adam step on the mean loss of n records.  Synchronises `stream`. */
+int xyzgpu_guide_train_step(xyzgpu_guide guide, const float *records, int n, void *stream);
+
 /* Host evaluation of the random stream defined above (for tests). */
 float xyzgpu_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim);
 

@@ -36,6 +36,9 @@ EXPORTED = [
     "xyzgpu_batch_config_default", "xyzgpu_batch_create", "xyzgpu_batch_launch",
     "xyzgpu_batch_set_sample_offsets", "xyzgpu_batch_autotune", "xyzgpu_batch_stats_get",
     "xyzgpu_batch_config_get", "xyzgpu_batch_destroy", "xyzgpu_render_batch",
+    "xyzgpu_guide_config_default", "xyzgpu_guide_create", "xyzgpu_guide_destroy",
+    "xyzgpu_guide_get_params", "xyzgpu_guide_set_params", "xyzgpu_guide_forward",
+    "xyzgpu_guide_gradient", "xyzgpu_guide_train_step",
 ]
 
 
@@ -84,6 +87,15 @@ class RenderParams(C.Structure):
                 ("hero_wavelengths", C.c_int)]
 
 SPECTRAL_MODES = {"off": 0, "xyz": 0, "binned": 1, "continuous": 2}
+
+
+GUIDE_PARAMS = 28992
+GUIDE_OUTPUTS = 64
+
+
+class GuideConfig(C.Structure):
+    _fields_ = [("alpha", C.c_float), ("learning_rate", C.c_float), ("batch_size", C.c_int),
+                ("steps_per_pass", C.c_int), ("train_bounces", C.c_int), ("seed", C.c_uint64)]
 
 
 class BatchJobDesc(C.Structure):
@@ -162,6 +174,14 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.xyzgpu_batch_config_get.argtypes = [C.c_void_p, C.POINTER(BatchConfig)]
     L.xyzgpu_batch_destroy.argtypes = [C.c_void_p]
     L.xyzgpu_render_batch.argtypes = [C.POINTER(BatchJobDesc), C.c_int, C.POINTER(BatchConfig), C.c_void_p]
+    L.xyzgpu_guide_config_default.argtypes = [C.POINTER(GuideConfig)]
+    L.xyzgpu_guide_create.argtypes = [C.c_void_p, C.POINTER(GuideConfig), C.POINTER(C.c_void_p)]
+    L.xyzgpu_guide_destroy.argtypes = [C.c_void_p]
+    L.xyzgpu_guide_get_params.argtypes = [C.c_void_p, C.c_void_p]
+    L.xyzgpu_guide_set_params.argtypes = [C.c_void_p, C.c_void_p]
+    L.xyzgpu_guide_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.xyzgpu_guide_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_void_p]
+    L.xyzgpu_guide_train_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.xyzgpu_build_params_default.argtypes = [C.POINTER(BuildParams)]
     L.xyzgpu_render_params_default.argtypes = [C.POINTER(RenderParams)]
     _LIB = L
@@ -526,6 +546,83 @@ class Batch:
     def close(self):
         if getattr(self, "handle", None):
             _LIB.xyzgpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def guide_config(**kw) -> GuideConfig:
+    c = GuideConfig()
+    load_library().xyzgpu_guide_config_default(C.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+class Guide:
+    """xyzgpu_guide: the learned path guide of a scene (an MLP on the tensor
+    cores from surface point to a von Mises-Fisher mixture)."""
+
+    def __init__(self, scene: Scene, **config):
+        L = load_library()
+        cfg = guide_config(**config)
+        h = C.c_void_p()
+        _check(L.xyzgpu_guide_create(scene.handle, C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self.scene = scene
+        st = scene.stats()
+        lo = np.array(st["bounds_min"], np.float32)
+        hi = np.array(st["bounds_max"], np.float32)
+        ext = (hi - lo).astype(np.float32)
+        self.lo = lo
+        self.inv_ext = np.where(ext > 0, np.float32(1.0) / np.where(ext > 0, ext, 1), 1).astype(np.float32)
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(GUIDE_PARAMS, np.float32)
+        _check(_LIB.xyzgpu_guide_get_params(self.handle, p.ctypes.data))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.shape == (GUIDE_PARAMS,)
+        _check(_LIB.xyzgpu_guide_set_params(self.handle, p.ctypes.data))
+
+    def forward(self, features, stream=None):
+        """features: CUDA float32 (n, 6) -> outputs (n, 64)."""
+        import torch
+        n = int(features.shape[0])
+        out = torch.empty((n, GUIDE_OUTPUTS), dtype=torch.float32, device=features.device)
+        _check(_LIB.xyzgpu_guide_forward(self.handle, features.contiguous().data_ptr(), n, out.data_ptr(),
+                                         _stream_ptr(stream)))
+        return out
+
+    def gradient(self, records, scale: float = 1.0, grad=None, stream=None):
+        """records: CUDA float32 (n, 10) -> flat gradient (accumulated into grad)."""
+        import torch
+        n = int(records.shape[0])
+        if grad is None:
+            grad = torch.zeros(GUIDE_PARAMS, dtype=torch.float32, device=records.device)
+        _check(_LIB.xyzgpu_guide_gradient(self.handle, records.contiguous().data_ptr(), n, float(scale),
+                                          grad.data_ptr(), _stream_ptr(stream)))
+        return grad
+
+    def train_step(self, records, stream=None):
+        _check(_LIB.xyzgpu_guide_train_step(self.handle, records.contiguous().data_ptr(), int(records.shape[0]),
+                                            _stream_ptr(stream)))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _LIB.xyzgpu_guide_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
