@@ -168,6 +168,8 @@ typedef struct {
   int spectral;            /* XYZGPU_SPECTRAL_*: XYZ tristimulus paths (the xyz renderer,
                               default) or hero-wavelength spectral paths */
   int hero_wavelengths;    /* 1..4 wavelengths per path in the spectral modes */
+  int row_begin, row_end;  /* render only image rows [row_begin, row_end) (a band of the same
+                              image: same pixels, same paths); 0, 0 = all rows */
 } xyzgpu_render_params;
 
 /* Film modes.  OFF: throughput and albedo are CIE XYZ triples, the estimator of
@@ -399,6 +401,28 @@ int xyzgpu_guide_gradient(xyzgpu_guide guide, const float *records, int n, float
                           void *stream);
 /* One Adam step on the mean loss of n records.  Synchronises `stream`. */
 int xyzgpu_guide_train_step(xyzgpu_guide guide, const float *records, int n, void *stream);
+
+/* Guided render: as xyzgpu_render (XYZ film mode) with every Lambert vertex
+ * sampled from the one-sample MIS of the guide (probability alpha) and the
+ * cosine lobe, and the next-event MIS weights computed with that mixture
+ * density, so the estimator stays unbiased whatever the network outputs.  Per
+ * bounce the wavefront runs closest hit, guide inference on the tensor cores
+ * (a mixture per queue entry), shading and shadow rays.  train != 0: the first
+ * train_bounces vertices of every path also leave training records (point,
+ * sampled direction, incident-radiance weight), and after each wave the guide
+ * takes steps_per_pass Adam steps on them (synchronises `stream`).  Russian
+ * roulette tests the throughput the path would have with Lambert sampling (the
+ * throughput times the product of the guide / Lambert density ratios): the
+ * guide sends paths towards bright regions with a high pdf, i.e. a low
+ * throughput, which roulette on the throughput itself would end. */
+int xyzgpu_render_guided(xyzgpu_guide guide, const xyzgpu_camera *camera,
+                         const xyzgpu_render_params *rp, int train, float *film, void *stream);
+
+typedef struct {
+  uint64_t adam_steps, trained_records;
+} xyzgpu_guide_stats;
+
+int xyzgpu_guide_stats_get(xyzgpu_guide guide, xyzgpu_guide_stats *out);
 
 /* Host evaluation of the random stream defined above (for tests). */
 float xyzgpu_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim);

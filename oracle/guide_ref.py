@@ -56,7 +56,8 @@ def bf16(x) -> np.ndarray:
 
 def encode(features, lo, inv_ext) -> np.ndarray:
     """One-blob encoding of (position, normal) rows: 32 Gaussian bins
-    (sigma 1/32) per input; positions normalised by the scene bounds."""
+    (sigma 1/32) per input, bins beyond 4.5 sigma set to 0; positions
+    normalised by the scene bounds."""
     f = np.asarray(features, np.float32)
     s = np.empty((f.shape[0], 6), np.float32)
     s[:, :3] = (f[:, :3] - np.asarray(lo, np.float32)) * np.asarray(inv_ext, np.float32)
@@ -65,6 +66,10 @@ def encode(features, lo, inv_ext) -> np.ndarray:
     centres = ((np.arange(BINS, dtype=np.float32) + np.float32(0.5)) * np.float32(1.0 / BINS)).astype(np.float32)
     d = (s[:, :, None] - centres[None, None, :]).astype(np.float32)
     v = np.exp(-d * d * np.float32(0.5 * BINS * BINS)).astype(np.float32)
+    # bins more than 4.5 sigma away are exactly 0
+    u = (s * np.float32(BINS)).astype(np.float32)
+    far = np.abs(u[:, :, None] - (np.arange(BINS, dtype=np.float32) + np.float32(0.5))[None, None, :]) > 4.5
+    v[far] = 0.0
     return bf16(v.reshape(f.shape[0], N_IN))
 
 

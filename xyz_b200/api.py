@@ -38,7 +38,7 @@ EXPORTED = [
     "xyzgpu_batch_config_get", "xyzgpu_batch_destroy", "xyzgpu_render_batch",
     "xyzgpu_guide_config_default", "xyzgpu_guide_create", "xyzgpu_guide_destroy",
     "xyzgpu_guide_get_params", "xyzgpu_guide_set_params", "xyzgpu_guide_forward",
-    "xyzgpu_guide_gradient", "xyzgpu_guide_train_step",
+    "xyzgpu_guide_gradient", "xyzgpu_guide_train_step", "xyzgpu_render_guided", "xyzgpu_guide_stats_get",
 ]
 
 
@@ -84,7 +84,7 @@ class RenderParams(C.Structure):
                 ("max_depth", C.c_int), ("rr_start_depth", C.c_int), ("rr_threshold", C.c_float),
                 ("seed", C.c_uint64), ("film_location", C.c_int), ("accumulate", C.c_int),
                 ("wave_paths", C.c_int), ("profile", C.c_int), ("spectral", C.c_int),
-                ("hero_wavelengths", C.c_int)]
+                ("hero_wavelengths", C.c_int), ("row_begin", C.c_int), ("row_end", C.c_int)]
 
 SPECTRAL_MODES = {"off": 0, "xyz": 0, "binned": 1, "continuous": 2}
 
@@ -96,6 +96,10 @@ GUIDE_OUTPUTS = 64
 class GuideConfig(C.Structure):
     _fields_ = [("alpha", C.c_float), ("learning_rate", C.c_float), ("batch_size", C.c_int),
                 ("steps_per_pass", C.c_int), ("train_bounces", C.c_int), ("seed", C.c_uint64)]
+
+
+class GuideStats(C.Structure):
+    _fields_ = [("adam_steps", C.c_uint64), ("trained_records", C.c_uint64)]
 
 
 class BatchJobDesc(C.Structure):
@@ -182,6 +186,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.xyzgpu_guide_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.xyzgpu_guide_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_void_p]
     L.xyzgpu_guide_train_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    L.xyzgpu_render_guided.argtypes = [C.c_void_p, C.POINTER(CameraDesc), C.POINTER(RenderParams), C.c_int,
+                                       C.c_void_p, C.c_void_p]
+    L.xyzgpu_guide_stats_get.argtypes = [C.c_void_p, C.POINTER(GuideStats)]
     L.xyzgpu_build_params_default.argtypes = [C.POINTER(BuildParams)]
     L.xyzgpu_render_params_default.argtypes = [C.POINTER(RenderParams)]
     _LIB = L
@@ -218,7 +225,7 @@ def camera_desc(camera) -> "CameraDesc":
 def render_params(width: int, height: int, spp: int, *, seed: int = 0, spp_offset: int = 0,
                   max_depth: int = 15, rr_start_depth: int = 1, rr_threshold: float = 0.2,
                   accumulate: bool = False, wave_paths: int = 0, profile: int = 0, spectral="off",
-                  hero_wavelengths: int = 4) -> "RenderParams":
+                  hero_wavelengths: int = 4, rows=None) -> "RenderParams":
     rp = RenderParams()
     load_library().xyzgpu_render_params_default(C.byref(rp))
     rp.width, rp.height, rp.spp, rp.spp_offset = width, height, spp, spp_offset
@@ -229,6 +236,8 @@ def render_params(width: int, height: int, spp: int, *, seed: int = 0, spp_offse
     rp.profile = profile
     rp.spectral = SPECTRAL_MODES[spectral] if isinstance(spectral, str) else int(spectral)
     rp.hero_wavelengths = hero_wavelengths
+    if rows is not None:
+        rp.row_begin, rp.row_end = int(rows[0]), int(rows[1])
     return rp
 
 
@@ -349,15 +358,16 @@ class Scene:
                spp_offset: int = 0, max_depth: int = 15, rr_start_depth: int = 1,
                rr_threshold: float = 0.2, film=None, accumulate: bool = False,
                wave_paths: int = 0, profile: int = 0, spectral="off", hero_wavelengths: int = 4,
-               stream=None):
+               rows=None, stream=None):
         """Renders into `film`: a CUDA tensor (H, W, 3) (device film) or a numpy
         float32 array (host film).  Allocates a CUDA tensor if film is None.
-        Returns the film (sums over samples, not means)."""
+        rows = (first, end): only that band of image rows.  Returns the film
+        (sums over samples, not means)."""
         cam = camera_desc(camera)
         rp = render_params(width, height, spp, seed=seed, spp_offset=spp_offset, max_depth=max_depth,
                            rr_start_depth=rr_start_depth, rr_threshold=rr_threshold,
                            accumulate=accumulate, wave_paths=wave_paths, profile=profile,
-                           spectral=spectral, hero_wavelengths=hero_wavelengths)
+                           spectral=spectral, hero_wavelengths=hero_wavelengths, rows=rows)
         if film is None:
             import torch
             film = torch.zeros((height, width, 3), dtype=torch.float32, device="cuda")
@@ -619,6 +629,28 @@ class Guide:
     def train_step(self, records, stream=None):
         _check(_LIB.xyzgpu_guide_train_step(self.handle, records.contiguous().data_ptr(), int(records.shape[0]),
                                             _stream_ptr(stream)))
+
+    def render(self, camera, width: int, height: int, spp: int, *, train: bool = False, seed: int = 0,
+               spp_offset: int = 0, max_depth: int = 15, rr_start_depth: int = 1, rr_threshold: float = 0.2,
+               film=None, accumulate: bool = False, wave_paths: int = 0, rows=None, stream=None):
+        """xyzgpu_render_guided into a CUDA film (H, W, 3) of sums; train: learn
+        from this render's paths (Adam steps after each wave)."""
+        import torch
+        if film is None:
+            film = torch.zeros((height, width, 3), dtype=torch.float32, device="cuda")
+        cam = camera_desc(camera)
+        rp = render_params(width, height, spp, seed=seed, spp_offset=spp_offset, max_depth=max_depth,
+                           rr_start_depth=rr_start_depth, rr_threshold=rr_threshold, accumulate=accumulate,
+                           wave_paths=wave_paths, rows=rows)
+        rp.film_location = XYZGPU_FILM_DEVICE
+        _check(_LIB.xyzgpu_render_guided(self.handle, C.byref(cam), C.byref(rp), int(bool(train)),
+                                         film.data_ptr(), _stream_ptr(stream)))
+        return film
+
+    def stats(self) -> dict:
+        st = GuideStats()
+        _check(_LIB.xyzgpu_guide_stats_get(self.handle, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in GuideStats._fields_}
 
     def close(self):
         if getattr(self, "handle", None):

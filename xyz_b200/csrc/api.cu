@@ -535,7 +535,9 @@ int check_render_args(const char *who, xyzgpu_scene scene, const xyzgpu_camera *
       !(rp->rr_threshold >= 0.0f) || rp->wave_paths < 0 || rp->profile < 0 || rp->profile > 2 ||
       rp->spectral < 0 || rp->spectral > 2 ||
       (rp->spectral && (rp->hero_wavelengths < 1 || rp->hero_wavelengths > 4)) ||
-      (rp->film_location != XYZGPU_FILM_DEVICE && rp->film_location != XYZGPU_FILM_HOST))
+      (rp->film_location != XYZGPU_FILM_DEVICE && rp->film_location != XYZGPU_FILM_HOST) ||
+      !((rp->row_begin == 0 && rp->row_end == 0) ||
+        (rp->row_begin >= 0 && rp->row_begin < rp->row_end && rp->row_end <= rp->height)))
     return set_error(XYZGPU_E_INVALID, "%s: parameters out of range", who);
   if (static_cast<int64_t>(rp->width) * rp->height >= (1ll << 31))
     return set_error(XYZGPU_E_LIMIT, "%s: image of %d x %d pixels exceeds 2^31", who, rp->width,
@@ -648,8 +650,8 @@ int xyzgpu_render_noalloc(xyzgpu_scene scene, const xyzgpu_camera *cam,
   if (!scene || !cam || !rp || !film) return set_error(XYZGPU_E_INVALID, "render_noalloc: null argument");
   if (rp->width <= 0 || rp->height <= 0 || rp->spp < 0 || rp->spp_offset < 0 ||
       rp->max_depth < 1 || rp->rr_start_depth < 1 || !(rp->rr_threshold >= 0.0f) ||
-      rp->wave_paths < 0)
-    return set_error(XYZGPU_E_INVALID, "render_noalloc: parameters out of range");
+      rp->wave_paths < 0 || rp->row_begin != 0 || rp->row_end != 0)
+    return set_error(XYZGPU_E_INVALID, "render_noalloc: parameters out of range (row bands are not available)");
   if (static_cast<int64_t>(rp->width) * rp->height >= (1ll << 31))
     return set_error(XYZGPU_E_LIMIT, "render_noalloc: image of %d x %d pixels exceeds 2^31",
                      rp->width, rp->height);

@@ -149,10 +149,10 @@ int upload_tables(Batch &b, const std::vector<float *> *films, cudaStream_t st) 
 void set_grids(Batch &b) {
   int const sms = sm_count(b.device);
   b.grid_raygen = occupancy_grid(k_raygen<true>, b.device);
-  b.grid_shade = occupancy_grid(k_shade<false, true>, b.device);
+  b.grid_shade = occupancy_grid(k_shade<kModeBatch>, b.device);
   b.grid_film = occupancy_grid(k_film_batch, b.device);
-  int const occ_e = occupancy_grid(k_trace_queue<false, false, false, true>, b.device) / sms;
-  int const occ_s = occupancy_grid(k_trace_queue<true, false, false, true>, b.device) / sms;
+  int const occ_e = occupancy_grid(k_trace_queue<false, false, kModeBatch>, b.device) / sms;
+  int const occ_s = occupancy_grid(k_trace_queue<true, false, kModeBatch>, b.device) / sms;
   int const want = b.cfg.trace_ctas_per_sm;
   b.grid_trace_e = (want > 0 ? std::min(want, occ_e) : occ_e) * sms;
   b.grid_trace_s = (want > 0 ? std::min(want, occ_s) : occ_s) * sms;
@@ -198,9 +198,9 @@ int issue(Batch &b, cudaStream_t st, const std::vector<float *> &films, bool cle
     int const gr = static_cast<int>(std::min<int64_t>(b.grid_raygen, (w.npaths + kThreads - 1) / kThreads));
     k_raygen<true><<<gr, kThreads, 0, st>>>(A);
     for (int it = 0; it < iters; ++it) {
-      k_trace_queue<false, false, false, true><<<b.grid_trace_e, kThreads, 0, st>>>(A, it, nullptr);
-      k_shade<false, true><<<b.grid_shade, kThreads, 0, st>>>(A, it);
-      k_trace_queue<true, false, false, true><<<b.grid_trace_s, kThreads, 0, st>>>(A, it, nullptr);
+      k_trace_queue<false, false, kModeBatch><<<b.grid_trace_e, kThreads, 0, st>>>(A, it, nullptr);
+      k_shade<kModeBatch><<<b.grid_shade, kThreads, 0, st>>>(A, it);
+      k_trace_queue<true, false, kModeBatch><<<b.grid_trace_s, kThreads, 0, st>>>(A, it, nullptr);
     }
     int const gf = static_cast<int>(std::min<int64_t>(b.grid_film, (w.film_threads + kThreads - 1) / kThreads));
     k_film_batch<<<gf, kThreads, 0, st>>>(A);
@@ -333,8 +333,8 @@ int xyzgpu_batch_create(const xyzgpu_batch_job *jobs, int n_jobs, const xyzgpu_b
     if (p.width <= 0 || p.height <= 0 || p.spp < 0 || p.spp_offset < 0 || p.max_depth < 1 ||
         p.max_depth > 1000 || p.rr_start_depth < 1 || !(p.rr_threshold >= 0.0f))
       return set_error(XYZGPU_E_INVALID, "batch_create: job %d: parameters out of range", j);
-    if (p.spectral != XYZGPU_SPECTRAL_OFF || p.profile != XYZGPU_PROFILE_OFF)
-      return set_error(XYZGPU_E_INVALID, "batch_create: job %d: XYZ film mode without profiling only", j);
+    if (p.spectral != XYZGPU_SPECTRAL_OFF || p.profile != XYZGPU_PROFILE_OFF || p.row_begin != 0 || p.row_end != 0)
+      return set_error(XYZGPU_E_INVALID, "batch_create: job %d: XYZ film mode, whole images, no profiling", j);
     if (static_cast<int64_t>(p.width) * p.height >= (1ll << 31))
       return set_error(XYZGPU_E_LIMIT, "batch_create: job %d: image exceeds 2^31 pixels", j);
     if (static_cast<int64_t>(p.spp_offset) + p.spp >= (1ll << 32))
@@ -485,7 +485,7 @@ int xyzgpu_batch_autotune(xyzgpu_batch h, int trials, int probe_spp, void *strea
     float best_ms = 0.0f;
     rc = time_cfg(best, &best_ms);
     if (rc) break;
-    int const occ = occupancy_grid(k_trace_queue<false, false, false, true>, b.device) / sm_count(b.device);
+    int const occ = occupancy_grid(k_trace_queue<false, false, kModeBatch>, b.device) / sm_count(b.device);
     std::vector<int> tiles = {1, 4, 8, 16};
     std::vector<int> waves;
     for (int64_t w = int64_t{1} << 22; w <= (int64_t{1} << 26); w <<= 1)

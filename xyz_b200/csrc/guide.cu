@@ -31,6 +31,7 @@
 #include <vector>
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "scene.h"
 #include "tc.cuh"
@@ -99,88 +100,127 @@ __device__ __forceinline__ void store_row8(uint8_t *buf, int r, int c, int cols,
   *reinterpret_cast<uint4 *>(buf + tc::blocked_offset(r, c, cols)) = q;
 }
 
-// One-blob value of bin j for s in [0, 1]: exp(-(s - (j + 1/2) / 32)^2 / (2 sigma^2)), sigma = 1/32.
-__device__ __forceinline__ float blob(float s, int j) {
-  float const d = s - (static_cast<float>(j) + 0.5f) * (1.0f / kBins);
-  return expf(-d * d * (0.5f * kBins * kBins));
-}
-
-// Writes row r of the input encoding from a raw point (position, normal).
-__device__ void encode_row(GuideSmem &S, const GuideDev &G, int r, const float f[6]) {
+// Row r of the input encoding from a raw point (position, normal): per
+// input s in [0, 1], 32 bins of exp(-(s - (j + 1/2) / 32)^2 / (2 sigma^2)),
+// sigma = 1/32.  Bins more than 4.5 sigma from s are exactly 0 (exp(-10) and
+// below; the oracle applies the same cut): the row is cleared, then the at
+// most 10 bins of the window are computed and stored one by one.
+__device__ void encode_row(uint8_t *x, int r, const GuideDev &G, const float f[6]) {
+#pragma unroll
+  for (int q = 0; q < kIn; q += 8) *reinterpret_cast<uint4 *>(x + tc::blocked_offset(r, q, kIn)) = make_uint4(0, 0, 0, 0);
 #pragma unroll 1
   for (int dim = 0; dim < 6; ++dim) {
     float s = dim < 3 ? (f[dim] - G.lo[dim]) * G.inv_ext[dim] : (f[dim] + 1.0f) * 0.5f;
     s = fminf(fmaxf(s, 0.0f), 1.0f);
+    float const u = s * static_cast<float>(kBins);
+    int const jlo = max(0, static_cast<int>(ceilf(u - 5.0f)));
 #pragma unroll
-    for (int j8 = 0; j8 < kBins; j8 += 8) {
-      float v[8];
-#pragma unroll
-      for (int t = 0; t < 8; ++t) v[t] = blob(s, j8 + t);
-      store_row8(S.x, r, dim * kBins + j8, kIn, v);
+    for (int t = 0; t < 10; ++t) {
+      int const j = jlo + t;
+      if (j < kBins && fabsf(u - (static_cast<float>(j) + 0.5f)) <= 4.5f) {
+        float const d = s - (static_cast<float>(j) + 0.5f) * (1.0f / kBins);
+        __nv_bfloat16 const v = __float2bfloat16_rn(__expf(-d * d * (0.5f * kBins * kBins)));
+        *reinterpret_cast<__nv_bfloat16 *>(x + tc::blocked_offset(r, dim * kBins + j, kIn)) = v;
+      }
     }
   }
 }
 
-// ---------------------------------------------------------------- stages
-__device__ __forceinline__ void publish() {
-  tc::fence_smem_to_async();
-  tc::fence_before_sync();
-  __syncthreads();
+// ---------------------------------------------------------------- tiles
+// The 128 rows one group of four warps works on: its buffers, its TMEM
+// accumulator (64 columns), its completion mbarrier and its barrier (0 = the
+// whole CTA, else a named barrier of the group's 128 threads).
+struct Tile {
+  uint8_t *x;     // encoding [128][192]
+  uint8_t *h[4];  // hidden outputs [128][64]: all four kept for training, else h[0], h[1] alternate
+  uint32_t tmem;
+  uint32_t mbar;
+  int bar;
+  int t;          // this thread's row
+};
+
+__device__ __forceinline__ void tile_sync(int bar) {
+  if (bar == 0)
+    __syncthreads();
+  else
+    asm volatile("bar.sync %0, 128;" ::"r"(bar) : "memory");
 }
 
-// Waits for the committed MMAs; false (uniformly) if any thread gave up,
-// in which case `phase` still names the pending completion.
-__device__ __forceinline__ bool await_mma(GuideSmem &S, uint32_t &phase) {
-  bool const ok = tc::mbar_wait(tc::smem_addr(&S.mbar), phase, kWaitLimit);
+// Uniform over the group: true if any thread's flag is set.
+__device__ __forceinline__ bool tile_any(int bar, bool flag) {
+  if (bar == 0) return __syncthreads_or(flag ? 1 : 0) != 0;
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, %2, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(r)
+      : "r"(flag ? 1u : 0u), "r"(bar)
+      : "memory");
+  return r != 0;
+}
+
+// Shared-memory writes of the group become visible to the tensor cores.
+__device__ __forceinline__ void publish(int bar) {
+  tc::fence_smem_to_async();
+  tc::fence_before_sync();
+  tile_sync(bar);
+}
+
+// Waits for the group's committed MMAs; false (uniformly) if any thread gave
+// up, in which case `phase` still names the pending completion.
+__device__ __forceinline__ bool await_mma(const Tile &c, uint32_t &phase) {
+  bool const ok = tc::mbar_wait(c.mbar, phase, kWaitLimit);
   tc::fence_after_sync();
-  int const bad = __syncthreads_or(ok ? 0 : 1);
-  if (bad) return false;
+  if (tile_any(c.bar, !ok)) return false;
   phase ^= 1u;
   return true;
 }
 
-__device__ __forceinline__ void issue_forward(GuideSmem &S, int l, const uint8_t *in) {
+__device__ __forceinline__ void issue_forward(uint32_t w_base, int l, const uint8_t *in, uint32_t tmem) {
   int const K = layer_in(l);
-  uint32_t const a0 = tc::smem_addr(in), b0 = tc::smem_addr(S.w) + wblk_off(l);
+  uint32_t const a0 = tc::smem_addr(in), b0 = w_base + wblk_off(l);
   uint32_t const id = tc::idesc_bf16(kRows, kW, false, false);
   for (int ks = 0; ks < K / 16; ++ks)
-    tc::mma_bf16(S.tmem, tc::desc_kmajor(a0 + ks * 256, K), tc::desc_kmajor(b0 + ks * 256, K), id, ks > 0);
+    tc::mma_bf16(tmem, tc::desc_kmajor(a0 + ks * 256, K), tc::desc_kmajor(b0 + ks * 256, K), id, ks > 0);
 }
 
-// This thread's row of the working accumulator (64 fp32).
-__device__ __forceinline__ void read_acc(const GuideSmem &S, float *v) {
-  uint32_t const taddr = S.tmem + ((threadIdx.x & ~31u) << 16);
+// This thread's row of an accumulator (64 fp32); a warp reads the 32 TMEM
+// lanes of its quarter (32 * (warp % 4)).
+__device__ __forceinline__ void read_acc(uint32_t tmem, float *v) {
+  uint32_t const taddr = tmem + (((threadIdx.x >> 5) & 3u) << 21);
 #pragma unroll
   for (int c = 0; c < kW; c += 16) tc::tmem_ld16(taddr + c, v + c);
   tc::tmem_wait_ld();
 }
 
-// Forward pass of the tile whose encoding is in S.x; leaves this thread's
-// row of raw outputs (with bias) in out[64].  keep: hidden layers go to
-// S.h[0..3] (training), else ping-pong in S.h[0], S.h[1].
-__device__ bool forward_tile(GuideSmem &S, uint32_t &phase, bool keep, float *out) {
-  int const r = threadIdx.x;
-  const uint8_t *in = S.x;
+// Forward pass of the tile whose encoding is in c.x; leaves this thread's row
+// of raw outputs (with bias) in out[64].
+__device__ bool forward(const uint8_t *w, const float (*bias)[kW], Tile &c, uint32_t &phase, bool keep,
+                        float *out) {
+  uint32_t const wb = tc::smem_addr(w);
+  const uint8_t *in = c.x;
   for (int l = 0; l < kLayers; ++l) {
-    publish();
-    if (threadIdx.x == 0) {
+    publish(c.bar);
+    if (c.t == 0) {
       tc::fence_after_sync();
-      issue_forward(S, l, in);
-      tc::mma_commit(tc::smem_addr(&S.mbar));
+      issue_forward(wb, l, in, c.tmem);
+      tc::mma_commit(c.mbar);
     }
-    if (!await_mma(S, phase)) return false;
+    if (!await_mma(c, phase)) return false;
     float v[kW];
-    read_acc(S, v);
+    read_acc(c.tmem, v);
     if (l == kLayers - 1) {
 #pragma unroll
-      for (int j = 0; j < kW; ++j) out[j] = v[j] + S.bias[l][j];
+      for (int j = 0; j < kW; ++j) out[j] = v[j] + bias[l][j];
       break;
     }
-    uint8_t *dst = keep ? S.h[l] : S.h[l & 1];
+    uint8_t *dst = keep ? c.h[l] : c.h[l & 1];
 #pragma unroll
-    for (int j = 0; j < kW; ++j) v[j] = fmaxf(v[j] + S.bias[l][j], 0.0f);
+    for (int j = 0; j < kW; ++j) v[j] = fmaxf(v[j] + bias[l][j], 0.0f);
 #pragma unroll
-    for (int c = 0; c < kW; c += 8) store_row8(dst, r, c, kW, v + c);
+    for (int q = 0; q < kW; q += 8) store_row8(dst, c.t, q, kW, v + q);
     in = dst;
   }
   return true;
@@ -246,64 +286,90 @@ __device__ void loss_grad(const float *o, const float w[3], float scale, float *
 }
 
 // ------------------------------------------------------------- kernels
-__device__ void load_weights(GuideSmem &S, const GuideDev &G) {
+__device__ void load_weights(uint8_t *w, float (*bias)[kW], const GuideDev &G) {
   const uint4 *src = reinterpret_cast<const uint4 *>(G.wblk);
-  uint4 *dst = reinterpret_cast<uint4 *>(S.w);
+  uint4 *dst = reinterpret_cast<uint4 *>(w);
   for (int i = threadIdx.x; i < static_cast<int>(kWBlkBytes / 16); i += blockDim.x) dst[i] = src[i];
-  for (int i = threadIdx.x; i < kLayers * kW; i += blockDim.x) {
-    int const l = i / kW, j = i % kW;
-    S.bias[l][j] = G.params[param_b(l) + j];
-  }
+  for (int i = threadIdx.x; i < kLayers * kW; i += blockDim.x) bias[i / kW][i % kW] = G.params[param_b(i / kW) + i % kW];
 }
 
-__device__ bool setup(GuideSmem &S, uint32_t ncols) {
-  if (threadIdx.x == 0) {
-    tc::mbar_init(tc::smem_addr(&S.mbar), 1);
-    S.abort = 0;
-  }
-  if (threadIdx.x < 32) tc::tmem_alloc(&S.tmem, ncols);
+// mbarriers (count 1) and `ncols` TMEM columns for the CTA.
+__device__ void setup(uint64_t *mbar, int nbar, uint32_t *tmem_slot, uint32_t ncols) {
+  if (threadIdx.x == 0)
+    for (int i = 0; i < nbar; ++i) tc::mbar_init(tc::smem_addr(&mbar[i]), 1);
+  if (threadIdx.x < 32) tc::tmem_alloc(tmem_slot, ncols);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  return true;
 }
 
-// Frees TMEM.  After a timed-out wait, first gives the MMAs still in flight
-// one more bounded wait.
-__device__ void teardown(GuideSmem &S, uint32_t ncols, bool aborted, uint32_t phase) {
-  if (aborted) tc::mbar_wait(tc::smem_addr(&S.mbar), phase, kWaitLimit);
+// Frees TMEM.  A group whose wait timed out first gives its MMAs still in
+// flight one more bounded wait.
+__device__ void teardown(uint32_t tmem, uint32_t ncols, bool aborted, uint32_t mbar, uint32_t phase) {
+  if (aborted) tc::mbar_wait(mbar, phase, kWaitLimit);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  if (threadIdx.x < 32) tc::tmem_free(S.tmem, ncols);
+  if (threadIdx.x < 32) tc::tmem_free(tmem, ncols);
+}
+
+// Inference CTAs: three groups of four warps, each with its own 128-row tile,
+// buffer and accumulator, sharing the weights; while one group waits for its
+// MMAs the others run their epilogues or gather their next rows.  A group's
+// hidden activations reuse its encoding buffer (the first layer's MMA has
+// finished reading it before the first epilogue writes).
+constexpr int kGroups = 3;
+constexpr int kInferThreads = kGroups * kRows;
+
+struct __align__(128) InferSmem {
+  uint8_t w[kWBlkBytes];
+  float bias[kLayers][kW];
+  uint8_t x[kGroups][kRows * kIn * 2];
+  uint64_t mbar[kGroups];
+  uint32_t tmem;
+};
+
+__device__ Tile infer_tile(InferSmem &S, int gi) {
+  Tile c;
+  c.x = S.x[gi];
+  c.h[0] = S.x[gi];
+  c.h[1] = S.x[gi] + kRows * kW * 2;
+  c.h[2] = c.h[3] = nullptr;
+  c.tmem = S.tmem + 64u * static_cast<uint32_t>(gi);
+  c.mbar = tc::smem_addr(&S.mbar[gi]);
+  c.bar = 1 + gi;
+  c.t = threadIdx.x & (kRows - 1);
+  return c;
 }
 
 // Raw outputs of n points (features: n x 6 = position, normal).
-__global__ void __launch_bounds__(kGuideThreads, 1)
+__global__ void __launch_bounds__(kInferThreads, 1)
     k_guide_forward(GuideDev G, const float *__restrict__ feat, int n, float *__restrict__ out) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
-  GuideSmem &S = *reinterpret_cast<GuideSmem *>(smem_raw);
-  load_weights(S, G);
-  setup(S, 64);
+  InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
+  load_weights(S.w, S.bias, G);
+  setup(S.mbar, kGroups, &S.tmem, 256);
+  int const gi = threadIdx.x >> 7;
+  Tile c = infer_tile(S, gi);
   uint32_t phase = 0;
   bool aborted = false;
   int const ntiles = (n + kRows - 1) / kRows;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    int const row = tile * kRows + threadIdx.x;
+  for (int tile = kGroups * blockIdx.x + gi; tile < ntiles; tile += kGroups * gridDim.x) {
+    int const row = tile * kRows + c.t;
     float f[6] = {0, 0, 0, 0, 0, 1};
     if (row < n)
       for (int k = 0; k < 6; ++k) f[k] = feat[6 * static_cast<int64_t>(row) + k];
-    encode_row(S, G, threadIdx.x, f);
+    encode_row(c.x, c.t, G, f);
     float o[kW];
-    if (!forward_tile(S, phase, false, o)) {
-      if (threadIdx.x == 0) atomicExch(G.err, 1);
+    if (!forward(S.w, S.bias, c, phase, false, o)) {
+      if (c.t == 0) atomicExch(G.err, 1);
       aborted = true;
       break;
     }
     if (row < n)
       for (int j = 0; j < kW; ++j) out[kW * static_cast<int64_t>(row) + j] = o[j];
   }
-  teardown(S, 64, aborted, phase);
+  teardown(S.tmem, 256, aborted, c.mbar, phase);
 }
 
 // Gradient of sum over records of -w * log p(dir) * scale, added to grad
@@ -312,9 +378,16 @@ __global__ void __launch_bounds__(kGuideThreads, 1)
     k_guide_gradient(GuideDev G, const float *__restrict__ rec, int n, float scale, float *__restrict__ grad) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
   GuideSmem &S = *reinterpret_cast<GuideSmem *>(smem_raw);
-  load_weights(S, G);
+  load_weights(S.w, S.bias, G);
   for (int i = threadIdx.x; i < kLayers * kW; i += blockDim.x) (&S.db[0][0])[i] = 0.0f;
-  setup(S, 512);
+  setup(&S.mbar, 1, &S.tmem, 512);
+  Tile c;
+  c.x = S.x;
+  for (int l = 0; l < 4; ++l) c.h[l] = S.h[l];
+  c.tmem = S.tmem;
+  c.mbar = tc::smem_addr(&S.mbar);
+  c.bar = 0;
+  c.t = threadIdx.x;
   uint32_t phase = 0;
   int const r = threadIdx.x;
   int const ntiles = (n + kRows - 1) / kRows;
@@ -330,9 +403,9 @@ __global__ void __launch_bounds__(kGuideThreads, 1)
       dir[2] = q[8];
       wgt = q[9];
     }
-    encode_row(S, G, r, f);
+    encode_row(S.x, r, G, f);
     float o[kW];
-    if (!forward_tile(S, phase, true, o)) {
+    if (!forward(S.w, S.bias, c, phase, true, o)) {
       ok = false;
       break;
     }
@@ -343,11 +416,11 @@ __global__ void __launch_bounds__(kGuideThreads, 1)
     else
       for (int j = 0; j < kW; ++j) g[j] = 0.0f;
 #pragma unroll
-    for (int c = 0; c < kW; c += 8) store_row8(S.d[0], r, c, kW, g + c);
-    // backward: layer l's delta is in S.d[db_i]
+    for (int q = 0; q < kW; q += 8) store_row8(S.d[0], r, q, kW, g + q);
+    // backward: layer l's delta is in S.d[dbuf]
     int dbuf = 0;
     for (int l = kLayers - 1; l >= 0 && ok; --l) {
-      publish();
+      publish(0);
       if (r < kW) {  // bias gradient: column sums of the (bf16) delta
         float acc = 0.0f;
         for (int m = 0; m < kRows; ++m)
@@ -372,29 +445,29 @@ __global__ void __launch_bounds__(kGuideThreads, 1)
             tc::mma_bf16(S.tmem, tc::desc_kmajor(da + ks * 256, kW),
                          tc::desc_mnmajor(wb + ks * 2 * (K / 8) * 128, K), idd, ks > 0);
         }
-        tc::mma_commit(tc::smem_addr(&S.mbar));
+        tc::mma_commit(c.mbar);
       }
-      if (!await_mma(S, phase)) {
+      if (!await_mma(c, phase)) {
         ok = false;
         break;
       }
       if (l > 0) {
         float v[kW];
-        read_acc(S, v);
+        read_acc(S.tmem, v);
         const uint8_t *hrow = S.h[l - 1];
 #pragma unroll
-        for (int c = 0; c < kW; c += 8) {
-          uint4 const q = *reinterpret_cast<const uint4 *>(hrow + tc::blocked_offset(r, c, kW));
-          uint32_t const hw[4] = {q.x, q.y, q.z, q.w};
+        for (int q = 0; q < kW; q += 8) {
+          uint4 const hq = *reinterpret_cast<const uint4 *>(hrow + tc::blocked_offset(r, q, kW));
+          uint32_t const hw[4] = {hq.x, hq.y, hq.z, hq.w};
 #pragma unroll
           for (int t = 0; t < 8; ++t) {
             uint16_t const bits = static_cast<uint16_t>(hw[t >> 1] >> (16 * (t & 1)));
-            if ((bits & 0x7FFFu) == 0u || (bits & 0x8000u)) v[c + t] = 0.0f;  // ReLU'(z) = [h > 0]
+            if ((bits & 0x7FFFu) == 0u || (bits & 0x8000u)) v[q + t] = 0.0f;  // ReLU'(z) = [h > 0]
           }
         }
         dbuf ^= 1;
 #pragma unroll
-        for (int c = 0; c < kW; c += 8) store_row8(S.d[dbuf], r, c, kW, v + c);
+        for (int q = 0; q < kW; q += 8) store_row8(S.d[dbuf], r, q, kW, v + q);
       }
     }
     first = false;
@@ -410,18 +483,135 @@ __global__ void __launch_bounds__(kGuideThreads, 1)
     int const nrow = warp * 16 + lane;  // output unit of this lane (lanes < 16)
     for (int l = 0; l < kLayers; ++l) {
       int const K = layer_in(l);
-      for (int c = 0; c < K; c += 16) {
+      for (int q = 0; q < K; q += 16) {
         float v[16];
-        tc::tmem_ld16(S.tmem + lane_base + dw_col(l) + c, v);
+        tc::tmem_ld16(S.tmem + lane_base + dw_col(l) + q, v);
         tc::tmem_wait_ld();
         if (lane < 16)
-          for (int t = 0; t < 16; ++t) atomicAdd(&grad[param_w(l) + (c + t) * kW + nrow], v[t]);
+          for (int t = 0; t < 16; ++t) atomicAdd(&grad[param_w(l) + (q + t) * kW + nrow], v[t]);
       }
     }
     for (int i = threadIdx.x; i < kLayers * kW; i += blockDim.x)
       atomicAdd(&grad[param_b(i / kW) + i % kW], (&S.db[0][0])[i]);
   }
-  teardown(S, 512, !ok, phase);
+  teardown(S.tmem, 512, !ok, c.mbar, phase);
+}
+
+// Guide inference for a render's extension queue: the hit point and shading
+// normal of every queue entry (computed as the shading kernel does) through
+// the network; per entry the mixture (weights, concentrations, means) as 40
+// fp16 values.  Persistent CTAs of three groups; the queue length is read on
+// the device.
+struct InferArgs {
+  const float4 *qo, *qd, *hits;
+  const int32_t *count;
+  const float4 *tri_ng, *tri_sn;
+  __half *mix;
+};
+
+// Surface point (position, shading normal facing the incoming ray) of queue
+// entry i, as the shading kernel computes it; the default row for a miss.
+__device__ void infer_features(const InferArgs &I, int i, float4 h, float f[6]) {
+  f[0] = f[1] = f[2] = f[3] = f[4] = 0.0f;
+  f[5] = 1.0f;
+  int32_t const code = __float_as_int(h.w);
+  if (code < 0) return;
+  int const tri = code >> 1;
+  float4 const o4 = I.qo[i], d4 = I.qd[i];
+  f3 const pos = add3(xyz3(o4), scl3(xyz3(d4), h.x));
+  f3 sn;
+  if (I.tri_sn) {
+    f3 const n0 = xyz3(__ldg(&I.tri_sn[3 * tri])), s1 = xyz3(__ldg(&I.tri_sn[3 * tri + 1])),
+             s2 = xyz3(__ldg(&I.tri_sn[3 * tri + 2]));
+    sn = normalize3(add3(add3(n0, scl3(s1, h.y)), scl3(s2, h.z)));
+  } else {
+    f3 const gn = xyz3(__ldg(&I.tri_ng[tri]));
+    f3 const z = mk3(0.0f, 0.0f, 0.0f);
+    sn = normalize3(add3(add3(gn, scl3(z, h.y)), scl3(z, h.z)));
+  }
+  if (code & 1) sn = neg3(sn);
+  f[0] = pos.x, f[1] = pos.y, f[2] = pos.z, f[3] = sn.x, f[4] = sn.y, f[5] = sn.z;
+}
+
+__global__ void __launch_bounds__(kInferThreads, 1) k_guide_infer(GuideDev G, InferArgs I) {
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
+  load_weights(S.w, S.bias, G);
+  setup(S.mbar, kGroups, &S.tmem, 256);
+  int const gi = threadIdx.x >> 7;
+  Tile c = infer_tile(S, gi);
+  uint32_t phase = 0;
+  bool aborted = false;
+  int const n = *I.count;
+  int const ntiles = (n + kRows - 1) / kRows;
+  int const step = kGroups * gridDim.x;
+  int tile = kGroups * blockIdx.x + gi;
+  // the hit record of this thread's row of the next tile is loaded one tile ahead
+  float4 hnext = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+  if (tile < ntiles && tile * kRows + c.t < n) hnext = I.hits[tile * kRows + c.t];
+  for (; tile < ntiles; tile += step) {
+    int const i = tile * kRows + c.t;
+    float f[6];
+    infer_features(I, i, i < n ? hnext : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1)), f);
+    int const inext = (tile + step) * kRows + c.t;
+    if (tile + step < ntiles && inext < n) hnext = I.hits[inext];
+    encode_row(c.x, c.t, G, f);
+    float o[kW];
+    if (!forward(S.w, S.bias, c, phase, false, o)) {
+      if (c.t == 0) atomicExch(G.err, 1);
+      aborted = true;
+      break;
+    }
+    if (i < n) {
+      float mx = o[0];
+      for (int j = 1; j < 8; ++j) mx = fmaxf(mx, o[j]);
+      float e[8], se = 0.0f;
+      for (int j = 0; j < 8; ++j) {
+        e[j] = expf(o[j] - mx);
+        se += e[j];
+      }
+      __half hv[40];
+      for (int j = 0; j < 8; ++j) {
+        float const k = expf(fminf(fmaxf(o[8 + j], -5.0f), 8.0f));
+        float const x = o[16 + 3 * j], y = o[17 + 3 * j], z = o[18 + 3 * j];
+        float const r = 1.0f / sqrtf(x * x + y * y + z * z + 1e-12f);
+        hv[5 * j] = __float2half_rn(e[j] / se);
+        hv[5 * j + 1] = __float2half_rn(k);
+        hv[5 * j + 2] = __float2half_rn(x * r);
+        hv[5 * j + 3] = __float2half_rn(y * r);
+        hv[5 * j + 4] = __float2half_rn(z * r);
+      }
+      uint4 *dst = reinterpret_cast<uint4 *>(I.mix + 40 * static_cast<int64_t>(i));
+      for (int t = 0; t < 5; ++t) dst[t] = reinterpret_cast<const uint4 *>(hv)[t];
+    }
+  }
+  teardown(S.tmem, 256, aborted, c.mbar, phase);
+}
+
+// Training records of a guided wave -> (position, normal, direction, weight)
+// rows: weight = Y of the incident radiance estimate along the sampled
+// direction, (L_path - L_before) / throughput, times the cosine, over the
+// sampling density.  Rows with no weight are dropped.
+__global__ void k_guide_records(const float *__restrict__ rec, int tb, int64_t npaths,
+                                const float4 *__restrict__ radiance, float *__restrict__ out, int *count,
+                                int64_t cap) {
+  int64_t const stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < npaths * tb;
+       idx += stride) {
+    const float *r = rec + idx * 16;
+    float const q = r[9];
+    if (!(q > 0.0f) || isnan(r[14]) || !(r[11] > 0.0f)) continue;
+    float4 const L = radiance[idx / tb];
+    float const li = (L.y - r[14]) / r[11];
+    float const cs = r[3] * r[6] + r[4] * r[7] + r[5] * r[8];
+    float const w = li * cs / q;
+    if (!(w > 0.0f) || !isfinite(w)) continue;
+    int const j = atomicAdd(count, 1);
+    if (j >= cap) continue;
+    float *o = out + 10 * static_cast<int64_t>(j);
+    for (int t = 0; t < 9; ++t) o[t] = r[t];
+    o[9] = w;
+  }
 }
 
 // fp32 master weights -> blocked bf16 W^T per layer.
@@ -464,6 +654,14 @@ struct GuideImpl {
   int *d_err = nullptr;
   int64_t step = 0;
   float lo[3] = {0, 0, 0}, inv_ext[3] = {1, 1, 1};
+  // guided-render buffers
+  __half *d_mix = nullptr;
+  int64_t mix_cap = 0;
+  float *d_rec = nullptr, *d_train = nullptr;
+  int64_t rec_cap = 0;  // paths
+  int *d_count = nullptr;
+  int64_t train_offset = 0;
+  uint64_t trained_records = 0;
 };
 
 namespace {
@@ -515,11 +713,12 @@ int guide_forward_launch(GuideImpl &g, const float *feat, int n, float *out, cud
   static bool attr = false;
   if (!attr) {
     XYZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(sizeof(GuideSmem))));
+                                      static_cast<int>(sizeof(InferSmem))));
     attr = true;
   }
   if (n <= 0) return XYZGPU_OK;
-  k_guide_forward<<<grid_for(g.device, n), kGuideThreads, sizeof(GuideSmem), st>>>(guide_dev(g), feat, n, out);
+  int const grid = std::max(1, std::min((n + kGroups * kRows - 1) / (kGroups * kRows), sm_count(g.device)));
+  k_guide_forward<<<grid, kInferThreads, sizeof(InferSmem), st>>>(guide_dev(g), feat, n, out);
   XYZ_CUDA_TRY(cudaGetLastError());
   return XYZGPU_OK;
 }
@@ -535,6 +734,83 @@ int guide_gradient_launch(GuideImpl &g, const float *rec, int n, float scale, fl
   k_guide_gradient<<<grid_for(g.device, n), kGuideThreads, sizeof(GuideSmem), st>>>(guide_dev(g), rec, n, scale,
                                                                                      grad);
   XYZ_CUDA_TRY(cudaGetLastError());
+  return XYZGPU_OK;
+}
+
+int guide_wave_prepare(GuideImpl &g, int64_t cap, bool train, cudaStream_t st, GuideWave *out) {
+  if (g.mix_cap < cap) {
+    XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFree(g.d_mix);
+    g.d_mix = nullptr;
+    g.mix_cap = 0;
+    cudaError_t const e = cudaMalloc(reinterpret_cast<void **>(&g.d_mix), static_cast<size_t>(cap) * 40 * sizeof(__half));
+    if (e != cudaSuccess) return set_error(XYZGPU_E_NOMEM, "render_guided: mixture buffer: %s", cudaGetErrorString(e));
+    g.mix_cap = cap;
+  }
+  int const tb = g.cfg.train_bounces;
+  if (train && tb > 0 && g.rec_cap < cap) {
+    XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFree(g.d_rec);
+    cudaFree(g.d_train);
+    g.d_rec = g.d_train = nullptr;
+    g.rec_cap = 0;
+    size_t const n = static_cast<size_t>(cap) * tb;
+    if (cudaMalloc(reinterpret_cast<void **>(&g.d_rec), n * 16 * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void **>(&g.d_train), n * 10 * sizeof(float)) != cudaSuccess)
+      return set_error(XYZGPU_E_NOMEM, "render_guided: training record buffers of %zu records", n);
+    g.rec_cap = cap;
+  }
+  if (!g.d_count) XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&g.d_count), sizeof(int)));
+  out->mix = g.d_mix;
+  out->records = train && tb > 0 ? g.d_rec : nullptr;
+  out->train_bounces = train ? tb : 0;
+  out->alpha = g.cfg.alpha;
+  return XYZGPU_OK;
+}
+
+int guide_infer_launch(GuideImpl &g, const float4 *qo, const float4 *qd, const float4 *hits,
+                       const int32_t *count, const DevScene &S, void *mix, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    XYZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(sizeof(InferSmem))));
+    attr = true;
+  }
+  InferArgs I{qo, qd, hits, count, S.tri_ng, S.tri_sn, static_cast<__half *>(mix)};
+  k_guide_infer<<<sm_count(g.device), kInferThreads, sizeof(InferSmem), st>>>(guide_dev(g), I);
+  XYZ_CUDA_TRY(cudaGetLastError());
+  return XYZGPU_OK;
+}
+
+int guide_adam_launch(GuideImpl &g, cudaStream_t st);
+
+// After a training wave: records -> training rows, then steps_per_pass Adam
+// steps on batches of batch_size rows (cycling through the rows).
+int guide_train_on_wave(GuideImpl &g, const float4 *radiance, int64_t npaths, cudaStream_t st) {
+  int const tb = g.cfg.train_bounces;
+  if (tb <= 0 || g.cfg.steps_per_pass <= 0 || !g.d_rec) return XYZGPU_OK;
+  int64_t const cap = npaths * tb;
+  XYZ_CUDA_TRY(cudaMemsetAsync(g.d_count, 0, sizeof(int), st));
+  int const blocks = std::max(1, std::min<int>(static_cast<int>((cap + 255) / 256), sm_count(g.device) * 8));
+  k_guide_records<<<blocks, 256, 0, st>>>(g.d_rec, tb, npaths, radiance, g.d_train, g.d_count, cap);
+  XYZ_CUDA_TRY(cudaGetLastError());
+  int count = 0;
+  XYZ_CUDA_TRY(cudaMemcpyAsync(&count, g.d_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+  XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+  int64_t const rows = std::min<int64_t>(count, cap);
+  g.trained_records += static_cast<uint64_t>(rows);
+  if (rows <= 0) return XYZGPU_OK;
+  int64_t const bs = std::min<int64_t>(g.cfg.batch_size, rows);
+  for (int s = 0; s < g.cfg.steps_per_pass; ++s) {
+    int64_t off = (g.train_offset + s * bs) % rows;
+    if (off + bs > rows) off = rows - bs;
+    int rc = guide_gradient_launch(g, g.d_train + 10 * off, static_cast<int>(bs), 1.0f / static_cast<float>(bs),
+                                   g.d_grad, st);
+    if (rc) return rc;
+    rc = guide_adam_launch(g, st);
+    if (rc) return rc;
+  }
+  g.train_offset += g.cfg.steps_per_pass * bs;
   return XYZGPU_OK;
 }
 
@@ -582,6 +858,10 @@ void xyzgpu_guide_destroy(xyzgpu_guide h) {
   cudaFree(g.d_v);
   cudaFree(g.d_wblk);
   cudaFree(g.d_err);
+  cudaFree(g.d_mix);
+  cudaFree(g.d_rec);
+  cudaFree(g.d_train);
+  cudaFree(g.d_count);
   cudaSetDevice(prev);
   delete h;
 }
@@ -693,6 +973,44 @@ int xyzgpu_guide_gradient(xyzgpu_guide h, const float *records, int n, float sca
   int const rc = guide_gradient_launch(g, records, n, scale, grad, st);
   if (rc) return rc;
   return check_err(g, st, "guide_gradient");
+}
+
+int xyzgpu_render_guided(xyzgpu_guide h, const xyzgpu_camera *cam, const xyzgpu_render_params *rp, int train,
+                         float *film, void *stream) {
+  clear_error();
+  if (!h || !cam || !rp || !film) return set_error(XYZGPU_E_INVALID, "render_guided: null argument");
+  if (rp->spectral != XYZGPU_SPECTRAL_OFF || (rp->profile != XYZGPU_PROFILE_OFF && rp->profile != XYZGPU_PROFILE_TIMING))
+    return set_error(XYZGPU_E_INVALID, "render_guided: the XYZ film mode only, profile off or timing");
+  if (rp->width <= 0 || rp->height <= 0 || rp->spp < 0 || rp->spp_offset < 0 || rp->max_depth < 1 ||
+      rp->max_depth > 1000 || rp->rr_start_depth < 1 || !(rp->rr_threshold >= 0.0f) || rp->wave_paths < 0 ||
+      (rp->film_location != XYZGPU_FILM_DEVICE && rp->film_location != XYZGPU_FILM_HOST) ||
+      !((rp->row_begin == 0 && rp->row_end == 0) ||
+        (rp->row_begin >= 0 && rp->row_begin < rp->row_end && rp->row_end <= rp->height)))
+    return set_error(XYZGPU_E_INVALID, "render_guided: parameters out of range");
+  if (static_cast<int64_t>(rp->width) * rp->height >= (1ll << 31) ||
+      static_cast<int64_t>(rp->spp_offset) + rp->spp >= (1ll << 32))
+    return set_error(XYZGPU_E_LIMIT, "render_guided: image or sample index too large");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(cam->eye[k]) || !std::isfinite(cam->at[k]))
+      return set_error(XYZGPU_E_INVALID, "render_guided: camera position is not finite");
+  if (!(cam->film_size > 0) || !(cam->focal_length > 0) || !(cam->f_number > 0))
+    return set_error(XYZGPU_E_INVALID, "render_guided: camera film size, focal length and F-number must be > 0");
+  GuideImpl &g = h->g;
+  cudaStream_t const st = static_cast<cudaStream_t>(stream);
+  XYZ_CUDA_TRY(cudaSetDevice(g.device));
+  XYZ_CUDA_TRY(cudaMemsetAsync(g.d_err, 0, sizeof(int), st));
+  GuideHooks hooks{&g, train != 0};
+  int const rc = render_launch(*g.scene, *cam, *rp, film, st, nullptr, &hooks);
+  if (rc) return rc;
+  return check_err(g, st, "render_guided");
+}
+
+int xyzgpu_guide_stats_get(xyzgpu_guide h, xyzgpu_guide_stats *out) {
+  clear_error();
+  if (!h || !out) return set_error(XYZGPU_E_INVALID, "guide_stats_get: null argument");
+  out->adam_steps = static_cast<uint64_t>(h->g.step);
+  out->trained_records = h->g.trained_records;
+  return XYZGPU_OK;
 }
 
 int xyzgpu_guide_train_step(xyzgpu_guide h, const float *records, int n, void *stream) {

@@ -10,6 +10,7 @@
 namespace xyzgpu {
 namespace {
 constexpr int64_t kMaxDefaultWave = int64_t{1} << 26;
+constexpr int64_t kMaxGuidedWave = int64_t{1} << 23;
 }  // namespace
 
 extern const int64_t kBytesPerPath = 3 * sizeof(float4) + sizeof(uint32_t) +  // beta, radiance, hits, misc
@@ -99,10 +100,14 @@ void render_workspace_free(RenderWorkspace &w) {
 }
 
 int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp, float *film,
-                  cudaStream_t st, const AdjointArgs *adj) {
+                  cudaStream_t st, const AdjointArgs *adj, const GuideHooks *guide) {
   XYZ_CUDA_TRY(cudaSetDevice(s.device));
-  int64_t const npix_total = static_cast<int64_t>(rp.width) * rp.height;
-  int64_t const film_elems = 3 * npix_total;
+  // a band of rows renders the same pixels (and paths) as the full image
+  int64_t const row0 = rp.row_end > 0 ? rp.row_begin : 0;
+  int64_t const rows = rp.row_end > 0 ? rp.row_end - rp.row_begin : rp.height;
+  int64_t const pix_first = row0 * rp.width;
+  int64_t const npix_total = static_cast<int64_t>(rp.width) * rows;
+  int64_t const film_elems = 3 * static_cast<int64_t>(rp.width) * rp.height;
   int const iters = rp.max_depth;
 
   CamDev const C = camera_setup(cam, rp.width, rp.height);
@@ -123,6 +128,8 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       cap = std::min(cap, std::max<int64_t>(afford, int64_t{1} << 20));
     }
     cap = std::max(cap, sw.ws.capacity);
+    // guided waves also hold a mixture (80 B) and training records per path
+    if (guide) cap = std::min<int64_t>(cap, kMaxGuidedWave);
   }
   if (sw.done && sw.last != st) XYZ_CUDA_TRY(cudaStreamWaitEvent(st, sw.done, 0));
   int rc = ensure_wave_buffers(sw.ws, cap, iters);
@@ -170,7 +177,7 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
     g_raygen = occupancy_grid(k_raygen<false>, s.device);
     g_trace_e = occupancy_grid(k_trace_queue<false, false>, s.device);
     g_trace_s = occupancy_grid(k_trace_queue<true, false>, s.device);
-    g_shade = occupancy_grid(k_shade<false>, s.device);
+    g_shade = occupancy_grid(k_shade<kModePlain>, s.device);
     g_shade_sp = occupancy_grid(k_shade_spectral, s.device);
     g_film = occupancy_grid(k_film, s.device);
   }
@@ -231,6 +238,15 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
     A.g_alb = adj->g_albedo;
     A.g_em = adj->g_emission;
   }
+  GuideWave gw;
+  if (guide) {
+    int const r = guide_wave_prepare(*guide->g, cap, guide->train, st, &gw);
+    if (r) return r;
+    A.mix = static_cast<const __half *>(gw.mix);
+    A.guide_alpha = gw.alpha;
+    A.records = gw.records;
+    A.train_bounces = gw.train_bounces;
+  }
 
   xyzgpu_render_counters rc_out{};
   uint64_t launches = 0;
@@ -240,12 +256,14 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   for (int64_t s0 = 0; s0 < rp.spp; s0 += spp_per_wave) {
     int const ns = static_cast<int>(std::min<int64_t>(spp_per_wave, rp.spp - s0));
     for (int64_t p0 = 0; p0 < npix_total; p0 += pix_per_wave) {
-      A.p0 = p0;
+      A.p0 = pix_first + p0;
       A.npix = std::min<int64_t>(pix_per_wave, npix_total - p0);
       A.s0 = static_cast<uint32_t>(rp.spp_offset + s0);
       A.nsamp = ns;
       A.npaths = A.npix * ns;
       XYZ_CUDA_TRY(cudaMemsetAsync(wv.counts, 0, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t), st));
+      if (A.train_bounces > 0)
+        XYZ_CUDA_TRY(cudaMemsetAsync(A.records, 0, static_cast<size_t>(A.npaths) * A.train_bounces * 16 * sizeof(float), st));
       int const gr = static_cast<int>(std::min<int64_t>(g_raygen, (A.npaths + kThreads - 1) / kThreads));
 #define XYZ_MARK(cls, start)              \
   do {                                    \
@@ -266,19 +284,31 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
           else
             k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, pc);
           XYZ_MARK(1, false);
+          // (the last bounce only meets the depth cap: no sampling, no inference)
+          if (guide && b < iters - 1) {
+            int const qi = b & 1;
+            int const r = guide_infer_launch(*guide->g, A.q_o[qi], A.q_d[qi], A.hits,
+                                             A.counts + b * kCountStride + kCExt, A.S, gw.mix, st);
+            if (r) return r;
+            ++launches;
+          }
           XYZ_MARK(2, true);
           if (spectral)
             k_shade_spectral<<<g_shade_sp, kThreads, 0, st>>>(A, b);
+          else if (guide)
+            k_shade<kModeGuided><<<g_shade, kThreads, 0, st>>>(A, b);
           else if (replay)
-            k_shade<true><<<g_shade, kThreads, 0, st>>>(A, b);
+            k_shade<kModeAdjoint><<<g_shade, kThreads, 0, st>>>(A, b);
           else
-            k_shade<false><<<g_shade, kThreads, 0, st>>>(A, b);
+            k_shade<kModePlain><<<g_shade, kThreads, 0, st>>>(A, b);
           XYZ_MARK(2, false);
           XYZ_MARK(3, true);
           if (counting)
             k_trace_queue<true, true><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
           else if (replay)
-            k_trace_queue<true, false, true><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
+            k_trace_queue<true, false, kModeAdjoint><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
+          else if (guide)
+            k_trace_queue<true, false, kModeGuided><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
           else
             k_trace_queue<true, false><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
           XYZ_MARK(3, false);
@@ -309,6 +339,10 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       k_tally<<<1, 32, 0, st>>>(A, iters, w.tally);
       ++launches;
       XYZ_CUDA_TRY(cudaGetLastError());
+      if (guide && A.train_bounces > 0) {
+        int const r = guide_train_on_wave(*guide->g, A.radiance, A.npaths, st);
+        if (r) return r;
+      }
       rc_out.paths += static_cast<uint64_t>(A.npaths);
       rc_out.waves += 1;
     }
@@ -493,7 +527,7 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
     g_raygen = occupancy_grid(k_raygen<false>, s.device);
     g_trace_e = occupancy_grid(k_trace_queue<false, false>, s.device);
     g_trace_s = occupancy_grid(k_trace_queue<true, false>, s.device);
-    g_shade = occupancy_grid(k_shade<false>, s.device);
+    g_shade = occupancy_grid(k_shade<kModePlain>, s.device);
     g_film = occupancy_grid(k_film, s.device);
   }
   int64_t const npix_total = static_cast<int64_t>(rp.width) * rp.height;
@@ -518,7 +552,7 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
       k_raygen<false><<<gr, kThreads, 0, st>>>(A);
       for (int b = 0; b < iters; ++b) {
         k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, tally + 8);
-        k_shade<false><<<g_shade, kThreads, 0, st>>>(A, b);
+        k_shade<kModePlain><<<g_shade, kThreads, 0, st>>>(A, b);
         k_trace_queue<true, false><<<g_trace_s, kThreads, 0, st>>>(A, b, tally + 8);
       }
       int const gf = static_cast<int>(std::min<int64_t>(g_film, (A.npix + kThreads - 1) / kThreads));

@@ -105,8 +105,27 @@ struct AdjointArgs {
   float *g_emission;
 };
 
+// Guided render (xyzgpu_render_guided): the guide's per-wave buffers and
+// hooks (guide.cu).
+struct GuideImpl;
+struct GuideWave {
+  void *mix = nullptr;       // fp16, 40 per extension-queue entry
+  float *records = nullptr;  // training records of the wave (16 floats x train_bounces per path)
+  int train_bounces = 0;     // 0: no training records
+  float alpha = 0.5f;
+};
+struct GuideHooks {
+  GuideImpl *g;
+  bool train;
+};
+int guide_wave_prepare(GuideImpl &g, int64_t capacity, bool train, cudaStream_t st, GuideWave *out);
+int guide_infer_launch(GuideImpl &g, const float4 *qo, const float4 *qd, const float4 *hits,
+                       const int32_t *count, const DevScene &S, void *mix, cudaStream_t st);
+int guide_train_on_wave(GuideImpl &g, const float4 *radiance, int64_t npaths, cudaStream_t st);
+
 int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp,
-                  float *film, cudaStream_t st, const AdjointArgs *adj = nullptr);
+                  float *film, cudaStream_t st, const AdjointArgs *adj = nullptr,
+                  const GuideHooks *guide = nullptr);
 void render_workspace_free(RenderWorkspace &ws);
 int render_collect(SceneImpl &s);
 int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp,

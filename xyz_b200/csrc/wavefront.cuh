@@ -33,6 +33,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <cuda_fp16.h>
+
 #include "scene.h"
 #include "spectral.h"
 #include "traverse.cuh"
@@ -82,6 +84,10 @@ struct WaveBlock {
   int64_t pix_off;   // first film thread of the block (film kernel)
 };
 
+// Variants of the shading and shadow kernels: the plain render, the replay
+// pass of the adjoint, batched renders and guided renders.
+enum WaveMode : int { kModePlain = 0, kModeAdjoint = 1, kModeBatch = 2, kModeGuided = 3 };
+
 struct WaveArgs {
   DevScene S;
   CamDev cam;
@@ -122,7 +128,85 @@ struct WaveArgs {
   const WaveBlock *blocks;
   int n_blocks;
   int64_t film_threads;  // pixels of all blocks of the wave
+  // guided renders: the guide's mixture per extension-queue entry (40 fp16:
+  // per lobe weight, concentration, mean xyz), the one-sample MIS probability
+  // of the guide, and training records (16 floats x train_bounces per path:
+  // position, normal, direction, pdf, throughput after the vertex, radiance
+  // before the next vertex)
+  const __half *mix;
+  float guide_alpha;
+  float *records;
+  int train_bounces;
 };
+
+// ------------------------------------------------------- guide mixture
+// von Mises-Fisher lobes: vMF(d; mu, k) = k / (2 pi (1 - e^{-2k})) exp(k (mu.d - 1)).
+// Loaded weights are renormalised and means normalised, so sampling and the
+// pdf use the same exact mixture whatever the fp16 rounding.
+struct GuideMix {
+  float w[8], k[8], c[8];
+  f3 mu[8];
+};
+
+XYZ_DEV void load_mix(const __half *src, GuideMix &M) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(src);
+  __half h[40];
+#pragma unroll
+  for (int t = 0; t < 5; ++t) reinterpret_cast<uint4 *>(h)[t] = q[t];
+  float ws = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    float const w = fmaxf(__half2float(h[5 * i]), 0.0f);
+    float const k = fmaxf(__half2float(h[5 * i + 1]), 1e-3f);
+    f3 m = mk3(__half2float(h[5 * i + 2]), __half2float(h[5 * i + 3]), __half2float(h[5 * i + 4]));
+    float const l2 = dot3(m, m);
+    m = l2 > 0.0f ? scl3(m, 1.0f / sqrtf(l2)) : mk3(0.0f, 0.0f, 1.0f);
+    M.w[i] = w;
+    M.k[i] = k;
+    M.c[i] = k / (static_cast<float>(2.0 * kPi) * -expm1f(-2.0f * k));
+    M.mu[i] = m;
+    ws += w;
+  }
+  float const inv = ws > 0.0f ? 1.0f / ws : 0.125f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) M.w[i] = ws > 0.0f ? M.w[i] * inv : inv;
+}
+
+XYZ_DEV float mix_pdf(const GuideMix &M, f3 d) {
+  float p = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) p += M.w[i] * M.c[i] * expf(M.k[i] * (dot3(M.mu[i], d) - 1.0f));
+  return p;
+}
+
+// Lobe by weight, then the lobe's cosine w = 1 + log(u1 + (1 - u1) e^{-2k}) / k
+// (Jakob, "Numerically stable sampling of the von Mises-Fisher distribution
+// on S^2", 2012) around its mean, in the orthonormal basis of Duff et al.,
+// "Building an Orthonormal Basis, Revisited" (JCGT 2017).
+XYZ_DEV f3 mix_sample(const GuideMix &M, float ul, float u1, float u2) {
+  int j = 7;
+  float acc = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    acc += M.w[i];
+    if (ul < acc) {
+      j = i;
+      break;
+    }
+  }
+  float const k = M.k[j];
+  float w = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * k)) / k;
+  w = fminf(fmaxf(w, -1.0f), 1.0f);
+  float const sw = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+  float const ph = static_cast<float>(2.0 * kPi) * u2;
+  f3 const n = M.mu[j];
+  float const sign = copysignf(1.0f, n.z);
+  float const a = -1.0f / (sign + n.z);
+  float const bb = n.x * n.y * a;
+  f3 const t = mk3(1.0f + sign * n.x * n.x * a, sign * bb, -sign * n.x);
+  f3 const bt = mk3(bb, sign + n.y * n.y * a, -n.y);
+  return add3(add3(scl3(t, sw * cosf(ph)), scl3(bt, sw * sinf(ph))), scl3(n, w));
+}
 
 XYZ_DEV uint32_t pack_misc(uint32_t dim, uint32_t k, uint32_t specular) {
   return (dim & 0xffffu) | ((k & 0x7fffu) << 16) | (specular << 31);
@@ -316,8 +400,11 @@ struct ExtSink {
   }
 };
 
-template <bool kSpec, bool kAdj, bool kBatch = false>
+template <bool kSpec, int kMode = kModePlain>
 struct ShadowSink {
+  static constexpr bool kAdj = kMode == kModeAdjoint;
+  static constexpr bool kBatch = kMode == kModeBatch;
+  static constexpr bool kGuide = kMode == kModeGuided;
   const WaveArgs *A;
   uint32_t visible;
   XYZ_DEV void load(int i, f3 &o, f3 &d, float &tmin, float &tmax) const {
@@ -334,7 +421,9 @@ struct ShadowSink {
     if (h.id < 0 || h.id != A->s_target[i]) return;
     // Lambert::CalculateWeightedDirectLighting, lambert.cpp:157-172
     float const G = A->s_d[i].w / (h.t * h.t);  // nk2 * nk3 / t^2
-    float const dimp = static_cast<float>(kInvPi * static_cast<double>(G));
+    float dimp = static_cast<float>(kInvPi * static_cast<double>(G));
+    // guided: the sampling density is the guide / Lambert mixture, rho times Lambert's
+    if (kGuide) dimp *= __int_as_float(A->s_slot[i]);
     float const light_area = kBatch ? scene(i)->light_area : A->S.light_area;
     float const dexp = 1.0f / light_area;
     float const dens = dimp / dexp;
@@ -368,32 +457,29 @@ struct ShadowSink {
   }
 };
 
-template <bool kShadow, bool kCount, bool kAdj = false, bool kBatch = false>
+template <bool kShadow, bool kCount, int kMode = kModePlain>
 __global__ void __launch_bounds__(kThreads) k_trace_queue(WaveArgs A, int b,
                                                           unsigned long long *prof) {
+  constexpr bool kBatch = kMode == kModeBatch;
   int32_t *const cnt = A.counts + b * kCountStride;
   int const n = kShadow ? cnt[kCShadow] : cnt[kCExt];
   int const lane = threadIdx.x & 31;
   int const qi = b & 1;
   TraceCount tc{0u, 0u, 0u};
   uint32_t visible = 0;
-  if (kShadow && kBatch) {
-    ShadowSink<false, false, true> sink{&A, 0u};
-    trace_persistent<kCount, true>(A.S, n, &cnt[kCFetchSh], sink, tc);
+  if (kShadow && kMode != kModePlain) {
+    ShadowSink<false, kMode> sink{&A, 0u};
+    trace_persistent<kCount, kBatch>(A.S, n, &cnt[kCFetchSh], sink, tc);
     visible = sink.visible;
   } else if (kBatch) {
     ExtSink<true> sink{A.q_o[qi], A.q_d[qi], A.hits, &A};
     trace_persistent<kCount, true>(A.S, n, &cnt[kCFetchExt], sink, tc);
-  } else if (kShadow && kAdj) {
-    ShadowSink<false, true> sink{&A, 0u};
-    trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
-    visible = sink.visible;
   } else if (kShadow && A.spectral) {
-    ShadowSink<true, false> sink{&A, 0u};
+    ShadowSink<true> sink{&A, 0u};
     trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
     visible = sink.visible;
   } else if (kShadow) {
-    ShadowSink<false, false> sink{&A, 0u};
+    ShadowSink<false> sink{&A, 0u};
     trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
     visible = sink.visible;
   } else {
@@ -488,10 +574,14 @@ XYZ_DEV LightSample sample_light(const DevScene &S, uint64_t seed, uint32_t pixe
   return L;
 }
 
-// kAdj: the replay pass of xyzgpu_adjoint (same path, plus gradients).
-// kBatch: paths of many scenes (xyzgpu_batch_*).
-template <bool kAdj, bool kBatch = false>
+// kModeAdjoint: the replay pass of xyzgpu_adjoint (same path, plus gradients).
+// kModeBatch: paths of many scenes (xyzgpu_batch_*).
+// kModeGuided: directions from the learned guide mixed with Lambert sampling.
+template <int kMode>
 __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
+  constexpr bool kAdj = kMode == kModeAdjoint;
+  constexpr bool kBatch = kMode == kModeBatch;
+  constexpr bool kGuide = kMode == kModeGuided;
   int32_t *const cnt = A.counts + b * kCountStride;
   int32_t *const cnt_next = A.counts + (b + 1) * kCountStride;
   int const n = cnt[kCExt];
@@ -508,6 +598,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
     float4 beta4{};
     uint32_t misc = 0;
     int32_t light_mat = 0;
+    float rho = 1.0f;
     int block = 0;
     if (i < n) {
       slot = A.q_slot[qi][i];
@@ -521,6 +612,14 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
         DevScene const &S = scene_of<kBatch>(A, block);
         PathParams const P = params_of<kBatch>(A, block);
         f3 const d = xyz3(d4);
+        if (kGuide && b >= 1 && b - 1 < A.train_bounces) {
+          // radiance gathered before this vertex: closes the previous vertex's record
+          float4 const L = A.radiance[slot];
+          float *rec = A.records + (static_cast<int64_t>(slot) * A.train_bounces + (b - 1)) * 16;
+          rec[13] = L.x;
+          rec[14] = L.y;
+          rec[15] = L.z;
+        }
         // Triangle::ShadingBasis (triangle.cpp:194-219)
         float4 const g4 = __ldg(&S.tri_ng[tri]);
         f3 gn = xyz3(g4);
@@ -603,6 +702,8 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
             if (static_cast<int>(k) >= P.kmax) alive = false;
           }
           uint32_t pixel = 0, sample = 0;
+          GuideMix M;
+          if (kGuide && alive && !is_light) load_mix(A.mix + 40 * static_cast<int64_t>(i), M);
           if (alive) {
             path_pixel_sample<kBatch>(A, block, slot, &pixel, &sample);
             if (!is_light) {
@@ -633,15 +734,28 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
                     pbv = mul3(S.power, beta);
                     light_mat = ls.mat;
                     if (!kAdj) pbv = scl3(pbv, __ldg(&S.emission[ls.mat]));
+                    if (kGuide) {
+                      float const pl = nk2 * static_cast<float>(kInvPi);
+                      rho = (A.guide_alpha * mix_pdf(M, neg3(v)) + (1.0f - A.guide_alpha) * pl) / pl;
+                    }
                   }
                 }
               }
             }
             PathRng rng;
             rng.init(P.seed, pixel, sample, dim);
+            // guided: the product of the guide / Lambert density ratios so far
+            // (radiance.w), so that Russian roulette sees the throughput the
+            // path would have with Lambert sampling and does not end paths
+            // for being sent towards bright regions
+            float rr_scale = 1.0f;
+            if (kGuide) {
+              float const w = reinterpret_cast<const float *>(A.radiance + slot)[3];
+              rr_scale = w > 0.0f ? w : 1.0f;
+            }
             // Russian roulette (scene_pathtracing.cpp:128-137)
             if (static_cast<int>(k) - 1 >= P.rr_start) {
-              float const ty = beta.y;
+              float const ty = kGuide ? beta.y * rr_scale : beta.y;
               if (ty < P.rr_threshold) {
                 float const q = ty / P.rr_threshold;
                 if (rng.next() >= q) {
@@ -652,7 +766,44 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
               }
             }
             if (alive && is_light) alive = false;  // Light::NextScatteringDirection
-            if (alive) {
+            if (kGuide && alive) {
+              // one-sample MIS of the guide (probability alpha) and Lambert
+              // sampling: the path weight uses the mixture density
+              f3 wd;
+              if (rng.next() < A.guide_alpha) {
+                float const ul = rng.next();
+                float const u1 = rng.next();
+                float const u2 = rng.next();
+                wd = mix_sample(M, ul, u1, u2);
+              } else {
+                float const mu_phi = rng.next();
+                float const mu_theta = rng.next();
+                float const phi = static_cast<float>(2.0 * kPi) * mu_phi;
+                float const sin_t = sqrtf(1.0f - mu_theta);
+                wd = add3(add3(scl3(tan, sin_t * cosf(phi)), scl3(bin, sin_t * sinf(phi))),
+                          scl3(sn, sqrtf(mu_theta)));
+              }
+              float const cs = dot3(wd, sn);
+              if (cs > 0.0f && dot3(wd, gn) > 0.0f) {
+                float const pdf = A.guide_alpha * mix_pdf(M, wd) +
+                                  (1.0f - A.guide_alpha) * cs * static_cast<float>(kInvPi);
+                float const lambert = cs * static_cast<float>(kInvPi);
+                beta = scl3(beta, lambert / pdf);
+                reinterpret_cast<float *>(A.radiance + slot)[3] = rr_scale * (pdf / lambert);
+                dir = wd;
+                push_ext = true;
+                beta4 = make_float4(beta.x, beta.y, beta.z, pdf);
+                misc = pack_misc(rng.dim, k, 0u);
+                if (b < A.train_bounces) {
+                  float *rec = A.records + (static_cast<int64_t>(slot) * A.train_bounces + b) * 16;
+                  float const r[13] = {pos.x, pos.y, pos.z, sn.x, sn.y, sn.z, wd.x, wd.y, wd.z, pdf,
+                                       beta.x, beta.y, beta.z};
+                  for (int t = 0; t < 13; ++t) rec[t] = r[t];
+                  // the next vertex (if the ray hits one) replaces these
+                  rec[13] = rec[14] = rec[15] = __int_as_float(0x7fc00000);
+                }
+              }
+            } else if (alive) {
               // Lambert::NextScatteringDirection / ComputeDiffusedVector
               // (lambert.cpp:176-187, stdafx.hpp:50-63); g++ passes the first
               // draw to fMuPhi and the second to fMuTheta.
@@ -681,6 +832,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
       A.s_pb[js] = make_float4(pbv.x, pbv.y, pbv.z, __int_as_float(slot));
       A.s_target[js] = tri;
       if (kAdj) A.s_slot[js] = light_mat;
+      if (kGuide) A.s_slot[js] = __float_as_int(rho);
     }
     int32_t const je = warp_append(&cnt_next[kCExt], push_ext);
     if (push_ext) {

@@ -551,6 +551,82 @@ def batch_workload(n: int = 64, first_seed: int = 0) -> list:
         out.append(BatchEntry(batch_scene(seed), res, res, spp, 8))
     return out
 
+
+def occluded_room(level: int = 6, wall_n: int = 48, seed: int = 0, radiance: float = 40.0,
+                  room_albedo: float = 0.75, compartment_albedo: float = 0.75) -> SceneData:
+    """Indirect-lit room for path guiding: a closed 4 x 4 x 3 m room (x, z in
+    [-2, 2], y in [0, 3]); a dividing wall at z = 1.5 that stops 0.1 m below
+    the ceiling; behind it a 3 x 0.3 m area light on the floor facing up.  The
+    main room sees no emitter: light reaches it through the 0.1 m gap after
+    bouncing off the compartment's ceiling and walls.  Furniture: two displaced
+    level-`level` icospheres and four boxes.  Walls are wall_n x wall_n grids;
+    at level 6 and wall_n 48: 2 x 81,920 sphere + 7 x 4,608 wall + 48 box +
+    2 light = 196,146 triangles.  Lambert albedos: walls `room_albedo` (the
+    wall behind the light `compartment_albedo`), a red and a blue sphere,
+    grey boxes.  Pinhole camera in the main room facing the dividing wall,
+    60 degree fov."""
+    rng = np.random.default_rng(seed)
+    WHITE, RED, BLUE, GREY, LIGHT, BRIGHT = 0, 1, 2, 3, 4, 5
+    b = _Builder()
+
+    def grid(origin, u, v, front, mat):
+        o, u, v = (np.asarray(x, dtype=np.float64) for x in (origin, u, v))
+        n = wall_n
+        for i in range(n):
+            for j in range(n):
+                p00 = o + u * (i / n) + v * (j / n)
+                p10 = o + u * ((i + 1) / n) + v * (j / n)
+                p11 = o + u * ((i + 1) / n) + v * ((j + 1) / n)
+                p01 = o + u * (i / n) + v * ((j + 1) / n)
+                b.add_tri(p00, p10, p11, mat, front)
+                b.add_tri(p00, p11, p01, mat, front)
+
+    grid((-2, 0, -2), (4, 0, 0), (0, 0, 4), (0, 1, 0), WHITE)      # floor
+    grid((-2, 3, -2), (4, 0, 0), (0, 0, 4), (0, -1, 0), WHITE)     # ceiling
+    grid((-2, 0, -2), (4, 0, 0), (0, 3, 0), (0, 0, 1), WHITE)      # back wall
+    grid((-2, 0, 2), (4, 0, 0), (0, 3, 0), (0, 0, -1), BRIGHT)     # wall behind the light
+    grid((-2, 0, -2), (0, 3, 0), (0, 0, 4), (1, 0, 0), WHITE)      # left
+    grid((2, 0, -2), (0, 3, 0), (0, 0, 4), (-1, 0, 0), WHITE)      # right
+    grid((-2, 0, 1.5), (4, 0, 0), (0, 2.9, 0), (0, 0, -1), WHITE)  # dividing wall, gap above
+    # boxes in the main room
+    for k in range(4):
+        x0, z0 = rng.uniform(-1.6, 1.0), rng.uniform(-1.6, 0.8)
+        sx, sz, sy = rng.uniform(0.2, 0.5), rng.uniform(0.2, 0.5), rng.uniform(0.2, 0.8)
+        b.add_box((x0, 0.0, z0), (x0 + sx, sy, z0 + sz), GREY)
+    # the light: on the compartment floor, facing up
+    b.add_quad((-1.5, 0.01, 1.6), (1.5, 0.01, 1.6), (1.5, 0.01, 1.9), (-1.5, 0.01, 1.9), LIGHT, (0, 1, 0))
+    pos_r, tris_r, mat_r = b.arrays()
+    nrm_r = np.zeros_like(pos_r)
+    a = pos_r[tris_r[:, 0]].astype(np.float64)
+    n = np.cross(pos_r[tris_r[:, 2]] - a, pos_r[tris_r[:, 1]] - a)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    for c in range(3):
+        nrm_r[tris_r[:, c]] = n.astype(np.float32)
+    pos_l, tri_l, nrm_l, mat_l = [pos_r], [tris_r], [nrm_r], [mat_r]
+    base = pos_r.shape[0]
+    for k, (cx, cz, mat) in enumerate([(-0.7, 0.3, RED), (0.8, -0.4, BLUE)]):
+        v, f = displaced_icosphere(level, seed * 17 + k, 0.15)
+        v = v * 0.45 + np.array([cx, 0.52, cz])
+        pos_l.append(v)
+        tri_l.append(f + base)
+        nrm_l.append(vertex_normals(v, f))
+        mat_l.append(np.full(f.shape[0], mat, np.int32))
+        base += v.shape[0]
+    pos = np.concatenate(pos_l).astype(np.float32)
+    tris = np.concatenate(tri_l).astype(np.int32)
+    tri_mat = np.concatenate(mat_l).astype(np.int32)
+    normals = np.concatenate(nrm_l).astype(np.float32)
+    ra, ca = room_albedo, compartment_albedo
+    albedo = np.stack([ccir601_rgb_to_xyz((ra, ra, ra)), ccir601_rgb_to_xyz((0.7, 0.15, 0.1)),
+                       ccir601_rgb_to_xyz((0.1, 0.2, 0.7)), ccir601_rgb_to_xyz((0.5, 0.5, 0.5)),
+                       np.zeros(3, np.float32), ccir601_rgb_to_xyz((ca, ca, ca))]).astype(np.float32)
+    is_light = np.array([0, 0, 0, 0, 1, 0], np.int32)
+    sd = SceneData(pos, tris, tri_mat, albedo, is_light, np.zeros(3, np.float32), normals=normals,
+                   camera=Camera.with_fov((0.0, 1.5, -1.9), (0.0, 1.3, 1.5), 60.0, pinhole=True),
+                   name=f"occluded-room-l{level}")
+    sd.light_power_xyz = flat_emitter_power(radiance, sd.light_area())
+    return sd
+
 def random_rays(scene: SceneData, n: int, seed: int = 0):
     """Seeded test rays: origins uniform in the scene box grown by 20 %,
     directions uniform on the sphere.  Returns (org, dir) float32 (n, 3)."""
