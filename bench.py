@@ -304,6 +304,123 @@ def batch_bench(steps: int, warmup: int):
             s.close()
 
 
+GUIDE_CAMERA = ((0.0, 1.5, 1.2), (0.0, 1.1, -2.0), 60.0)
+
+
+def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_spp: int = 1024,
+                max_seconds: float = 30.0, guide_cfg=None, variants=()):
+    """Time to relative MSE 0.01, guided vs plain, on the indirect-lit room
+    (196,146 triangles; light only through a 0.1 m gap), 1024 x 1024 camera,
+    max depth 10, Russian roulette 0.2.  The error is measured on a band of
+    `band` image rows through the image centre (both tracers render that band),
+    against a `ref_spp` plain render of the band (float64 accumulation),
+    relMSE = mean((Y - Y_ref)^2 / (Y_ref^2 + 1e-2)) with the image exposed so
+    that the band's mean reference Y is 1, minus the reference's own share of
+    that error (estimated from the difference of its two independent halves
+    A and B: var(Y_ref) = E[(A - B)^2] / 4).  Both tracers render passes of
+    `pass_spp` until the error reaches 0.01; each pass is timed with CUDA
+    events around the render call (the error evaluation is not timed).  The
+    reported time is robust to host-side launch stalls of the shared machine:
+    the number of passes times the median pass time (training and rendering
+    passes of the guided tracer separately); the plain sum of the pass times
+    is reported beside it.  The guided tracer trains during the first 25 % of
+    a planned `plan_spp`.  A tracer that has not reached 0.01 after
+    `max_seconds` reports the time extrapolated from relMSE ~ 1 / spp.  `variants`: further guide settings (dicts of
+    guide_cfg overrides, optionally with their own plan_spp) measured against
+    the same reference and plain run."""
+    import torch
+    from xyz_b200 import api, scenes
+    W = H = 1024
+    rows = (H // 2 - band // 2, H // 2 + band // 2)
+    depth = 10
+    sd = scenes.occluded_room()
+    cam = scenes.Camera.with_fov(*GUIDE_CAMERA, pinhole=True)
+    cfg = dict(train_bounces=3, guide_bounces=4, alpha=0.5)
+    cfg.update(guide_cfg or {})
+    with api.Scene(sd) as s:
+        halves = [torch.zeros((band, W, 3), dtype=torch.float64, device="cuda") for _ in range(2)]
+        chunk = 4096
+        t0 = time.perf_counter()
+        for k in range(0, ref_spp, chunk):
+            f = s.render(cam, W, H, chunk, seed=99, spp_offset=k, max_depth=depth, rows=rows)
+            halves[(k // chunk) & 1] += f[rows[0]:rows[1]].double()
+        torch.cuda.synchronize()
+        ref_s = time.perf_counter() - t0
+        a, b = (h[..., 1] / (ref_spp // 2) for h in halves)
+        ref_y = (a + b) / 2
+        scale = 1.0 / float(ref_y.mean())
+        ry = ref_y * scale
+        den = ry ** 2 + 1e-2
+        ref_noise = float((((a - b) * scale) ** 2 / 4 / den).mean())
+
+        def relmse(img):
+            return float((((img[..., 1] * scale - ry) ** 2) / den).mean()) - ref_noise
+
+        def run(render_pass, train_passes=0):
+            acc = torch.zeros((band, W, 3), dtype=torch.float64, device="cuda")
+            film = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
+            times, p, e = [], 0, float("inf")
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            while True:
+                torch.cuda.synchronize()
+                e0.record()
+                render_pass(p, film)
+                e1.record()
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1) * 1e-3)
+                acc += film[rows[0]:rows[1]].double()
+                p += 1
+                e = relmse(acc / (p * pass_spp))
+                tr, rd = times[:train_passes], times[train_passes:]
+                robust = len(tr) * (statistics.median(tr) if tr else 0.0) + len(rd) * (statistics.median(rd) if rd else 0.0)
+                out = {"spp": p * pass_spp, "relmse": round(e, 5), "passes": p,
+                       "median_pass_ms": round(statistics.median(rd if rd else tr) * 1e3, 3),
+                       "sum_of_pass_seconds": round(sum(times), 3)}
+                if e <= 0.01:
+                    return {"seconds": round(robust, 3), "reached": True} | out
+                if sum(times) > max_seconds:
+                    return {"seconds": round(robust * e / 0.01, 3), "reached": False} | out
+
+        def plain_pass(p, film):
+            s.render(cam, W, H, pass_spp, seed=1, spp_offset=p * pass_spp, max_depth=depth, film=film, rows=rows)
+
+        # untimed warm-up of both tracers (module loading, first-use allocations)
+        s.render(cam, W, H, pass_spp, seed=7, max_depth=depth, rows=rows)
+        with api.Guide(s, **cfg) as g0:
+            g0.render(cam, W, H, pass_spp, seed=7, max_depth=depth, rows=rows, train=True)
+        torch.cuda.synchronize()
+        plain = run(plain_pass)
+
+        def guided_run(gcfg, gplan):
+            train_passes = max(1, (gplan // 4) // pass_spp)
+            with api.Guide(s, **gcfg) as g:
+                def guided_pass(p, film):
+                    g.render(cam, W, H, pass_spp, seed=1, spp_offset=p * pass_spp, max_depth=depth, film=film,
+                             rows=rows, train=p < train_passes)
+
+                res = run(guided_pass, train_passes)
+                return res, gcfg | g.stats() | {"training_spp": train_passes * pass_spp}
+
+        guided, ginfo = guided_run(cfg, plan_spp)
+        more = []
+        for v in variants:
+            v = dict(v)
+            vplan = v.pop("plan_spp", plan_spp)
+            r, info = guided_run(cfg | v, vplan)
+            more.append({"guide": info, "guided": r, "speedup": round(plain["seconds"] / r["seconds"], 2)})
+    out = {"metric": "seconds to relMSE 0.01 (lower is better)",
+           "plain": plain, "guided": guided,
+           "speedup": round(plain["seconds"] / guided["seconds"], 2),
+           "guide": ginfo,
+           "reference": {"spp": ref_spp, "seconds": round(ref_s, 2), "own_relmse": round(ref_noise, 5),
+                         "tracer": "plain GPU path tracer, float64 sums"},
+           "config": f"occluded room, 196,146 triangles, 1024x1024 camera, rows {rows[0]}-{rows[1]}, max depth 10, "
+                     f"Russian roulette 0.2, passes of {pass_spp} spp, exposure: band mean Y = 1"}
+    if more:
+        out["variants"] = more
+    return out
+
+
 def profiled_traffic():
     """DRAM bytes per traced ray of the trace kernel from the committed ncu
     summary (profiles/trace_queue_spheres1m.txt), if present."""

@@ -380,6 +380,8 @@ typedef struct {
   int steps_per_pass;    /* Adam steps after each training render (16) */
   int train_bounces;     /* path vertices per path that give training records (2) */
   uint64_t seed;         /* weight initialisation */
+  int guide_bounces;     /* path vertices sampled with the guide (the first ones); deeper
+                            vertices use Lambert sampling alone and need no inference (4) */
 } xyzgpu_guide_config;
 
 typedef struct xyzgpu_guide_s *xyzgpu_guide;

@@ -95,7 +95,8 @@ GUIDE_OUTPUTS = 64
 
 class GuideConfig(C.Structure):
     _fields_ = [("alpha", C.c_float), ("learning_rate", C.c_float), ("batch_size", C.c_int),
-                ("steps_per_pass", C.c_int), ("train_bounces", C.c_int), ("seed", C.c_uint64)]
+                ("steps_per_pass", C.c_int), ("train_bounces", C.c_int), ("seed", C.c_uint64),
+                ("guide_bounces", C.c_int)]
 
 
 class GuideStats(C.Structure):

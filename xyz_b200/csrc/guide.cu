@@ -11,9 +11,12 @@
 // Arithmetic: bf16 weights and activations, fp32 accumulation, on the 5th
 // generation tensor cores: every layer of a tile of 128 rows is a chain of
 // tcgen05.mma (M = 128, N = 64, K = 16 each) with both operands in shared
-// memory and the accumulator in TMEM; the epilogue (bias, ReLU, bf16 pack)
-// reads the accumulator back with tcgen05.ld, one TMEM lane per thread = one
-// row.  Training runs the forward pass, the loss gradient at the output, and
+// memory and the accumulator in TMEM; the epilogue (ReLU, bf16 pack) reads
+// the accumulator back with tcgen05.ld, one TMEM lane per thread = one
+// row.  The bias enters the accumulator as one more MMA (K = 16) of a
+// constant tile of ones with the bias split into three bf16 parts (hi, mid,
+// lo: their sum is the fp32 bias to within fp32 rounding), so the epilogue is
+// only ReLU and the bf16 pack, one cvt.rn.relu.bf16x2 per pair.  Training runs the forward pass, the loss gradient at the output, and
 // the backward pass on the same tensor cores: the input deltas of a layer
 // (delta * W, M = 128) and the weight gradients (delta^T * activations,
 // M = 64, N = 64 or 192, reduced over the 128 rows) accumulate in TMEM over
@@ -60,6 +63,17 @@ __host__ __device__ constexpr uint32_t wblk_off(int l) {
   return l == 0 ? 0u : static_cast<uint32_t>(kW * kIn * 2 + (l - 1) * kW * kW * 2);
 }
 constexpr uint32_t kWBlkBytes = kW * kIn * 2 + 4 * kW * kW * 2;  // 57344
+constexpr int kHBytes = kRows * kW * 2;  // one hidden activation buffer
+constexpr int kBiasK = 16;               // K of the bias MMA (columns 0..2 used)
+
+// The weights as the tensor cores read them: blocked bf16 W^T per layer, the
+// ones tile (128 x 16, columns 0..2 = 1) and per layer the bias tile (64 x 16,
+// columns 0..2 = the bias's hi, mid and lo bf16 parts).
+struct WeightsSmem {
+  uint8_t w[kWBlkBytes];
+  uint8_t ones[kRows * kBiasK * 2];
+  uint8_t bias[kLayers][kW * kBiasK * 2];
+};
 
 // TMEM columns: [0, 64) the working accumulator; weight gradients (M = 64
 // layout: rows 16w..16w+15 in lanes 32w..32w+15) of layer 0 at [64, 256),
@@ -67,8 +81,7 @@ constexpr uint32_t kWBlkBytes = kW * kIn * 2 + 4 * kW * kW * 2;  // 57344
 __device__ __forceinline__ uint32_t dw_col(int l) { return l == 0 ? 64u : 256u + 64u * (l - 1); }
 
 struct __align__(128) GuideSmem {
-  uint8_t w[kWBlkBytes];
-  float bias[kLayers][kW];
+  WeightsSmem wt;
   uint8_t x[kRows * kIn * 2];
   uint8_t h[4][kRows * kW * 2];
   uint8_t d[2][kRows * kW * 2];
@@ -91,6 +104,22 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
   return *reinterpret_cast<const uint32_t *>(&v);
 }
 
+// ReLU and bf16 pack of two values (a in the low half).
+__device__ __forceinline__ uint32_t pack_relu_bf16x2(float a, float b) {
+  uint32_t d;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
+  return d;
+}
+
+__device__ __forceinline__ void store_row8_relu(uint8_t *buf, int r, int c, int cols, const float *v) {
+  uint4 q;
+  q.x = pack_relu_bf16x2(v[0], v[1]);
+  q.y = pack_relu_bf16x2(v[2], v[3]);
+  q.z = pack_relu_bf16x2(v[4], v[5]);
+  q.w = pack_relu_bf16x2(v[6], v[7]);
+  *reinterpret_cast<uint4 *>(buf + tc::blocked_offset(r, c, cols)) = q;
+}
+
 __device__ __forceinline__ void store_row8(uint8_t *buf, int r, int c, int cols, const float *v) {
   uint4 q;
   q.x = pack_bf16x2(v[0], v[1]);
@@ -104,24 +133,29 @@ __device__ __forceinline__ void store_row8(uint8_t *buf, int r, int c, int cols,
 // input s in [0, 1], 32 bins of exp(-(s - (j + 1/2) / 32)^2 / (2 sigma^2)),
 // sigma = 1/32.  Bins more than 4.5 sigma from s are exactly 0 (exp(-10) and
 // below; the oracle applies the same cut): the row is cleared, then the at
-// most 10 bins of the window are computed and stored one by one.
+// most 10 bins of the window are computed and stored one by one.  In bin
+// units (u = 32 s, t_j = u - j - 1/2) the bins are g_j = exp(-t_j^2 / 2), and
+// g_{j+1} = g_j exp(t_j - 1/2), exp(t_{j+1} - 1/2) = exp(t_j - 1/2) / e: two
+// exponentials per input and two products per bin.
 __device__ void encode_row(uint8_t *x, int r, const GuideDev &G, const float f[6]) {
 #pragma unroll
   for (int q = 0; q < kIn; q += 8) *reinterpret_cast<uint4 *>(x + tc::blocked_offset(r, q, kIn)) = make_uint4(0, 0, 0, 0);
-#pragma unroll 1
+#pragma unroll
   for (int dim = 0; dim < 6; ++dim) {
     float s = dim < 3 ? (f[dim] - G.lo[dim]) * G.inv_ext[dim] : (f[dim] + 1.0f) * 0.5f;
     s = fminf(fmaxf(s, 0.0f), 1.0f);
     float const u = s * static_cast<float>(kBins);
     int const jlo = max(0, static_cast<int>(ceilf(u - 5.0f)));
+    float const t0 = u - (static_cast<float>(jlo) + 0.5f);
+    float g = __expf(-0.5f * t0 * t0);
+    float ratio = __expf(t0 - 0.5f);
 #pragma unroll
     for (int t = 0; t < 10; ++t) {
       int const j = jlo + t;
-      if (j < kBins && fabsf(u - (static_cast<float>(j) + 0.5f)) <= 4.5f) {
-        float const d = s - (static_cast<float>(j) + 0.5f) * (1.0f / kBins);
-        __nv_bfloat16 const v = __float2bfloat16_rn(__expf(-d * d * (0.5f * kBins * kBins)));
-        *reinterpret_cast<__nv_bfloat16 *>(x + tc::blocked_offset(r, dim * kBins + j, kIn)) = v;
-      }
+      if (j < kBins && fabsf(u - (static_cast<float>(j) + 0.5f)) <= 4.5f)
+        *reinterpret_cast<__nv_bfloat16 *>(x + tc::blocked_offset(r, dim * kBins + j, kIn)) = __float2bfloat16_rn(g);
+      g *= ratio;
+      ratio *= 0.36787944117144233f;  // 1 / e
     }
   }
 }
@@ -132,7 +166,8 @@ __device__ void encode_row(uint8_t *x, int r, const GuideDev &G, const float f[6
 // whole CTA, else a named barrier of the group's 128 threads).
 struct Tile {
   uint8_t *x;     // encoding [128][192]
-  uint8_t *h[4];  // hidden outputs [128][64]: all four kept for training, else h[0], h[1] alternate
+  uint8_t *h;     // hidden outputs [128][64] at h + l * kHBytes: all four kept for training,
+                  // else two buffers alternate (l & 1)
   uint32_t tmem;
   uint32_t mbar;
   int bar;
@@ -178,12 +213,15 @@ __device__ __forceinline__ bool await_mma(const Tile &c, uint32_t &phase) {
   return true;
 }
 
-__device__ __forceinline__ void issue_forward(uint32_t w_base, int l, const uint8_t *in, uint32_t tmem) {
+__device__ __forceinline__ void issue_forward(const WeightsSmem &wt, int l, const uint8_t *in, uint32_t tmem) {
   int const K = layer_in(l);
-  uint32_t const a0 = tc::smem_addr(in), b0 = w_base + wblk_off(l);
+  uint32_t const a0 = tc::smem_addr(in), b0 = tc::smem_addr(wt.w) + wblk_off(l);
   uint32_t const id = tc::idesc_bf16(kRows, kW, false, false);
+  // D = ones * bias_parts^T (every row the bias), then D += in * W
+  tc::mma_bf16(tmem, tc::desc_kmajor(tc::smem_addr(wt.ones), kBiasK), tc::desc_kmajor(tc::smem_addr(wt.bias[l]), kBiasK),
+               id, false);
   for (int ks = 0; ks < K / 16; ++ks)
-    tc::mma_bf16(tmem, tc::desc_kmajor(a0 + ks * 256, K), tc::desc_kmajor(b0 + ks * 256, K), id, ks > 0);
+    tc::mma_bf16(tmem, tc::desc_kmajor(a0 + ks * 256, K), tc::desc_kmajor(b0 + ks * 256, K), id, true);
 }
 
 // This thread's row of an accumulator (64 fp32); a warp reads the 32 TMEM
@@ -197,15 +235,13 @@ __device__ __forceinline__ void read_acc(uint32_t tmem, float *v) {
 
 // Forward pass of the tile whose encoding is in c.x; leaves this thread's row
 // of raw outputs (with bias) in out[64].
-__device__ bool forward(const uint8_t *w, const float (*bias)[kW], Tile &c, uint32_t &phase, bool keep,
-                        float *out) {
-  uint32_t const wb = tc::smem_addr(w);
+__device__ bool forward(const WeightsSmem &wt, Tile &c, uint32_t &phase, bool keep, float *out) {
   const uint8_t *in = c.x;
   for (int l = 0; l < kLayers; ++l) {
     publish(c.bar);
     if (c.t == 0) {
       tc::fence_after_sync();
-      issue_forward(wb, l, in, c.tmem);
+      issue_forward(wt, l, in, c.tmem);
       tc::mma_commit(c.mbar);
     }
     if (!await_mma(c, phase)) return false;
@@ -213,14 +249,12 @@ __device__ bool forward(const uint8_t *w, const float (*bias)[kW], Tile &c, uint
     read_acc(c.tmem, v);
     if (l == kLayers - 1) {
 #pragma unroll
-      for (int j = 0; j < kW; ++j) out[j] = v[j] + bias[l][j];
+      for (int j = 0; j < kW; ++j) out[j] = v[j];
       break;
     }
-    uint8_t *dst = keep ? c.h[l] : c.h[l & 1];
+    uint8_t *dst = c.h + (keep ? l : (l & 1)) * kHBytes;
 #pragma unroll
-    for (int j = 0; j < kW; ++j) v[j] = fmaxf(v[j] + bias[l][j], 0.0f);
-#pragma unroll
-    for (int q = 0; q < kW; q += 8) store_row8(dst, c.t, q, kW, v + q);
+    for (int q = 0; q < kW; q += 8) store_row8_relu(dst, c.t, q, kW, v + q);
     in = dst;
   }
   return true;
@@ -286,11 +320,25 @@ __device__ void loss_grad(const float *o, const float w[3], float scale, float *
 }
 
 // ------------------------------------------------------------- kernels
-__device__ void load_weights(uint8_t *w, float (*bias)[kW], const GuideDev &G) {
+__device__ void load_weights(WeightsSmem &wt, const GuideDev &G) {
   const uint4 *src = reinterpret_cast<const uint4 *>(G.wblk);
-  uint4 *dst = reinterpret_cast<uint4 *>(w);
+  uint4 *dst = reinterpret_cast<uint4 *>(wt.w);
   for (int i = threadIdx.x; i < static_cast<int>(kWBlkBytes / 16); i += blockDim.x) dst[i] = src[i];
-  for (int i = threadIdx.x; i < kLayers * kW; i += blockDim.x) bias[i / kW][i % kW] = G.params[param_b(i / kW) + i % kW];
+  for (int i = threadIdx.x; i < kRows * kBiasK; i += blockDim.x) {
+    int const r = i / kBiasK, c = i % kBiasK;
+    *reinterpret_cast<__nv_bfloat16 *>(wt.ones + tc::blocked_offset(r, c, kBiasK)) =
+        __float2bfloat16_rn(c < 3 ? 1.0f : 0.0f);
+  }
+  for (int i = threadIdx.x; i < kLayers * kW * kBiasK; i += blockDim.x) {
+    int const l = i / (kW * kBiasK), n = (i / kBiasK) % kW, c = i % kBiasK;
+    float const b = G.params[param_b(l) + n];
+    __nv_bfloat16 const hi = __float2bfloat16_rn(b);
+    float const r1 = b - __bfloat162float(hi);
+    __nv_bfloat16 const mid = __float2bfloat16_rn(r1);
+    __nv_bfloat16 const lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
+    __nv_bfloat16 const v = c == 0 ? hi : c == 1 ? mid : c == 2 ? lo : __float2bfloat16_rn(0.0f);
+    *reinterpret_cast<__nv_bfloat16 *>(wt.bias[l] + tc::blocked_offset(n, c, kBiasK)) = v;
+  }
 }
 
 // mbarriers (count 1) and `ncols` TMEM columns for the CTA.
@@ -298,6 +346,7 @@ __device__ void setup(uint64_t *mbar, int nbar, uint32_t *tmem_slot, uint32_t nc
   if (threadIdx.x == 0)
     for (int i = 0; i < nbar; ++i) tc::mbar_init(tc::smem_addr(&mbar[i]), 1);
   if (threadIdx.x < 32) tc::tmem_alloc(tmem_slot, ncols);
+  tc::fence_smem_to_async();  // the weights every thread stored, for every group's MMAs
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -322,19 +371,19 @@ constexpr int kGroups = 3;
 constexpr int kInferThreads = kGroups * kRows;
 
 struct __align__(128) InferSmem {
-  uint8_t w[kWBlkBytes];
-  float bias[kLayers][kW];
+  WeightsSmem wt;
   uint8_t x[kGroups][kRows * kIn * 2];
   uint64_t mbar[kGroups];
   uint32_t tmem;
 };
 
+static_assert(sizeof(InferSmem) <= 227 * 1024, "inference CTA shared memory");
+static_assert(sizeof(GuideSmem) <= 227 * 1024, "training CTA shared memory");
+
 __device__ Tile infer_tile(InferSmem &S, int gi) {
   Tile c;
   c.x = S.x[gi];
-  c.h[0] = S.x[gi];
-  c.h[1] = S.x[gi] + kRows * kW * 2;
-  c.h[2] = c.h[3] = nullptr;
+  c.h = S.x[gi];
   c.tmem = S.tmem + 64u * static_cast<uint32_t>(gi);
   c.mbar = tc::smem_addr(&S.mbar[gi]);
   c.bar = 1 + gi;
@@ -344,10 +393,10 @@ __device__ Tile infer_tile(InferSmem &S, int gi) {
 
 // Raw outputs of n points (features: n x 6 = position, normal).
 __global__ void __launch_bounds__(kInferThreads, 1)
-    k_guide_forward(GuideDev G, const float *__restrict__ feat, int n, float *__restrict__ out) {
+    k_guide_forward(const __grid_constant__ GuideDev G, const float *__restrict__ feat, int n, float *__restrict__ out) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
   InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
-  load_weights(S.w, S.bias, G);
+  load_weights(S.wt, G);
   setup(S.mbar, kGroups, &S.tmem, 256);
   int const gi = threadIdx.x >> 7;
   Tile c = infer_tile(S, gi);
@@ -361,7 +410,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
       for (int k = 0; k < 6; ++k) f[k] = feat[6 * static_cast<int64_t>(row) + k];
     encode_row(c.x, c.t, G, f);
     float o[kW];
-    if (!forward(S.w, S.bias, c, phase, false, o)) {
+    if (!forward(S.wt, c, phase, false, o)) {
       if (c.t == 0) atomicExch(G.err, 1);
       aborted = true;
       break;
@@ -375,15 +424,15 @@ __global__ void __launch_bounds__(kInferThreads, 1)
 // Gradient of sum over records of -w * log p(dir) * scale, added to grad
 // (flat parameter layout).  records: n x 10 = position, normal, direction, w.
 __global__ void __launch_bounds__(kGuideThreads, 1)
-    k_guide_gradient(GuideDev G, const float *__restrict__ rec, int n, float scale, float *__restrict__ grad) {
+    k_guide_gradient(const __grid_constant__ GuideDev G, const float *__restrict__ rec, int n, float scale, float *__restrict__ grad) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
   GuideSmem &S = *reinterpret_cast<GuideSmem *>(smem_raw);
-  load_weights(S.w, S.bias, G);
+  load_weights(S.wt, G);
   for (int i = threadIdx.x; i < kLayers * kW; i += blockDim.x) (&S.db[0][0])[i] = 0.0f;
   setup(&S.mbar, 1, &S.tmem, 512);
   Tile c;
   c.x = S.x;
-  for (int l = 0; l < 4; ++l) c.h[l] = S.h[l];
+  c.h = S.h[0];
   c.tmem = S.tmem;
   c.mbar = tc::smem_addr(&S.mbar);
   c.bar = 0;
@@ -405,7 +454,7 @@ __global__ void __launch_bounds__(kGuideThreads, 1)
     }
     encode_row(S.x, r, G, f);
     float o[kW];
-    if (!forward(S.w, S.bias, c, phase, true, o)) {
+    if (!forward(S.wt, c, phase, true, o)) {
       ok = false;
       break;
     }
@@ -439,7 +488,7 @@ __global__ void __launch_bounds__(kGuideThreads, 1)
                        tc::desc_mnmajor(aa + ks * 2 * (K / 8) * 128, K), idw, !first || ks > 0);
         if (l > 0) {
           // delta_{l-1} (128 x 64) = delta (128 x 64) * W_l (64 x 64, from W_l^T as MN-major)
-          uint32_t const wb = tc::smem_addr(S.w) + wblk_off(l);
+          uint32_t const wb = tc::smem_addr(S.wt.w) + wblk_off(l);
           uint32_t const idd = tc::idesc_bf16(kRows, kW, false, true);
           for (int ks = 0; ks < kW / 16; ++ks)
             tc::mma_bf16(S.tmem, tc::desc_kmajor(da + ks * 256, kW),
@@ -533,10 +582,10 @@ __device__ void infer_features(const InferArgs &I, int i, float4 h, float f[6]) 
   f[0] = pos.x, f[1] = pos.y, f[2] = pos.z, f[3] = sn.x, f[4] = sn.y, f[5] = sn.z;
 }
 
-__global__ void __launch_bounds__(kInferThreads, 1) k_guide_infer(GuideDev G, InferArgs I) {
+__global__ void __launch_bounds__(kInferThreads, 1) k_guide_infer(const __grid_constant__ GuideDev G, InferArgs I) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
   InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
-  load_weights(S.w, S.bias, G);
+  load_weights(S.wt, G);
   setup(S.mbar, kGroups, &S.tmem, 256);
   int const gi = threadIdx.x >> 7;
   Tile c = infer_tile(S, gi);
@@ -557,32 +606,45 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_guide_infer(GuideDev G, In
     if (tile + step < ntiles && inext < n) hnext = I.hits[inext];
     encode_row(c.x, c.t, G, f);
     float o[kW];
-    if (!forward(S.w, S.bias, c, phase, false, o)) {
+    if (!forward(S.wt, c, phase, false, o)) {
       if (c.t == 0) atomicExch(G.err, 1);
       aborted = true;
       break;
     }
     if (i < n) {
+      // mixture values (weight, kappa, mean xyz per lobe) packed as fp16
+      // pairs in registers; the renderer renormalises what it reads, so the
+      // fast intrinsics here only shape the proposal
       float mx = o[0];
+#pragma unroll
       for (int j = 1; j < 8; ++j) mx = fmaxf(mx, o[j]);
       float e[8], se = 0.0f;
+#pragma unroll
       for (int j = 0; j < 8; ++j) {
-        e[j] = expf(o[j] - mx);
+        e[j] = __expf(o[j] - mx);
         se += e[j];
       }
-      __half hv[40];
+      float const inv_se = 1.0f / se;
+      float hv[40];
+#pragma unroll
       for (int j = 0; j < 8; ++j) {
-        float const k = expf(fminf(fmaxf(o[8 + j], -5.0f), 8.0f));
         float const x = o[16 + 3 * j], y = o[17 + 3 * j], z = o[18 + 3 * j];
-        float const r = 1.0f / sqrtf(x * x + y * y + z * z + 1e-12f);
-        hv[5 * j] = __float2half_rn(e[j] / se);
-        hv[5 * j + 1] = __float2half_rn(k);
-        hv[5 * j + 2] = __float2half_rn(x * r);
-        hv[5 * j + 3] = __float2half_rn(y * r);
-        hv[5 * j + 4] = __float2half_rn(z * r);
+        float const r = rsqrtf(x * x + y * y + z * z + 1e-12f);
+        hv[5 * j] = e[j] * inv_se;
+        hv[5 * j + 1] = __expf(fminf(fmaxf(o[8 + j], -5.0f), 8.0f));
+        hv[5 * j + 2] = x * r;
+        hv[5 * j + 3] = y * r;
+        hv[5 * j + 4] = z * r;
+      }
+      uint32_t wv[20];
+#pragma unroll
+      for (int t = 0; t < 20; ++t) {
+        __half2 const h2 = __floats2half2_rn(hv[2 * t], hv[2 * t + 1]);
+        wv[t] = *reinterpret_cast<const uint32_t *>(&h2);
       }
       uint4 *dst = reinterpret_cast<uint4 *>(I.mix + 40 * static_cast<int64_t>(i));
-      for (int t = 0; t < 5; ++t) dst[t] = reinterpret_cast<const uint4 *>(hv)[t];
+#pragma unroll
+      for (int t = 0; t < 5; ++t) dst[t] = make_uint4(wv[4 * t], wv[4 * t + 1], wv[4 * t + 2], wv[4 * t + 3]);
     }
   }
   teardown(S.tmem, 256, aborted, c.mbar, phase);
@@ -765,6 +827,7 @@ int guide_wave_prepare(GuideImpl &g, int64_t cap, bool train, cudaStream_t st, G
   out->records = train && tb > 0 ? g.d_rec : nullptr;
   out->train_bounces = train ? tb : 0;
   out->alpha = g.cfg.alpha;
+  out->guide_bounces = g.cfg.guide_bounces;
   return XYZGPU_OK;
 }
 
@@ -843,6 +906,7 @@ void xyzgpu_guide_config_default(xyzgpu_guide_config *c) {
   c->steps_per_pass = 16;
   c->train_bounces = 2;
   c->seed = 0;
+  c->guide_bounces = 4;
 }
 
 void xyzgpu_guide_destroy(xyzgpu_guide h) {
@@ -876,7 +940,7 @@ int xyzgpu_guide_create(xyzgpu_scene scene, const xyzgpu_guide_config *cfg, xyzg
   else
     xyzgpu_guide_config_default(&c);
   if (!(c.alpha >= 0.0f && c.alpha < 1.0f) || !(c.learning_rate > 0.0f) || c.batch_size < 1 ||
-      c.steps_per_pass < 0 || c.train_bounces < 0 || c.train_bounces > 8)
+      c.steps_per_pass < 0 || c.train_bounces < 0 || c.train_bounces > 8 || c.guide_bounces < 0)
     return set_error(XYZGPU_E_INVALID, "guide_create: configuration out of range");
   auto *h = new (std::nothrow) xyzgpu_guide_s();
   if (!h) return set_error(XYZGPU_E_NOMEM, "guide_create: host allocation failed");

@@ -172,12 +172,20 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
     }
   } ltot_guard{ltot, st};
 
+  // Grids of one full wave of resident CTAs per kernel variant (the
+  // grid-stride loops give every CTA an equal share, so a grid larger than
+  // what fits at once would run a second, tail wave).
   static int g_raygen = 0, g_trace_e = 0, g_trace_s = 0, g_shade = 0, g_film = 0, g_shade_sp = 0;
+  static int g_shade_adj = 0, g_shade_guide = 0, g_trace_s_adj = 0, g_trace_s_guide = 0;
   if (!g_raygen) {
     g_raygen = occupancy_grid(k_raygen<false>, s.device);
     g_trace_e = occupancy_grid(k_trace_queue<false, false>, s.device);
     g_trace_s = occupancy_grid(k_trace_queue<true, false>, s.device);
+    g_trace_s_adj = occupancy_grid(k_trace_queue<true, false, kModeAdjoint>, s.device);
+    g_trace_s_guide = occupancy_grid(k_trace_queue<true, false, kModeGuided>, s.device);
     g_shade = occupancy_grid(k_shade<kModePlain>, s.device);
+    g_shade_adj = occupancy_grid(k_shade<kModeAdjoint>, s.device);
+    g_shade_guide = occupancy_grid(k_shade<kModeGuided>, s.device);
     g_shade_sp = occupancy_grid(k_shade_spectral, s.device);
     g_film = occupancy_grid(k_film, s.device);
   }
@@ -284,8 +292,11 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
           else
             k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, pc);
           XYZ_MARK(1, false);
-          // (the last bounce only meets the depth cap: no sampling, no inference)
-          if (guide && b < iters - 1) {
+          // (the last bounce only meets the depth cap: no sampling, no inference;
+          // beyond guide_bounces the guided kernels sample Lambert alone)
+          bool const guided_here = guide && b < iters - 1 && b < gw.guide_bounces;
+          A.guide_alpha = guided_here ? gw.alpha : 0.0f;
+          if (guided_here) {
             int const qi = b & 1;
             int const r = guide_infer_launch(*guide->g, A.q_o[qi], A.q_d[qi], A.hits,
                                              A.counts + b * kCountStride + kCExt, A.S, gw.mix, st);
@@ -296,9 +307,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
           if (spectral)
             k_shade_spectral<<<g_shade_sp, kThreads, 0, st>>>(A, b);
           else if (guide)
-            k_shade<kModeGuided><<<g_shade, kThreads, 0, st>>>(A, b);
+            k_shade<kModeGuided><<<g_shade_guide, kThreads, 0, st>>>(A, b);
           else if (replay)
-            k_shade<kModeAdjoint><<<g_shade, kThreads, 0, st>>>(A, b);
+            k_shade<kModeAdjoint><<<g_shade_adj, kThreads, 0, st>>>(A, b);
           else
             k_shade<kModePlain><<<g_shade, kThreads, 0, st>>>(A, b);
           XYZ_MARK(2, false);
@@ -306,9 +317,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
           if (counting)
             k_trace_queue<true, true><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
           else if (replay)
-            k_trace_queue<true, false, kModeAdjoint><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
+            k_trace_queue<true, false, kModeAdjoint><<<g_trace_s_adj, kThreads, 0, st>>>(A, b, pc);
           else if (guide)
-            k_trace_queue<true, false, kModeGuided><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
+            k_trace_queue<true, false, kModeGuided><<<g_trace_s_guide, kThreads, 0, st>>>(A, b, pc);
           else
             k_trace_queue<true, false><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
           XYZ_MARK(3, false);

@@ -113,6 +113,7 @@ struct GuideWave {
   float *records = nullptr;  // training records of the wave (16 floats x train_bounces per path)
   int train_bounces = 0;     // 0: no training records
   float alpha = 0.5f;
+  int guide_bounces = 0;     // bounces sampled with the guide
 };
 struct GuideHooks {
   GuideImpl *g;

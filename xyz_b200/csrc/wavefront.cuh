@@ -141,71 +141,111 @@ struct WaveArgs {
 
 // ------------------------------------------------------- guide mixture
 // von Mises-Fisher lobes: vMF(d; mu, k) = k / (2 pi (1 - e^{-2k})) exp(k (mu.d - 1)).
-// Loaded weights are renormalised and means normalised, so sampling and the
-// pdf use the same exact mixture whatever the fp16 rounding.
+// A vertex's mixture stays in its 40 raw fp16 values (8 lobes of weight,
+// kappa, mean xyz; 20 registers) and every use decodes a lobe the same way:
+// weight max(w, 0) / sum (uniform if the sum is 0), kappa max(k, 1e-3), mean
+// normalised ((0, 0, 1) if zero).  Sampling and the pdf therefore describe
+// the same mixture whatever the fp16 rounding.  The decode and the density use
+// the fast intrinsics (rsqrt, fast divide, exp2-based exp): both sides read the
+// same decoded lobes, and the density's relative error (~1e-6) is far below
+// the Monte Carlo noise.
 struct GuideMix {
-  float w[8], k[8], c[8];
-  f3 mu[8];
+  uint4 q[5];
+  float ws;  // sum of the clamped weights
 };
 
-XYZ_DEV void load_mix(const __half *src, GuideMix &M) {
-  const uint4 *q = reinterpret_cast<const uint4 *>(src);
-  __half h[40];
-#pragma unroll
-  for (int t = 0; t < 5; ++t) reinterpret_cast<uint4 *>(h)[t] = q[t];
-  float ws = 0.0f;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    float const w = fmaxf(__half2float(h[5 * i]), 0.0f);
-    float const k = fmaxf(__half2float(h[5 * i + 1]), 1e-3f);
-    f3 m = mk3(__half2float(h[5 * i + 2]), __half2float(h[5 * i + 3]), __half2float(h[5 * i + 4]));
-    float const l2 = dot3(m, m);
-    m = l2 > 0.0f ? scl3(m, 1.0f / sqrtf(l2)) : mk3(0.0f, 0.0f, 1.0f);
-    M.w[i] = w;
-    M.k[i] = k;
-    M.c[i] = k / (static_cast<float>(2.0 * kPi) * -expm1f(-2.0f * k));
-    M.mu[i] = m;
-    ws += w;
-  }
-  float const inv = ws > 0.0f ? 1.0f / ws : 0.125f;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) M.w[i] = ws > 0.0f ? M.w[i] * inv : inv;
+XYZ_DEV float mix_half(const GuideMix &M, int t) {
+  uint4 const v = M.q[t >> 3];
+  int const c = (t >> 1) & 3;
+  uint32_t const w = c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+  return __half2float(__ushort_as_half(static_cast<unsigned short>((t & 1) ? (w >> 16) : (w & 0xffffu))));
 }
 
-XYZ_DEV float mix_pdf(const GuideMix &M, f3 d) {
-  float p = 0.0f;
+// The raw values (issued early: they do not depend on the hit) ...
+XYZ_DEV void load_mix(const __half *src, GuideMix &M) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(src);
 #pragma unroll
-  for (int i = 0; i < 8; ++i) p += M.w[i] * M.c[i] * expf(M.k[i] * (dot3(M.mu[i], d) - 1.0f));
-  return p;
+  for (int t = 0; t < 5; ++t) M.q[t] = q[t];
+}
+// ... and the weight sum, once they are needed.
+XYZ_DEV void finish_mix(GuideMix &M) {
+  float ws = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) ws += fmaxf(mix_half(M, 5 * i), 0.0f);
+  M.ws = ws;
+}
+
+XYZ_DEV float mix_weight(const GuideMix &M, int i) {
+  return M.ws > 0.0f ? fmaxf(mix_half(M, 5 * i), 0.0f) : 1.0f;
+}
+XYZ_DEV float mix_kappa(const GuideMix &M, int i) { return fmaxf(mix_half(M, 5 * i + 1), 1e-3f); }
+XYZ_DEV f3 mix_mean(f3 m) {
+  float const l2 = dot3(m, m);
+  return l2 > 0.0f ? scl3(m, rsqrtf(l2)) : mk3(0.0f, 0.0f, 1.0f);
+}
+XYZ_DEV f3 mix_mean(const GuideMix &M, int i) {
+  return mix_mean(mk3(mix_half(M, 5 * i + 2), mix_half(M, 5 * i + 3), mix_half(M, 5 * i + 4)));
+}
+
+// vMF normaliser k / (2 pi (1 - e^{-2k})); below k = 0.05 the series
+// 1 - e^{-2k} = 2k (1 - k + 2k^2/3 - k^3/3) avoids the cancellation.
+XYZ_DEV float vmf_norm(float k) {
+  float const den = k < 0.05f ? 2.0f * k * (1.0f - k * (1.0f - k * (2.0f / 3.0f - k * (1.0f / 3.0f))))
+                              : 1.0f - __expf(-2.0f * k);
+  return __fdividef(k, static_cast<float>(2.0 * kPi) * den);
+}
+
+// Mixture density at two directions in one pass over the lobes.
+XYZ_DEV void mix_pdf2(const GuideMix &M, f3 d1, f3 d2, float *p1, float *p2) {
+  float a1 = 0.0f, a2 = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    float const k = mix_kappa(M, i);
+    float const wc = mix_weight(M, i) * vmf_norm(k);
+    f3 const mu = mix_mean(M, i);
+    a1 += wc * __expf(k * (dot3(mu, d1) - 1.0f));
+    a2 += wc * __expf(k * (dot3(mu, d2) - 1.0f));
+  }
+  float const inv = M.ws > 0.0f ? 1.0f / M.ws : 0.125f;
+  *p1 = a1 * inv;
+  *p2 = a2 * inv;
 }
 
 // Lobe by weight, then the lobe's cosine w = 1 + log(u1 + (1 - u1) e^{-2k}) / k
 // (Jakob, "Numerically stable sampling of the von Mises-Fisher distribution
 // on S^2", 2012) around its mean, in the orthonormal basis of Duff et al.,
-// "Building an Orthonormal Basis, Revisited" (JCGT 2017).
+// "Building an Orthonormal Basis, Revisited" (JCGT 2017).  The lobe's raw
+// values are picked with selects (no indexed access to the registers); the
+// inversion uses the fast intrinsics (the density above is that of the
+// exact inversion, ~1e-6 relative away).
 XYZ_DEV f3 mix_sample(const GuideMix &M, float ul, float u1, float u2) {
-  int j = 7;
+  float const target = ul * (M.ws > 0.0f ? M.ws : 8.0f);
   float acc = 0.0f;
+  bool found = false;
+  float kr = mix_half(M, 36), mx = mix_half(M, 37), my = mix_half(M, 38), mz = mix_half(M, 39);
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    acc += M.w[i];
-    if (ul < acc) {
-      j = i;
-      break;
-    }
+  for (int i = 0; i < 7; ++i) {
+    acc += mix_weight(M, i);
+    bool const take = !found && target < acc;
+    kr = take ? mix_half(M, 5 * i + 1) : kr;
+    mx = take ? mix_half(M, 5 * i + 2) : mx;
+    my = take ? mix_half(M, 5 * i + 3) : my;
+    mz = take ? mix_half(M, 5 * i + 4) : mz;
+    found = found || take;
   }
-  float const k = M.k[j];
-  float w = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * k)) / k;
+  float const k = fmaxf(kr, 1e-3f);
+  f3 const n = mix_mean(mk3(mx, my, mz));
+  float w = 1.0f + __fdividef(__logf(u1 + (1.0f - u1) * __expf(-2.0f * k)), k);
   w = fminf(fmaxf(w, -1.0f), 1.0f);
   float const sw = sqrtf(fmaxf(0.0f, 1.0f - w * w));
-  float const ph = static_cast<float>(2.0 * kPi) * u2;
-  f3 const n = M.mu[j];
+  float sp, cp;
+  __sincosf(static_cast<float>(2.0 * kPi) * u2, &sp, &cp);
   float const sign = copysignf(1.0f, n.z);
-  float const a = -1.0f / (sign + n.z);
+  float const a = __fdividef(-1.0f, sign + n.z);
   float const bb = n.x * n.y * a;
   f3 const t = mk3(1.0f + sign * n.x * n.x * a, sign * bb, -sign * n.x);
   f3 const bt = mk3(bb, sign + n.y * n.y * a, -n.y);
-  return add3(add3(scl3(t, sw * cosf(ph)), scl3(bt, sw * sinf(ph))), scl3(n, w));
+  return add3(add3(scl3(t, sw * cp), scl3(bt, sw * sp)), scl3(n, w));
 }
 
 XYZ_DEV uint32_t pack_misc(uint32_t dim, uint32_t k, uint32_t specular) {
@@ -578,7 +618,7 @@ XYZ_DEV LightSample sample_light(const DevScene &S, uint64_t seed, uint32_t pixe
 // kModeBatch: paths of many scenes (xyzgpu_batch_*).
 // kModeGuided: directions from the learned guide mixed with Lambert sampling.
 template <int kMode>
-__global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
+__global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shade(WaveArgs A, int b) {
   constexpr bool kAdj = kMode == kModeAdjoint;
   constexpr bool kBatch = kMode == kModeBatch;
   constexpr bool kGuide = kMode == kModeGuided;
@@ -600,6 +640,11 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
     int32_t light_mat = 0;
     float rho = 1.0f;
     int block = 0;
+    // guide_alpha is 0 at bounces without inference: Lambert sampling
+    // alone, and the mixture buffer is not read
+    bool const use_guide = kGuide && A.guide_alpha > 0.0f;
+    GuideMix M;
+    if (use_guide && i < n) load_mix(A.mix + 40 * static_cast<int64_t>(i), M);
     if (i < n) {
       slot = A.q_slot[qi][i];
       float4 const h = A.hits[i];
@@ -702,8 +747,8 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
             if (static_cast<int>(k) >= P.kmax) alive = false;
           }
           uint32_t pixel = 0, sample = 0;
-          GuideMix M;
-          if (kGuide && alive && !is_light) load_mix(A.mix + 40 * static_cast<int64_t>(i), M);
+          if (use_guide && alive && !is_light) finish_mix(M);
+          float nee_pl = 0.0f;  // guided: Lambert density of the light direction (0: no shadow ray)
           if (alive) {
             path_pixel_sample<kBatch>(A, block, slot, &pixel, &sample);
             if (!is_light) {
@@ -734,10 +779,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
                     pbv = mul3(S.power, beta);
                     light_mat = ls.mat;
                     if (!kAdj) pbv = scl3(pbv, __ldg(&S.emission[ls.mat]));
-                    if (kGuide) {
-                      float const pl = nk2 * static_cast<float>(kInvPi);
-                      rho = (A.guide_alpha * mix_pdf(M, neg3(v)) + (1.0f - A.guide_alpha) * pl) / pl;
-                    }
+                    if (use_guide) nee_pl = nk2 * static_cast<float>(kInvPi);
                   }
                 }
               }
@@ -766,27 +808,39 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs A, int b) {
               }
             }
             if (alive && is_light) alive = false;  // Light::NextScatteringDirection
-            if (kGuide && alive) {
+            if (kGuide) {
               // one-sample MIS of the guide (probability alpha) and Lambert
-              // sampling: the path weight uses the mixture density
-              f3 wd;
-              if (rng.next() < A.guide_alpha) {
-                float const ul = rng.next();
-                float const u1 = rng.next();
-                float const u2 = rng.next();
-                wd = mix_sample(M, ul, u1, u2);
-              } else {
-                float const mu_phi = rng.next();
-                float const mu_theta = rng.next();
-                float const phi = static_cast<float>(2.0 * kPi) * mu_phi;
-                float const sin_t = sqrtf(1.0f - mu_theta);
-                wd = add3(add3(scl3(tan, sin_t * cosf(phi)), scl3(bin, sin_t * sinf(phi))),
-                          scl3(sn, sqrtf(mu_theta)));
+              // sampling: the path weight uses the mixture density; one pass
+              // over the lobes gives it for the sampled and the light direction
+              f3 wd = mk3(0.0f, 0.0f, 1.0f);
+              bool cont = false;
+              float cs = 0.0f;
+              if (alive) {
+                if (use_guide && rng.next() < A.guide_alpha) {
+                  float const ul = rng.next();
+                  float const u1 = rng.next();
+                  float const u2 = rng.next();
+                  wd = mix_sample(M, ul, u1, u2);
+                } else {
+                  // cosine-weighted (the density below is evaluated at the
+                  // direction produced, so the fast sincos is exact enough)
+                  float const mu_phi = rng.next();
+                  float const mu_theta = rng.next();
+                  float sp, cp;
+                  __sincosf(static_cast<float>(2.0 * kPi) * mu_phi, &sp, &cp);
+                  float const sin_t = sqrtf(1.0f - mu_theta);
+                  wd = add3(add3(scl3(tan, sin_t * cp), scl3(bin, sin_t * sp)), scl3(sn, sqrtf(mu_theta)));
+                }
+                cs = dot3(wd, sn);
+                cont = cs > 0.0f && dot3(wd, gn) > 0.0f;
               }
-              float const cs = dot3(wd, sn);
-              if (cs > 0.0f && dot3(wd, gn) > 0.0f) {
-                float const pdf = A.guide_alpha * mix_pdf(M, wd) +
-                                  (1.0f - A.guide_alpha) * cs * static_cast<float>(kInvPi);
+              float pm_light = 0.0f, pm_wd = 0.0f;
+              if (use_guide && (cont || nee_pl > 0.0f)) mix_pdf2(M, neg3(vin), wd, &pm_light, &pm_wd);
+              if (nee_pl > 0.0f) rho = (A.guide_alpha * pm_light + (1.0f - A.guide_alpha) * nee_pl) / nee_pl;
+              if (cont) {
+                float const pdf = use_guide ? A.guide_alpha * pm_wd +
+                                                  (1.0f - A.guide_alpha) * cs * static_cast<float>(kInvPi)
+                                            : cs * static_cast<float>(kInvPi);
                 float const lambert = cs * static_cast<float>(kInvPi);
                 beta = scl3(beta, lambert / pdf);
                 reinterpret_cast<float *>(A.radiance + slot)[3] = rr_scale * (pdf / lambert);
