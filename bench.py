@@ -307,8 +307,13 @@ def batch_bench(steps: int, warmup: int):
 GUIDE_CAMERA = ((0.0, 1.5, 1.2), (0.0, 1.1, -2.0), 60.0)
 
 
-def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_spp: int = 1024,
-                max_seconds: float = 30.0, guide_cfg=None, variants=()):
+GUIDE_SETTINGS = dict(train_bounces=5, guide_bounces=9, alpha=0.5, steps_per_pass=512, batch_size=16384)
+# forward flops of one guide query, 2 (192 * 64 + 3 * 64 * 64 + 64 * 40)
+GUIDE_QUERY_FLOPS = 2 * (192 * 64 + 3 * 64 * 64 + 64 * 40)
+
+
+def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_spp: int = 2048,
+                max_seconds: float = 30.0, guide_cfg=None, variants=(), repeats: int = 2):
     """Time to relative MSE 0.01, guided vs plain, on the indirect-lit room
     (196,146 triangles; light only through a 0.1 m gap), 1024 x 1024 camera,
     max depth 10, Russian roulette 0.2.  The error is measured on a band of
@@ -324,8 +329,12 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
     the number of passes times the median pass time (training and rendering
     passes of the guided tracer separately); the plain sum of the pass times
     is reported beside it.  The guided tracer trains during the first 25 % of
-    a planned `plan_spp`.  A tracer that has not reached 0.01 after
-    `max_seconds` reports the time extrapolated from relMSE ~ 1 / spp.  `variants`: further guide settings (dicts of
+    a planned `plan_spp` (Adam steps after every training pass); as in path
+    guiding practice the training passes' samples, drawn while the guide is
+    still immature, are left out of the image, but their time counts.  Plain
+    and guided runs alternate `repeats` times and each tracer reports its
+    faster run.  A tracer that has not reached 0.01 after `max_seconds`
+    reports the time extrapolated from relMSE ~ 1 / spp.  `variants`: further guide settings (dicts of
     guide_cfg overrides, optionally with their own plan_spp) measured against
     the same reference and plain run."""
     import torch
@@ -335,7 +344,7 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
     depth = 10
     sd = scenes.occluded_room()
     cam = scenes.Camera.with_fov(*GUIDE_CAMERA, pinhole=True)
-    cfg = dict(train_bounces=3, guide_bounces=4, alpha=0.5)
+    cfg = dict(GUIDE_SETTINGS)
     cfg.update(guide_cfg or {})
     with api.Scene(sd) as s:
         halves = [torch.zeros((band, W, 3), dtype=torch.float64, device="cuda") for _ in range(2)]
@@ -368,12 +377,15 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
                 e1.record()
                 torch.cuda.synchronize()
                 times.append(e0.elapsed_time(e1) * 1e-3)
-                acc += film[rows[0]:rows[1]].double()
                 p += 1
-                e = relmse(acc / (p * pass_spp))
+                if p <= train_passes:
+                    continue
+                acc += film[rows[0]:rows[1]].double()
+                e = relmse(acc / ((p - train_passes) * pass_spp))
                 tr, rd = times[:train_passes], times[train_passes:]
                 robust = len(tr) * (statistics.median(tr) if tr else 0.0) + len(rd) * (statistics.median(rd) if rd else 0.0)
-                out = {"spp": p * pass_spp, "relmse": round(e, 5), "passes": p,
+                out = {"spp": p * pass_spp, "image_spp": (p - train_passes) * pass_spp, "relmse": round(e, 5),
+                       "passes": p,
                        "median_pass_ms": round(statistics.median(rd if rd else tr) * 1e3, 3),
                        "sum_of_pass_seconds": round(sum(times), 3)}
                 if e <= 0.01:
@@ -389,8 +401,6 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
         with api.Guide(s, **cfg) as g0:
             g0.render(cam, W, H, pass_spp, seed=7, max_depth=depth, rows=rows, train=True)
         torch.cuda.synchronize()
-        plain = run(plain_pass)
-
         def guided_run(gcfg, gplan):
             train_passes = max(1, (gplan // 4) // pass_spp)
             with api.Guide(s, **gcfg) as g:
@@ -399,9 +409,29 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
                              rows=rows, train=p < train_passes)
 
                 res = run(guided_pass, train_passes)
-                return res, gcfg | g.stats() | {"training_spp": train_passes * pass_spp}
+                info = gcfg | g.stats() | {"training_spp": train_passes * pass_spp}
+                # one profiled pass of the trained guide: the network's share
+                # and its rate (queries = extension-queue entries of the
+                # guided bounces; the last bounce and those past guide_bounces
+                # run no inference)
+                g.render(cam, W, H, pass_spp, seed=5, max_depth=depth, rows=rows, profile=1)
+                pr = s.render_profile()
+                nb = min(depth - 1, gcfg.get("guide_bounces", depth))
+                queries = sum(pr["ext_rays_by_iter"][:nb])
+                gms = pr["ms"]["guide"]
+                info["profiled_pass"] = {
+                    "ms": {k: round(v, 3) for k, v in pr["ms"].items()},
+                    "guide_queries": queries,
+                    "guide_inference_tflops": round(queries * GUIDE_QUERY_FLOPS / (gms * 1e-3) / 1e12, 1)
+                    if gms > 0 else None}
+                return res, info
 
-        guided, ginfo = guided_run(cfg, plan_spp)
+        plains, guideds = [], []
+        for _ in range(max(1, repeats)):
+            plains.append(run(plain_pass))
+            guideds.append(guided_run(cfg, plan_spp))
+        plain = min(plains, key=lambda r: r["seconds"])
+        guided, ginfo = min(guideds, key=lambda r: r[0]["seconds"])
         more = []
         for v in variants:
             v = dict(v)
@@ -412,6 +442,8 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
            "plain": plain, "guided": guided,
            "speedup": round(plain["seconds"] / guided["seconds"], 2),
            "guide": ginfo,
+           "runs": {"plain_seconds": [r["seconds"] for r in plains],
+                    "guided_seconds": [r[0]["seconds"] for r in guideds]},
            "reference": {"spp": ref_spp, "seconds": round(ref_s, 2), "own_relmse": round(ref_noise, 5),
                          "tracer": "plain GPU path tracer, float64 sums"},
            "config": f"occluded room, 196,146 triangles, 1024x1024 camera, rows {rows[0]}-{rows[1]}, max depth 10, "
@@ -566,10 +598,11 @@ def run_gpu_arm(args, rank, world):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(sd)
-    adjoint = batch = None
+    adjoint = batch = guiding = None
     if rank == 0 and world == 1 and not args.no_extras:
         adjoint = adjoint_bench(args.steps, args.warmup)
         batch = batch_bench(args.steps, args.warmup)
+        guiding = guide_bench()
 
     if rank == 0:
         line = {
@@ -580,7 +613,7 @@ def run_gpu_arm(args, rank, world):
             "config": workload_config(stats) | {"parallelism": f"sample-parallel x{world}",
                                                  "waves_per_step": counters["waves"]},
             "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-            "adjoint": adjoint, "batch": batch,
+            "adjoint": adjoint, "batch": batch, "guiding": guiding,
             "clocks": clk, "wall_ms_timed_region": round(wall_ms, 1),
             "render_counters": counters,
         }
@@ -597,7 +630,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the differentiable-rendering and batched-rendering measurements")
+                    help="skip the differentiable-rendering, batched-rendering and guided-rendering measurements")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -210,11 +210,13 @@ typedef struct {
 /* Counters of the last xyzgpu_render on this scene (synchronises). */
 int xyzgpu_render_counters_get(xyzgpu_scene scene, xyzgpu_render_counters *out);
 
-/* Per-kernel-class profile of the last xyzgpu_render that had profile != 0
- * (synchronises).  Classes: 0 raygen, 1 extension trace, 2 shade,
- * 3 shadow trace, 4 film.  ms: summed CUDA-event time (TIMING); the traversal
- * counters are filled by a COUNTERS render. */
-#define XYZGPU_KERNEL_CLASSES 5
+/* Per-kernel-class profile of the last xyzgpu_render (or
+ * xyzgpu_render_guided) that had profile != 0 (synchronises).  Classes:
+ * 0 raygen, 1 extension trace, 2 shade, 3 shadow trace, 4 film, 5 guide
+ * (network inference per bounce and, in training renders, the training
+ * records and Adam steps).  ms: summed CUDA-event time (TIMING); the
+ * traversal counters are filled by a COUNTERS render. */
+#define XYZGPU_KERNEL_CLASSES 6
 #define XYZGPU_PROFILE_MAX_ITERS 64
 typedef struct {
   uint64_t launches[XYZGPU_KERNEL_CLASSES];

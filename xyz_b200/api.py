@@ -120,7 +120,7 @@ class BatchStats(C.Structure):
 
 
 class RenderProfile(C.Structure):
-    _fields_ = [("launches", C.c_uint64 * 5), ("ms", C.c_double * 5), ("ext_rays", C.c_uint64),
+    _fields_ = [("launches", C.c_uint64 * 6), ("ms", C.c_double * 6), ("ext_rays", C.c_uint64),
                 ("ext_nodes", C.c_uint64), ("ext_leaves", C.c_uint64), ("ext_tri_tests", C.c_uint64),
                 ("shadow_rays", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_leaves", C.c_uint64),
                 ("shadow_tri_tests", C.c_uint64), ("shadow_visible", C.c_uint64),
@@ -128,7 +128,7 @@ class RenderProfile(C.Structure):
                 ("shadow_rays_by_iter", C.c_uint64 * 64)]
 
 
-KERNEL_CLASSES = ["raygen", "trace_extension", "shade", "trace_shadow", "film"]
+KERNEL_CLASSES = ["raygen", "trace_extension", "shade", "trace_shadow", "film", "guide"]
 
 
 class RenderCounters(C.Structure):
@@ -633,9 +633,11 @@ class Guide:
 
     def render(self, camera, width: int, height: int, spp: int, *, train: bool = False, seed: int = 0,
                spp_offset: int = 0, max_depth: int = 15, rr_start_depth: int = 1, rr_threshold: float = 0.2,
-               film=None, accumulate: bool = False, wave_paths: int = 0, rows=None, stream=None):
+               film=None, accumulate: bool = False, wave_paths: int = 0, rows=None, profile: int = 0,
+               stream=None):
         """xyzgpu_render_guided into a CUDA film (H, W, 3) of sums; train: learn
-        from this render's paths (Adam steps after each wave)."""
+        from this render's paths (Adam steps after each wave); profile=1: per
+        kernel class timing (Scene.render_profile, class "guide" = the network)."""
         import torch
         if film is None:
             film = torch.zeros((height, width, 3), dtype=torch.float32, device="cuda")
@@ -643,6 +645,7 @@ class Guide:
         rp = render_params(width, height, spp, seed=seed, spp_offset=spp_offset, max_depth=max_depth,
                            rr_start_depth=rr_start_depth, rr_threshold=rr_threshold, accumulate=accumulate,
                            wave_paths=wave_paths, rows=rows)
+        rp.profile = profile
         rp.film_location = XYZGPU_FILM_DEVICE
         _check(_LIB.xyzgpu_render_guided(self.handle, C.byref(cam), C.byref(rp), int(bool(train)),
                                          film.data_ptr(), _stream_ptr(stream)))

@@ -298,9 +298,11 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
           A.guide_alpha = guided_here ? gw.alpha : 0.0f;
           if (guided_here) {
             int const qi = b & 1;
+            XYZ_MARK(5, true);
             int const r = guide_infer_launch(*guide->g, A.q_o[qi], A.q_d[qi], A.hits,
                                              A.counts + b * kCountStride + kCExt, A.S, gw.mix, st);
             if (r) return r;
+            XYZ_MARK(5, false);
             ++launches;
           }
           XYZ_MARK(2, true);
@@ -346,14 +348,16 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
         XYZ_MARK(4, false);
         ++launches;
       }
-#undef XYZ_MARK
       k_tally<<<1, 32, 0, st>>>(A, iters, w.tally);
       ++launches;
       XYZ_CUDA_TRY(cudaGetLastError());
       if (guide && A.train_bounces > 0) {
+        XYZ_MARK(5, true);
         int const r = guide_train_on_wave(*guide->g, A.radiance, A.npaths, st);
         if (r) return r;
+        XYZ_MARK(5, false);
       }
+#undef XYZ_MARK
       rc_out.paths += static_cast<uint64_t>(A.npaths);
       rc_out.waves += 1;
     }
