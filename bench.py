@@ -453,6 +453,33 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
     return out
 
 
+def guide_profile_case():
+    """The guide's kernels on a small case for ncu: one Adam step on 65,536
+    synthetic training rows (k_guide_gradient), then one guided 64-spp pass
+    over rows 496-528 of the occluded room at 1024 x 1024 (k_guide_infer at
+    every bounce; the first launch sees the 2,097,152 camera hits)."""
+    import numpy as np
+    import torch
+    from xyz_b200 import api, scenes
+    W = H = 1024
+    rows = (H // 2 - 16, H // 2 + 16)
+    sd = scenes.occluded_room()
+    cam = scenes.Camera.with_fov(*GUIDE_CAMERA, pinhole=True)
+    rng = np.random.default_rng(0)
+    n = 1 << 16
+    rec = np.zeros((n, 10), np.float32)
+    rec[:, 0:3] = rng.uniform(-2.0, 2.0, (n, 3))
+    for c in (3, 6):
+        v = rng.normal(size=(n, 3))
+        rec[:, c:c + 3] = v / np.linalg.norm(v, axis=1, keepdims=True)
+    rec[:, 9] = rng.exponential(1.0, n)
+    with api.Scene(sd) as s, api.Guide(s, **GUIDE_SETTINGS) as g:
+        g.train_step(torch.from_numpy(rec).cuda())
+        f = g.render(cam, W, H, 64, seed=5, max_depth=10, rows=rows)
+        torch.cuda.synchronize()
+        print(json.dumps({"guide_profile_case": "ok", "film_sum": float(f.sum())}))
+
+
 def profiled_traffic():
     """DRAM bytes per traced ray of the trace kernel from the committed ncu
     summary (profiles/trace_queue_spheres1m.txt), if present."""
@@ -631,7 +658,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the differentiable-rendering, batched-rendering and guided-rendering measurements")
+    ap.add_argument("--guide-profile-case", action="store_true",
+                    help="run only the guide kernels' small profiling case (for ncu) and exit")
     args = ap.parse_args()
+    if args.guide_profile_case:
+        guide_profile_case()
+        return
     if args.warmup < 3:
         args.warmup = 3
 
