@@ -526,23 +526,17 @@ def run_gpu_arm(args, rank, world):
         dist.barrier()
 
     clocks = ClockSampler(dev)
-    ms_cls = {k: 0.0 for k in api.KERNEL_CLASSES}
-    n_cls = {k: 0 for k in api.KERNEL_CLASSES}
-    launches = 0
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
     t_wall = time.perf_counter()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    # the K steps are enqueued back to back with no host synchronisation in
+    # between, so the device time does not depend on host scheduling
     ev0.record()
     for k in range(args.steps):
-        step(offset, profile=1)
-        prof = scene.render_profile()
-        for c in api.KERNEL_CLASSES:
-            ms_cls[c] += prof["ms"][c]
-            n_cls[c] += prof["launches"][c]
-        launches += scene.render_counters()["kernel_launches"]
+        step(offset)
     ev1.record()
     torch.cuda.synchronize()
     if dist is not None:
@@ -558,6 +552,13 @@ def run_gpu_arm(args, rank, world):
     samples_per_step = W_PIX * H_PIX * SPP
     value = samples_per_step * world * args.steps / (ms / 1000.0) / 1e6
 
+    # per-kernel-class times and launch counts from one profiled step (CUDA
+    # events around every launch), outside the timed region
+    step(offset, profile=1)
+    prof = scene.render_profile()
+    ms_cls = {c: prof["ms"][c] * args.steps for c in api.KERNEL_CLASSES}
+    n_cls = {c: prof["launches"][c] * args.steps for c in api.KERNEL_CLASSES}
+    launches = scene.render_counters()["kernel_launches"] * args.steps
     # work per ray from one counted render (outside the timed region)
     step(offset, profile=2)
     cp = scene.render_profile()

@@ -59,89 +59,15 @@ XYZ_DEV bool hit_triangle(const float4 *__restrict__ tri, int32_t i, f3 o, f3 d,
   return true;
 }
 
-// One 16-byte record so that a push or pop is a single vector access to the
-// (local-memory) stack.
-struct __align__(16) StackEntry {
+// A deferred far child: its node and exit distance.  Its entry distance is
+// not stored: in front-to-back order the far child pushed last is popped
+// right after the subtree that ends at its split plane, so the entry equals
+// the exit distance of the leaf just finished (8 bytes per entry keep the
+// local-memory stack small; it competes with node fetches for L1).
+struct __align__(8) StackEntry {
   uint32_t node;
-  float tn, tf;
-  uint32_t pad;
+  float tf;
 };
-
-// Closest hit in [tmin, tmax].  h.id = -1 on a miss.  Counts work if cnt != 0.
-template <bool kCount>
-XYZ_DEV void trace_closest(const DevScene &S, f3 o, f3 d, float tmin, float tmax, RayHit &h,
-                           TraceCount *cnt) {
-  h.t = tmax;
-  h.id = -1;
-  h.f = h.g = 0.0f;
-  h.back = 0;
-  float const inv[3] = {__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z)};
-  float const org[3] = {o.x, o.y, o.z};
-  float const lo[3] = {S.bmin.x, S.bmin.y, S.bmin.z};
-  float const hi[3] = {S.bmax.x, S.bmax.y, S.bmax.z};
-  float t0 = tmin, t1 = tmax;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    float const ta = (lo[k] - org[k]) * inv[k];
-    float const tb = (hi[k] - org[k]) * inv[k];
-    t0 = fmaxf(t0, fminf(ta, tb));
-    t1 = fminf(t1, fmaxf(ta, tb));
-  }
-  if (!(t0 <= t1)) return;
-
-  StackEntry stack[kKdMaxDepthLimit];
-  int sp = 0;
-  uint32_t node = 0;
-  float tn = t0, tf = t1;
-  for (;;) {
-    uint2 nd = __ldg(&S.nodes[node]);
-    if (kCount) cnt->nodes++;
-    while ((nd.y & 3u) != kKdLeafTag) {
-      uint32_t const ax = nd.y & 3u;
-      float const split = __uint_as_float(nd.x);
-      uint32_t const child = nd.y >> 2;
-      float const oa = ax == 0 ? org[0] : (ax == 1 ? org[1] : org[2]);
-      float const ia = ax == 0 ? inv[0] : (ax == 1 ? inv[1] : inv[2]);
-      float const da = ax == 0 ? d.x : (ax == 1 ? d.y : d.z);
-      float const tp = (split - oa) * ia;
-      // near side: the origin's side; an origin on the plane takes the side
-      // its direction enters (the reference would take the far child there,
-      // since its plane distance 0 is below t_min, and skip the near one).
-      uint32_t const above_first = (oa < split || (oa == split && da <= 0.0f)) ? 0u : 1u;
-      uint32_t const first = child + above_first;
-      uint32_t const second = child + (above_first ^ 1u);
-      if ((tp > tf) || (tp <= 0.0f)) {
-        node = first;
-      } else if (tp < tn) {
-        node = second;
-      } else {
-        stack[sp] = StackEntry{second, tp, tf, 0u};
-        ++sp;
-        node = first;
-        tf = tp;
-      }
-      nd = __ldg(&S.nodes[node]);
-      if (kCount) cnt->nodes++;
-    }
-    uint32_t const n = nd.y >> 2;
-    if (kCount) {
-      cnt->leaves++;
-      cnt->tris += n;
-    }
-    for (uint32_t j = 0; j < n; ++j) {
-      int32_t const i = __ldg(&S.refs[nd.x + j]);
-      hit_triangle(S.tri, i, o, d, tmin, h);
-    }
-    if (h.id >= 0 && h.t <= tf) break;
-    if (sp == 0) break;
-    --sp;
-    StackEntry const e = stack[sp];
-    node = e.node;
-    tn = e.tn;
-    tf = e.tf;
-    if (h.id >= 0 && h.t < tn) break;
-  }
-}
 
 // Persistent closest-hit loop over rays [0, n) taken from a shared work
 // counter, with per-lane refill: after every leaf visit the lanes whose ray
@@ -245,7 +171,7 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
       } else if (tp < tn) {
         node = second;
       } else {
-        stack[sp] = StackEntry{second, tp, tf, 0u};
+        stack[sp] = StackEntry{second, tf};
         ++sp;
         node = first;
         tf = tp;
@@ -265,15 +191,14 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
       int32_t const t = __ldg(&refs[nd.x + j]);
       hit_triangle(tris, t, o, d, tmin, h);
     }
-    // next leaf, or done
-    bool done = (h.id >= 0 && h.t <= tf) || sp == 0;
+    // next leaf (entered at this leaf's exit), or done
+    bool const done = (h.id >= 0 && h.t <= tf) || sp == 0;
     if (!done) {
       --sp;
       StackEntry const e = stack[sp];
       node = e.node;
-      tn = e.tn;
+      tn = tf;
       tf = e.tf;
-      done = h.id >= 0 && h.t < tn;
     }
     if (done) {
       sink.store(ray, h);

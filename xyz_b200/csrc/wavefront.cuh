@@ -498,7 +498,7 @@ struct ShadowSink {
 };
 
 template <bool kShadow, bool kCount, int kMode = kModePlain>
-__global__ void __launch_bounds__(kThreads) k_trace_queue(WaveArgs A, int b,
+__global__ void __launch_bounds__(kThreads, 10) k_trace_queue(WaveArgs A, int b,
                                                           unsigned long long *prof) {
   constexpr bool kBatch = kMode == kModeBatch;
   int32_t *const cnt = A.counts + b * kCountStride;
