@@ -659,9 +659,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the differentiable-rendering, batched-rendering and guided-rendering measurements")
+    ap.add_argument("--spp", type=int, default=None,
+                    help="samples per pixel per step (default 64; smaller for profiler captures)")
     ap.add_argument("--guide-profile-case", action="store_true",
                     help="run only the guide kernels' small profiling case (for ncu) and exit")
     args = ap.parse_args()
+    if args.spp is not None:
+        global SPP
+        SPP = max(1, args.spp)
     if args.guide_profile_case:
         guide_profile_case()
         return

@@ -427,6 +427,20 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
     for (int64_t j = 0; j < s->n_nodes; ++j) nodes[j] = make_uint2(tree.nodes[2 * j], tree.nodes[2 * j + 1]);
     int r2 = dev_upload(&s->d_nodes, nodes.data(), nodes.size(), &bytes, st);
     if (!r2) r2 = dev_upload(&s->d_refs, tree.refs.data(), tree.refs.size(), &bytes, st);
+    if (!r2) {
+      // level ranges of the breadth-first array: each level's interior nodes
+      // own the next level's child pairs
+      std::vector<int64_t> level_start{0};
+      int64_t b = 0, e = s->n_nodes > 0 ? 1 : 0;
+      while (e > b) {
+        level_start.push_back(e);
+        int64_t interior = 0;
+        for (int64_t j = b; j < e; ++j) interior += (nodes[j].y & 3u) != kKdLeafTag;
+        b = e;
+        e = b + 2 * interior;
+      }
+      if (s->n_nodes > 0) r2 = kd_layout_depth_first(*s, level_start, st);
+    }
     if (r2) {
       free_scene(s);
       return r2;

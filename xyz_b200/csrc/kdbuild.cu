@@ -17,6 +17,15 @@
 //              keep the parent's order) or into the leaf reference array
 // The host reads two small values per level (the big-node count and the scan
 // totals) to size the next level; everything else stays on the device.
+//
+// Layout (kd_layout_depth_first, after either builder): the breadth-first
+// array is permuted so that every subtree occupies one contiguous range, in
+// depth-first order of child pairs: a pair (first, second) is followed by
+// the first child's descendants, then the second's.  A ray descending into
+// the first child finds that child's pair in the next bytes, usually the
+// same 32-byte sector, and rays working in one region of space read one
+// region of the array.  Node words keep their format; only child indices
+// change.
 #include <algorithm>
 #include <vector>
 
@@ -656,6 +665,55 @@ int grid_for(int64_t work, int threads, int device) {
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, int64_t{sm_count(device)} * 16)));
 }
 
+// ---- depth-first layout
+// Descendant counts of the nodes [begin, end) of one level (their children
+// lie in deeper levels, counted before).
+__global__ void k_layout_desc(const uint2 *__restrict__ nodes, int64_t begin, int64_t end, int32_t *desc) {
+  for (int64_t i = begin + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < end;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint2 const nd = nodes[i];
+    if ((nd.y & 3u) == kKdLeafTag) {
+      desc[i] = 0;
+    } else {
+      uint32_t const c = nd.y >> 2;
+      desc[i] = 2 + desc[c] + desc[c + 1];
+    }
+  }
+}
+
+__global__ void k_layout_root(int32_t *pos, int32_t *base) {
+  pos[0] = 0;
+  base[0] = 1;
+}
+
+// New positions of the children of the nodes [begin, end): the pair at
+// base(parent); the first child's descendants from base + 2, the second's
+// after them.
+__global__ void k_layout_place(const uint2 *__restrict__ nodes, int64_t begin, int64_t end,
+                               const int32_t *__restrict__ desc, int32_t *pos, int32_t *base) {
+  for (int64_t i = begin + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < end;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint2 const nd = nodes[i];
+    if ((nd.y & 3u) == kKdLeafTag) continue;
+    uint32_t const c = nd.y >> 2;
+    int32_t const b = base[i];
+    pos[c] = b;
+    pos[c + 1] = b + 1;
+    base[c] = b + 2;
+    base[c + 1] = b + 2 + desc[c];
+  }
+}
+
+__global__ void k_layout_scatter(const uint2 *__restrict__ nodes, int64_t n, const int32_t *__restrict__ pos,
+                                 const int32_t *__restrict__ base, uint2 *__restrict__ out) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint2 nd = nodes[i];
+    if ((nd.y & 3u) != kKdLeafTag) nd.y = (static_cast<uint32_t>(base[i]) << 2) | (nd.y & 3u);
+    out[pos[i]] = nd;
+  }
+}
+
 }  // namespace
 
 #define XYZ_BUILD_TRY(call)                                                                       \
@@ -720,7 +778,9 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
 
   int64_t level_base = 0, leaf_total = 0, leaves = 0, empty = 0;
   int m = 1, depth = 0, cur = 0;
+  std::vector<int64_t> level_start;
   for (depth = 0;; ++depth) {
+    level_start.push_back(level_base);
     A.depth = depth;
     LevelArrays L = lv[cur].view();
     // big nodes
@@ -780,6 +840,7 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
     cur ^= 1;
   }
   XYZ_BUILD_TRY(cudaStreamSynchronize(st));
+  level_start.push_back(level_base);
   s.n_nodes = level_base;
   s.n_refs = leaf_total;
   s.n_leaves = leaves;
@@ -787,6 +848,37 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
   s.depth = depth;
   s.d_nodes = nodes.release();
   s.d_refs = leaf_refs.release();
+  return kd_layout_depth_first(s, level_start, st);
+}
+
+int kd_layout_depth_first(SceneImpl &s, const std::vector<int64_t> &level_start, cudaStream_t st) {
+  int64_t const n = s.n_nodes;
+  if (n <= 1) return XYZGPU_OK;
+  if (level_start.size() < 2 || level_start.front() != 0 || level_start.back() != n)
+    return set_error(XYZGPU_E_INVALID, "kd-tree layout: level ranges do not cover the nodes");
+  int const dev = s.device;
+  DevBuf<int32_t> desc, pos, base;
+  DevBuf<uint2> out;
+  desc.st = pos.st = base.st = out.st = st;
+  XYZ_BUILD_TRY(desc.reserve(n));
+  XYZ_BUILD_TRY(pos.reserve(n));
+  XYZ_BUILD_TRY(base.reserve(n));
+  XYZ_BUILD_TRY(out.reserve(n));
+  size_t const levels = level_start.size() - 1;
+  for (size_t l = levels; l-- > 0;) {
+    int64_t const b = level_start[l], e = level_start[l + 1];
+    if (e > b) k_layout_desc<<<grid_for(e - b, 256, dev), 256, 0, st>>>(s.d_nodes, b, e, desc.p);
+  }
+  k_layout_root<<<1, 1, 0, st>>>(pos.p, base.p);
+  for (size_t l = 0; l < levels; ++l) {
+    int64_t const b = level_start[l], e = level_start[l + 1];
+    if (e > b) k_layout_place<<<grid_for(e - b, 256, dev), 256, 0, st>>>(s.d_nodes, b, e, desc.p, pos.p, base.p);
+  }
+  k_layout_scatter<<<grid_for(n, 256, dev), 256, 0, st>>>(s.d_nodes, n, pos.p, base.p, out.p);
+  XYZ_BUILD_TRY(cudaGetLastError());
+  XYZ_BUILD_TRY(cudaFreeAsync(s.d_nodes, st));
+  s.d_nodes = out.release();
+  XYZ_BUILD_TRY(cudaStreamSynchronize(st));
   return XYZGPU_OK;
 }
 

@@ -133,6 +133,9 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
                           float *film, cudaStream_t st);
 int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig &cfg,
                     cudaStream_t st);
+// Permutes the scene's breadth-first node array (level l = nodes
+// [level_start[l], level_start[l + 1])) into depth-first order of child pairs.
+int kd_layout_depth_first(SceneImpl &s, const std::vector<int64_t> &level_start, cudaStream_t st);
 int sm_count(int device);
 
 }  // namespace xyzgpu
