@@ -418,6 +418,8 @@ __global__ void __launch_bounds__(kThreads) k_raygen(WaveArgs A) {
 // Persistent warps with per-lane refill over a device-sized queue
 // (trace_persistent).  kShadow: the ray starts at a light point and the
 // vertex's NEE term is added when the closest hit is the vertex's own triangle.
+// Queue records are read and written once: streaming (evict-first) accesses
+// keep them from displacing tree nodes and triangles in L1.
 template <bool kBatch>
 struct ExtSink {
   const float4 *__restrict__ qo;
@@ -425,7 +427,7 @@ struct ExtSink {
   float4 *__restrict__ hits;
   const WaveArgs *A;
   XYZ_DEV void load(int i, f3 &o, f3 &d, float &tmin, float &tmax) const {
-    float4 const a = qo[i], b = qd[i];
+    float4 const a = __ldcs(&qo[i]), b = __ldcs(&qd[i]);
     o = xyz3(a);
     d = xyz3(b);
     tmin = kBatch ? kRayTMin : a.w;  // batched: w holds the path's block
@@ -436,7 +438,7 @@ struct ExtSink {
   }
   XYZ_DEV void store(int i, const RayHit &h) {
     int32_t const code = h.id >= 0 ? ((h.id << 1) | h.back) : -1;
-    hits[i] = make_float4(h.t, h.f, h.g, __int_as_float(code));
+    __stcs(&hits[i], make_float4(h.t, h.f, h.g, __int_as_float(code)));
   }
 };
 
@@ -448,7 +450,7 @@ struct ShadowSink {
   const WaveArgs *A;
   uint32_t visible;
   XYZ_DEV void load(int i, f3 &o, f3 &d, float &tmin, float &tmax) const {
-    float4 const a = A->s_o[i], b = A->s_d[i];
+    float4 const a = __ldcs(&A->s_o[i]), b = __ldcs(&A->s_d[i]);
     o = xyz3(a);
     d = xyz3(b);
     tmin = kRayTMin;
