@@ -82,6 +82,13 @@ struct __align__(8) StackEntry {
 //   Sink::scene(i)                    (kBatch) the scene of ray i; rays of one
 //                                     queue may belong to different scenes
 constexpr int kRefillIdle = 12;
+// A round descends at most this many nodes; a lane still above its next leaf
+// resumes there in the next round, so the warp's leaf tests do not wait for
+// its longest descent (counting renders descend without the cap).
+#ifndef XYZ_DESCEND_STEPS
+#define XYZ_DESCEND_STEPS 8
+#endif
+constexpr int kDescendSteps = XYZ_DESCEND_STEPS;
 
 template <bool kCount, bool kBatch = false, class Sink>
 XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, TraceCount &tc) {
@@ -155,7 +162,9 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
     // descend to a leaf
     uint2 nd = __ldg(&nodes[node]);
     if (kCount) tc.nodes++;
-    while ((nd.y & 3u) != kKdLeafTag) {
+    int steps = 0;
+    while ((nd.y & 3u) != kKdLeafTag && (kCount || steps < kDescendSteps)) {
+      ++steps;
       uint32_t const ax = nd.y & 3u;
       float const split = __uint_as_float(nd.x);
       uint32_t const child = nd.y >> 2;
@@ -179,6 +188,7 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
       nd = __ldg(&nodes[node]);
       if (kCount) tc.nodes++;
     }
+    if ((nd.y & 3u) != kKdLeafTag) continue;  // resumes at `node` next round
     // test the leaf
     uint32_t const cnt = nd.y >> 2;
     if (kCount) {
@@ -187,8 +197,10 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
     }
     const int32_t *__restrict__ refs = kBatch ? lane_scene->refs : S.refs;
     const float4 *__restrict__ tris = kBatch ? lane_scene->tri : S.tri;
+    int32_t t_next = cnt > 0 ? __ldg(&refs[nd.x]) : 0;
     for (uint32_t j = 0; j < cnt; ++j) {
-      int32_t const t = __ldg(&refs[nd.x + j]);
+      int32_t const t = t_next;
+      if (j + 1 < cnt) t_next = __ldg(&refs[nd.x + j + 1]);
       hit_triangle(tris, t, o, d, tmin, h);
     }
     // next leaf (entered at this leaf's exit), or done
