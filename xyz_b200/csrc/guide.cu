@@ -558,25 +558,48 @@ struct InferArgs {
   __half *mix;
 };
 
-// Surface point (position, shading normal facing the incoming ray) of queue
-// entry i, as the shading kernel computes it; the default row for a miss.
-__device__ void infer_features(const InferArgs &I, int i, float4 h, float f[6]) {
-  f[0] = f[1] = f[2] = f[3] = f[4] = 0.0f;
-  f[5] = 1.0f;
-  int32_t const code = __float_as_int(h.w);
+// One queue entry's inputs: hit record, ray origin and direction, and the
+// hit triangle's shading normals (n0, n1 - n0, n2 - n0; or the geometric
+// normal in n0 for scenes without normals).  The kernel loads them one and
+// two tiles ahead so that these gathers overlap the network of the current
+// tile.
+struct InferRow {
+  float4 h, o, d, n0, s1, s2;
+};
+
+__device__ __forceinline__ float4 miss_hit() { return make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1)); }
+
+// Ray and normals of entry i (its hit record r.h already loaded).
+__device__ __forceinline__ void infer_gather(const InferArgs &I, int i, InferRow &r) {
+  int32_t const code = __float_as_int(r.h.w);
   if (code < 0) return;
   int const tri = code >> 1;
-  float4 const o4 = I.qo[i], d4 = I.qd[i];
-  f3 const pos = add3(xyz3(o4), scl3(xyz3(d4), h.x));
+  r.o = I.qo[i];
+  r.d = I.qd[i];
+  if (I.tri_sn) {
+    r.n0 = __ldg(&I.tri_sn[3 * tri]);
+    r.s1 = __ldg(&I.tri_sn[3 * tri + 1]);
+    r.s2 = __ldg(&I.tri_sn[3 * tri + 2]);
+  } else {
+    r.n0 = __ldg(&I.tri_ng[tri]);
+  }
+}
+
+// Surface point (position, shading normal facing the incoming ray) of a
+// gathered entry, as the shading kernel computes it; the default row for a
+// miss.
+__device__ void infer_features(const InferArgs &I, const InferRow &r, float f[6]) {
+  f[0] = f[1] = f[2] = f[3] = f[4] = 0.0f;
+  f[5] = 1.0f;
+  int32_t const code = __float_as_int(r.h.w);
+  if (code < 0) return;
+  f3 const pos = add3(xyz3(r.o), scl3(xyz3(r.d), r.h.x));
   f3 sn;
   if (I.tri_sn) {
-    f3 const n0 = xyz3(__ldg(&I.tri_sn[3 * tri])), s1 = xyz3(__ldg(&I.tri_sn[3 * tri + 1])),
-             s2 = xyz3(__ldg(&I.tri_sn[3 * tri + 2]));
-    sn = normalize3(add3(add3(n0, scl3(s1, h.y)), scl3(s2, h.z)));
+    sn = normalize3(add3(add3(xyz3(r.n0), scl3(xyz3(r.s1), r.h.y)), scl3(xyz3(r.s2), r.h.z)));
   } else {
-    f3 const gn = xyz3(__ldg(&I.tri_ng[tri]));
     f3 const z = mk3(0.0f, 0.0f, 0.0f);
-    sn = normalize3(add3(add3(gn, scl3(z, h.y)), scl3(z, h.z)));
+    sn = normalize3(add3(add3(xyz3(r.n0), scl3(z, r.h.y)), scl3(z, r.h.z)));
   }
   if (code & 1) sn = neg3(sn);
   f[0] = pos.x, f[1] = pos.y, f[2] = pos.z, f[3] = sn.x, f[4] = sn.y, f[5] = sn.z;
@@ -595,15 +618,20 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_guide_infer(const __grid_c
   int const ntiles = (n + kRows - 1) / kRows;
   int const step = kGroups * gridDim.x;
   int tile = kGroups * blockIdx.x + gi;
-  // the hit record of this thread's row of the next tile is loaded one tile ahead
-  float4 hnext = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
-  if (tile < ntiles && tile * kRows + c.t < n) hnext = I.hits[tile * kRows + c.t];
+  // this thread's row: entry i of tile `tile`; the next tile's ray and normals
+  // are gathered while this tile runs, its hit record one tile earlier
+  auto row_of = [&](int tl) { return tl * kRows + c.t; };
+  auto valid = [&](int tl) { return tl < ntiles && row_of(tl) < n; };
+  InferRow cur{}, nxt{};
+  cur.h = valid(tile) ? I.hits[row_of(tile)] : miss_hit();
+  infer_gather(I, row_of(tile), cur);
+  nxt.h = valid(tile + step) ? I.hits[row_of(tile + step)] : miss_hit();
   for (; tile < ntiles; tile += step) {
-    int const i = tile * kRows + c.t;
+    int const i = row_of(tile);
     float f[6];
-    infer_features(I, i, i < n ? hnext : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1)), f);
-    int const inext = (tile + step) * kRows + c.t;
-    if (tile + step < ntiles && inext < n) hnext = I.hits[inext];
+    infer_features(I, cur, f);
+    if (valid(tile + step)) infer_gather(I, row_of(tile + step), nxt);
+    float4 const h2 = valid(tile + 2 * step) ? I.hits[row_of(tile + 2 * step)] : miss_hit();
     encode_row(c.x, c.t, G, f);
     float o[kW];
     if (!forward(S.wt, c, phase, false, o)) {
@@ -646,6 +674,9 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_guide_infer(const __grid_c
 #pragma unroll
       for (int t = 0; t < 5; ++t) dst[t] = make_uint4(wv[4 * t], wv[4 * t + 1], wv[4 * t + 2], wv[4 * t + 3]);
     }
+    cur = nxt;
+    nxt = InferRow{};
+    nxt.h = h2;
   }
   teardown(S.tmem, 256, aborted, c.mbar, phase);
 }
