@@ -14,6 +14,7 @@
 // Header-only; link with libxyzgpu.so.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -248,6 +249,60 @@ class PathTracer {
       if (on_pass && !on_pass(*film, done)) break;
     }
     return done;
+  }
+};
+
+// PathTracer::run with the learned path guide (xyzgpu_guide_*, no
+// counterpart in the reference): the first `train_fraction` of the samples
+// train the guide (Adam steps after every pass) and, drawn while the guide is
+// still immature, go to a scratch film; the rest are rendered with the guide
+// into `film`, so `film` holds total_spp - training samples, the number run()
+// returns and the callback receives.  The estimator is unbiased with any
+// guide (one-sample MIS with Lambert sampling).
+class GuidedPathTracer {
+ public:
+  int max_depth = 15;
+  int rr_start_depth = 1;
+  float rr_threshold = 0.2f;
+  uint64_t seed = 0;
+  double train_fraction = 0.25;
+  xyzgpu_guide_config config;
+
+  GuidedPathTracer() { xyzgpu_guide_config_default(&config); }
+
+  int run(const Scene &scene, ImageFilm *film, int total_spp, int interval,
+          const std::function<bool(const ImageFilm &, int)> &on_pass = {}) const {
+    film->Resize(scene.GetWidth(), scene.GetHeight());
+    ImageFilm scratch(scene.GetWidth(), scene.GetHeight());
+    xyzgpu_guide g = nullptr;
+    check(xyzgpu_guide_create(scene.handle(), &config, &g));
+    struct Guard {
+      xyzgpu_guide g;
+      ~Guard() { xyzgpu_guide_destroy(g); }
+    } guard{g};
+    int const train = std::min(total_spp, static_cast<int>(total_spp * train_fraction));
+    int done = 0;
+    while (done < total_spp) {
+      bool const training = done < train;
+      int const n = std::min(interval, (training ? train : total_spp) - done);
+      xyzgpu_render_params rp;
+      xyzgpu_render_params_default(&rp);
+      rp.width = scene.GetWidth();
+      rp.height = scene.GetHeight();
+      rp.spp = n;
+      rp.spp_offset = done;
+      rp.max_depth = max_depth;
+      rp.rr_start_depth = rr_start_depth;
+      rp.rr_threshold = rr_threshold;
+      rp.seed = seed;
+      rp.film_location = XYZGPU_FILM_HOST;
+      rp.accumulate = 1;
+      check(xyzgpu_render_guided(g, &scene.ThinLensCamera().desc(), &rp, training ? 1 : 0,
+                                 training ? scratch.data() : film->data(), nullptr));
+      done += n;
+      if (!training && on_pass && !on_pass(*film, done - train)) break;
+    }
+    return done - train;
   }
 };
 

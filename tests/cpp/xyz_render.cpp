@@ -2,11 +2,12 @@
 // the way the reference's shell drives xyz::Scene and PathTracer
 // (xyz/core/shell.cpp:204-497: load, set eye/at/dim, ren).
 //
-//   xyz_render <scene_dir> <out.pfm> <spp> <interval> <seed> <max_depth>
+//   xyz_render <scene_dir> <out.pfm> <spp> <interval> <seed> <max_depth> [--guided]
 //       scene_dir holds positions.f32 triangles.i32 material.i32 albedo.f32
 //       is_light.i32 power.f32 camera.f32 (eye, at, film, focal, F, pinhole)
 //       dims.i32 (W, H) and, optionally, normals.f32; writes the film / spp as
-//       PFM after every pass and prints "passes N spp S sum X".
+//       PFM after every pass and prints "passes N spp S sum X"; --guided renders
+//       with GuidedPathTracer (the first quarter of the samples train the guide).
 //   xyz_render --film-selftest <out.pfm> <out.float>
 //       writes a synthetic 3 x 2 film with both writers (no GPU needed).
 #include <cstdio>
@@ -42,8 +43,9 @@ int main(int argc, char **argv) {
     bool const ok = film.Save(argv[2], 2.0f) && film.Save(argv[3], 2.0f) && !film.Save("x.bmp", 2.0f);
     return ok ? 0 : 1;
   }
-  if (argc != 7) {
-    std::fprintf(stderr, "usage: xyz_render <scene_dir> <out.pfm> <spp> <interval> <seed> <max_depth>\n");
+  bool const guided = argc == 8 && std::string(argv[7]) == "--guided";
+  if (argc != 7 && !guided) {
+    std::fprintf(stderr, "usage: xyz_render <scene_dir> <out.pfm> <spp> <interval> <seed> <max_depth> [--guided]\n");
     return 2;
   }
   std::string const dir = argv[1];
@@ -67,17 +69,25 @@ int main(int argc, char **argv) {
     scene.ThinLensCamera().SetFNumber(cam[8]);
     scene.ThinLensCamera().SetPinhole(cam[9] > 0.5f);
     scene.SetDimension(dims[0], dims[1]);                    // set dim
-    xyzgpu::PathTracer pt;                                   // ren
-    pt.seed = std::strtoull(argv[5], nullptr, 10);
-    pt.max_depth = std::atoi(argv[6]);
     xyzgpu::ImageFilm film;
     int passes = 0;
     std::string const out = argv[2];
-    int const spp = pt.run(scene, &film, std::atoi(argv[3]), std::atoi(argv[4]),
-                           [&](const xyzgpu::ImageFilm &f, int s) {
-                             ++passes;
-                             return f.Save(out, static_cast<float>(s));
-                           });
+    auto on_pass = [&](const xyzgpu::ImageFilm &f, int s) {
+      ++passes;
+      return f.Save(out, static_cast<float>(s));
+    };
+    int spp = 0;
+    if (guided) {
+      xyzgpu::GuidedPathTracer gpt;                          // ren, guided
+      gpt.seed = std::strtoull(argv[5], nullptr, 10);
+      gpt.max_depth = std::atoi(argv[6]);
+      spp = gpt.run(scene, &film, std::atoi(argv[3]), std::atoi(argv[4]), on_pass);
+    } else {
+      xyzgpu::PathTracer pt;                                 // ren
+      pt.seed = std::strtoull(argv[5], nullptr, 10);
+      pt.max_depth = std::atoi(argv[6]);
+      spp = pt.run(scene, &film, std::atoi(argv[3]), std::atoi(argv[4]), on_pass);
+    }
     double sum = 0.0;
     for (int i = 0; i < 3 * film.width() * film.height(); ++i) sum += film.data()[i];
     std::printf("passes %d spp %d sum %.9g\n", passes, spp, sum);

@@ -76,3 +76,37 @@ def test_cpp_path_tracer_equals_the_c_abi_render(tmp_path):
     inv = np.float32(1.0) / np.float32(12.0)
     # progressive passes add the same samples in the same order: identical film
     assert np.array_equal(read_pfm(out), (ref * inv).astype(np.float32))
+
+
+@pytest.mark.gpu
+def test_cpp_guided_path_tracer(tmp_path):
+    """GuidedPathTracer: the first quarter of the samples train the guide and
+    stay out of the film; the film holds the rest, rendered with the guide,
+    and its image agrees with the plain tracer's."""
+    import torch
+    from xyz_b200 import api, scenes
+    exe = _compile(tmp_path)
+    sd = scenes.cornell_box(pinhole=True)
+    d = tmp_path / "scene"
+    d.mkdir()
+    sd.positions.astype("<f4").tofile(d / "positions.f32")
+    sd.tris.astype("<i4").tofile(d / "triangles.i32")
+    sd.tri_mat.astype("<i4").tofile(d / "material.i32")
+    sd.albedo_xyz.astype("<f4").tofile(d / "albedo.f32")
+    sd.is_light.astype("<i4").tofile(d / "is_light.i32")
+    sd.light_power_xyz.astype("<f4").tofile(d / "power.f32")
+    c = sd.camera
+    np.array(list(c.eye) + list(c.at) + [c.film_size, c.focal_length, c.f_number, float(c.pinhole)],
+             "<f4").tofile(d / "camera.f32")
+    np.array([64, 48], "<i4").tofile(d / "dims.i32")
+    out = str(tmp_path / "guided.pfm")
+    r = subprocess.run([exe, str(d), out, "64", "16", "3", "8", "--guided"], check=True, capture_output=True,
+                       text=True)
+    assert "passes 3 spp 48" in r.stdout, r.stdout
+    img = read_pfm(out)
+    with api.Scene(sd) as s:
+        plain = s.render(sd.camera, 64, 48, 64, seed=9, max_depth=8)
+        torch.cuda.synchronize()
+        plain = plain.cpu().numpy() / 64
+    assert np.isfinite(img).all() and (img >= 0).all()
+    assert abs(img.mean() / plain.mean() - 1.0) < 0.05
