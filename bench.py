@@ -372,6 +372,7 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             while True:
                 torch.cuda.synchronize()
+                gpu_lead(5.0)
                 e0.record()
                 render_pass(p, film)
                 e1.record()
@@ -480,6 +481,15 @@ def guide_profile_case():
         print(json.dumps({"guide_profile_case": "ok", "film_sum": float(f.sum())}))
 
 
+def gpu_lead(ms: float = 100.0):
+    """Occupies the current stream for about `ms` (torch's spin kernel,
+    outside any timed region) so that the host can enqueue the timed work
+    behind it: a host thread descheduled while enqueueing then cannot leave
+    the GPU idle inside the timed region."""
+    import torch
+    torch.cuda._sleep(int(ms * 1e-3 * 1.9e9))
+
+
 def profiled_traffic():
     """DRAM bytes per traced ray of the trace kernel from the committed ncu
     summary (profiles/trace_queue_spheres1m.txt), if present."""
@@ -532,8 +542,10 @@ def run_gpu_arm(args, rank, world):
     t_wall = time.perf_counter()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    # the K steps are enqueued back to back with no host synchronisation in
-    # between, so the device time does not depend on host scheduling
+    # the K steps are enqueued back to back behind a lead kernel, with no
+    # host synchronisation in between, so the device time does not depend on
+    # host scheduling
+    gpu_lead()
     ev0.record()
     for k in range(args.steps):
         step(offset)
