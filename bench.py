@@ -444,7 +444,8 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
            "speedup": round(plain["seconds"] / guided["seconds"], 2),
            "guide": ginfo,
            "runs": {"plain_seconds": [r["seconds"] for r in plains],
-                    "guided_seconds": [r[0]["seconds"] for r in guideds]},
+                    "guided_seconds": [r[0]["seconds"] for r in guideds],
+                    "guided_spp": [r[0]["spp"] for r in guideds]},
            "reference": {"spp": ref_spp, "seconds": round(ref_s, 2), "own_relmse": round(ref_noise, 5),
                          "tracer": "plain GPU path tracer, float64 sums"},
            "config": f"occluded room, 196,146 triangles, 1024x1024 camera, rows {rows[0]}-{rows[1]}, max depth 10, "

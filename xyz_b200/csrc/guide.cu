@@ -74,6 +74,12 @@ struct WeightsSmem {
   uint8_t ones[kRows * kBiasK * 2];
   uint8_t bias[kLayers][kW * kBiasK * 2];
 };
+// The same image lives in global memory (GuideImpl::d_wblk), rebuilt by
+// k_guide_pack after every weight update; each CTA copies it as is.
+constexpr uint32_t kOnesOff = kWBlkBytes;
+constexpr uint32_t kBiasOff = kOnesOff + kRows * kBiasK * 2;
+constexpr uint32_t kWImageBytes = kBiasOff + kLayers * kW * kBiasK * 2;  // 71680
+static_assert(sizeof(WeightsSmem) == kWImageBytes && kWImageBytes % 16 == 0, "weight image layout");
 
 // TMEM columns: [0, 64) the working accumulator; weight gradients (M = 64
 // layout: rows 16w..16w+15 in lanes 32w..32w+15) of layer 0 at [64, 256),
@@ -92,7 +98,7 @@ struct __align__(128) GuideSmem {
 };
 
 struct GuideDev {
-  const uint8_t *wblk;  // blocked bf16 weights
+  const uint8_t *wblk;  // packed weight image (WeightsSmem layout)
   const float *params;  // fp32 master (biases read from here)
   float lo[3], inv_ext[3];  // position normalisation: s = (p - lo) * inv_ext
   int *err;
@@ -320,25 +326,13 @@ __device__ void loss_grad(const float *o, const float w[3], float scale, float *
 }
 
 // ------------------------------------------------------------- kernels
+// Copies the packed weight image (weights, ones tile, bias tiles) into shared
+// memory: 4,480 independent 16-byte loads, several in flight per thread.
 __device__ void load_weights(WeightsSmem &wt, const GuideDev &G) {
   const uint4 *src = reinterpret_cast<const uint4 *>(G.wblk);
-  uint4 *dst = reinterpret_cast<uint4 *>(wt.w);
-  for (int i = threadIdx.x; i < static_cast<int>(kWBlkBytes / 16); i += blockDim.x) dst[i] = src[i];
-  for (int i = threadIdx.x; i < kRows * kBiasK; i += blockDim.x) {
-    int const r = i / kBiasK, c = i % kBiasK;
-    *reinterpret_cast<__nv_bfloat16 *>(wt.ones + tc::blocked_offset(r, c, kBiasK)) =
-        __float2bfloat16_rn(c < 3 ? 1.0f : 0.0f);
-  }
-  for (int i = threadIdx.x; i < kLayers * kW * kBiasK; i += blockDim.x) {
-    int const l = i / (kW * kBiasK), n = (i / kBiasK) % kW, c = i % kBiasK;
-    float const b = G.params[param_b(l) + n];
-    __nv_bfloat16 const hi = __float2bfloat16_rn(b);
-    float const r1 = b - __bfloat162float(hi);
-    __nv_bfloat16 const mid = __float2bfloat16_rn(r1);
-    __nv_bfloat16 const lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
-    __nv_bfloat16 const v = c == 0 ? hi : c == 1 ? mid : c == 2 ? lo : __float2bfloat16_rn(0.0f);
-    *reinterpret_cast<__nv_bfloat16 *>(wt.bias[l] + tc::blocked_offset(n, c, kBiasK)) = v;
-  }
+  uint4 *dst = reinterpret_cast<uint4 *>(&wt);
+#pragma unroll 4
+  for (int i = threadIdx.x; i < static_cast<int>(kWImageBytes / 16); i += blockDim.x) dst[i] = __ldg(&src[i]);
 }
 
 // mbarriers (count 1) and `ncols` TMEM columns for the CTA.
@@ -707,19 +701,43 @@ __global__ void k_guide_records(const float *__restrict__ rec, int tb, int64_t n
   }
 }
 
-// fp32 master weights -> blocked bf16 W^T per layer.
+// fp32 master parameters -> the weight image: blocked bf16 W^T per layer, the
+// ones tile (128 x 16, columns 0..2 = 1) and per layer the bias tile (64 x 16,
+// columns 0..2 = the bias's hi, mid and lo bf16 parts, whose sum is the fp32
+// bias to within fp32 rounding).  One thread per image element.
+constexpr int kPackWeights = kParams - kLayers * kW;
+constexpr int kPackOnes = kRows * kBiasK;
+constexpr int kPackBias = kLayers * kW * kBiasK;
+constexpr int kPackThreads = kPackWeights + kPackOnes + kPackBias;
+
 __global__ void k_guide_pack(const float *__restrict__ params, uint8_t *__restrict__ wblk) {
   int const i = blockIdx.x * blockDim.x + threadIdx.x;
-  int l = 0, rem = i;
-  while (l < kLayers && rem >= layer_in(l) * kW) {
-    rem -= layer_in(l) * kW;
-    ++l;
+  if (i < kPackWeights) {
+    int l = 0, rem = i;
+    while (l < kLayers && rem >= layer_in(l) * kW) {
+      rem -= layer_in(l) * kW;
+      ++l;
+    }
+    int const K = layer_in(l);
+    int const k = rem / kW, nn = rem % kW;  // W_l[k][nn]
+    __nv_bfloat16 const b = __float2bfloat16_rn(params[param_w(l) + k * kW + nn]);
+    *reinterpret_cast<__nv_bfloat16 *>(wblk + wblk_off(l) + tc::blocked_offset(nn, k, K)) = b;
+  } else if (i < kPackWeights + kPackOnes) {
+    int const j = i - kPackWeights;
+    int const r = j / kBiasK, c = j % kBiasK;
+    *reinterpret_cast<__nv_bfloat16 *>(wblk + kOnesOff + tc::blocked_offset(r, c, kBiasK)) =
+        __float2bfloat16_rn(c < 3 ? 1.0f : 0.0f);
+  } else if (i < kPackThreads) {
+    int const j = i - kPackWeights - kPackOnes;
+    int const l = j / (kW * kBiasK), n = (j / kBiasK) % kW, c = j % kBiasK;
+    float const b = params[param_b(l) + n];
+    __nv_bfloat16 const hi = __float2bfloat16_rn(b);
+    float const r1 = b - __bfloat162float(hi);
+    __nv_bfloat16 const mid = __float2bfloat16_rn(r1);
+    __nv_bfloat16 const lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
+    __nv_bfloat16 const v = c == 0 ? hi : c == 1 ? mid : c == 2 ? lo : __float2bfloat16_rn(0.0f);
+    *reinterpret_cast<__nv_bfloat16 *>(wblk + kBiasOff + l * (kW * kBiasK * 2) + tc::blocked_offset(n, c, kBiasK)) = v;
   }
-  if (l >= kLayers) return;
-  int const K = layer_in(l);
-  int const k = rem / kW, nn = rem % kW;  // W_l[k][nn]
-  __nv_bfloat16 const b = __float2bfloat16_rn(params[param_w(l) + k * kW + nn]);
-  *reinterpret_cast<__nv_bfloat16 *>(wblk + wblk_off(l) + tc::blocked_offset(nn, k, K)) = b;
 }
 
 __global__ void k_guide_adam(float *__restrict__ p, float *__restrict__ g, float *__restrict__ m,
@@ -772,8 +790,7 @@ GuideDev guide_dev(const GuideImpl &g) {
 }
 
 int pack(GuideImpl &g, cudaStream_t st) {
-  int const nw = kParams - kLayers * kW;
-  k_guide_pack<<<(nw + 255) / 256, 256, 0, st>>>(g.d_params, g.d_wblk);
+  k_guide_pack<<<(kPackThreads + 255) / 256, 256, 0, st>>>(g.d_params, g.d_wblk);
   XYZ_CUDA_TRY(cudaGetLastError());
   return XYZGPU_OK;
 }
@@ -996,7 +1013,7 @@ int xyzgpu_guide_create(xyzgpu_scene scene, const xyzgpu_guide_config *cfg, xyzg
       cudaMalloc(reinterpret_cast<void **>(&g.d_grad), kParams * sizeof(float)) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void **>(&g.d_m), kParams * sizeof(float)) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void **>(&g.d_v), kParams * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(reinterpret_cast<void **>(&g.d_wblk), kWBlkBytes) != cudaSuccess ||
+      cudaMalloc(reinterpret_cast<void **>(&g.d_wblk), kWImageBytes) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void **>(&g.d_err), sizeof(int)) != cudaSuccess)
     return fail(set_error(XYZGPU_E_NOMEM, "guide_create: device allocation failed"));
   // He-uniform hidden layers, a small output layer (near-uniform mixture at
