@@ -82,9 +82,10 @@ struct __align__(8) StackEntry {
 //   Sink::scene(i)                    (kBatch) the scene of ray i; rays of one
 //                                     queue may belong to different scenes
 constexpr int kRefillIdle = 12;
-// A round descends at most this many nodes; a lane still above its next leaf
-// resumes there in the next round, so the warp's leaf tests do not wait for
-// its longest descent (counting renders descend without the cap).
+// One iteration of the persistent loop descends at most this many nodes; a lane
+// still above its next leaf resumes there in the next iteration, so the warp's
+// leaf tests do not wait for its longest descent (counting renders descend
+// without the cap).
 #ifndef XYZ_DESCEND_STEPS
 #define XYZ_DESCEND_STEPS 8
 #endif
@@ -188,7 +189,7 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
       nd = __ldg(&nodes[node]);
       if (kCount) tc.nodes++;
     }
-    if ((nd.y & 3u) != kKdLeafTag) continue;  // resumes at `node` next round
+    if ((nd.y & 3u) != kKdLeafTag) continue;  // resumes at `node` in the next iteration
     // test the leaf
     uint32_t const cnt = nd.y >> 2;
     if (kCount) {
