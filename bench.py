@@ -307,6 +307,27 @@ def batch_bench(steps: int, warmup: int):
 GUIDE_CAMERA = ((0.0, 1.5, 1.2), (0.0, 1.1, -2.0), 60.0)
 
 
+def relmse_estimator(half_a, half_b):
+    """relMSE on Y against a reference given as two independent half
+    estimates A and B (arrays of Y, numpy or torch): the reference is
+    R = (A + B) / 2, the image is exposed so that mean(R) = 1, and
+    relMSE(I) = mean((I - R)^2 / (R^2 + 1e-2)) - mean(Var(R) / (R^2 + 1e-2)) with
+    Var(R) = (A - B)^2 / 4, which removes the reference's own noise from the
+    measured error (for an image I independent of A and B the result is an
+    unbiased estimate of mean(Var(I) / (R^2 + 1e-2))).  Returns (relmse, the
+    subtracted noise term, the exposure scale); relmse takes the image's Y."""
+    ref_y = (half_a + half_b) / 2
+    scale = 1.0 / float(ref_y.mean())
+    ry = ref_y * scale
+    den = ry ** 2 + 1e-2
+    ref_noise = float((((half_a - half_b) * scale) ** 2 / 4 / den).mean())
+
+    def relmse(img_y):
+        return float((((img_y * scale - ry) ** 2) / den).mean()) - ref_noise
+
+    return relmse, ref_noise, scale
+
+
 GUIDE_SETTINGS = dict(train_bounces=5, guide_bounces=9, alpha=0.5, steps_per_pass=512, batch_size=16384)
 # forward flops of one guide query, 2 (192 * 64 + 3 * 64 * 64 + 64 * 40)
 GUIDE_QUERY_FLOPS = 2 * (192 * 64 + 3 * 64 * 64 + 64 * 40)
@@ -356,14 +377,10 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
         torch.cuda.synchronize()
         ref_s = time.perf_counter() - t0
         a, b = (h[..., 1] / (ref_spp // 2) for h in halves)
-        ref_y = (a + b) / 2
-        scale = 1.0 / float(ref_y.mean())
-        ry = ref_y * scale
-        den = ry ** 2 + 1e-2
-        ref_noise = float((((a - b) * scale) ** 2 / 4 / den).mean())
+        relmse_y, ref_noise, _ = relmse_estimator(a, b)
 
         def relmse(img):
-            return float((((img[..., 1] * scale - ry) ** 2) / den).mean()) - ref_noise
+            return relmse_y(img[..., 1])
 
         def run(render_pass, train_passes=0):
             acc = torch.zeros((band, W, 3), dtype=torch.float64, device="cuda")
