@@ -4,8 +4,9 @@
 // order, --fmad=false; integer histograms and scans are order independent).
 //
 // Per level (m nodes, R references, each node's references contiguous):
-//   classify   nodes with >= kBigRefs references are listed for one CTA each;
-//              the rest get one warp each
+//   classify   nodes with >= kBigRefs references are listed ("big"): one CTA
+//              each decides, up to 128 CTAs each (slices) emit; the rest get
+//              one warp each
 //   decide     binned start/end histograms per axis in shared memory
 //              (shared-memory atomics), exclusive prefix per axis, SAH cost of
 //              every candidate plane, arg-min with the host's tie-break
@@ -13,8 +14,9 @@
 //   scan       exclusive scan over nodes of (split, leaf refs, next refs,
 //              empty leaf) -> child pair index, leaf offset, child ref offset
 //   emit       node words, next-level node bounds and ranges, and a stable
-//              scatter of references into the children (ballot / block scans
-//              keep the parent's order) or into the leaf reference array
+//              scatter of references into the children (ballot / block scans,
+//              and per-slice counts for big nodes, keep the parent's order) or
+//              into the leaf reference array
 // The host reads two small values per level (the big-node count and the scan
 // totals) to size the next level; everything else stays on the device.
 //
@@ -36,6 +38,8 @@ namespace {
 
 constexpr int kBigRefs = 2048;
 constexpr int kBigThreads = 256;
+constexpr int kBigSlicesMax = 128;     // CTAs per big node when emitting
+constexpr int kBigSliceBudget = 1024;  // CTAs per emit launch (about)
 constexpr int kWarpsPerBlock = 4;
 constexpr int kScanThreads = 256;
 constexpr int kScanPerThread = 8;
@@ -526,36 +530,102 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_emit_small(EmitArgs E, 
   }
 }
 
+// Big nodes are emitted by `slices` CTAs each: CTA g of a node takes the g-th
+// contiguous slice of its references.  A counting pass records each slice's
+// left and right counts; the scatter pass starts each slice after the counts
+// of the node's earlier slices and keeps the order within the slice, so the
+// children receive the parent's references in the parent's order, as from a
+// single CTA.
+__device__ __forceinline__ void big_slice(int n, int slices, int g, int *b, int *e) {
+  int const s = (n + slices - 1) / slices;
+  *b = min(n, g * s);
+  *e = min(n, *b + s);
+}
+
 __global__ void __launch_bounds__(kBigThreads)
-    k_emit_big(EmitArgs E, const int32_t *__restrict__ big_list) {
+    k_emit_big_count(EmitArgs E, const int32_t *__restrict__ big_list, int slices, int2 *__restrict__ cnt) {
+  __shared__ int s_red[2][kBigThreads / 32];
+  int const j = big_list[blockIdx.x / slices], g = blockIdx.x % slices;
+  int const axis = E.L.axis[j];
+  if (axis < 0) return;  // leaf: its references are copied, not counted
+  int const n = E.L.count[j], rb = E.L.begin[j];
+  float const plane = E.L.plane[j];
+  int b, e;
+  big_slice(n, slices, g, &b, &e);
+  int const tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  int cl = 0, cr = 0;
+  for (int r = b + tid; r < e; r += kBigThreads) {
+    bool l = false, rr = false;
+    classify_ref(E.R.lo[axis][rb + r], E.R.hi[axis][rb + r], plane, &l, &rr);
+    cl += l;
+    cr += rr;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    cl += __shfl_down_sync(0xffffffffu, cl, o);
+    cr += __shfl_down_sync(0xffffffffu, cr, o);
+  }
+  if (lane == 0) {
+    s_red[0][w] = cl;
+    s_red[1][w] = cr;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int tl = 0, tr = 0;
+    for (int k = 0; k < kBigThreads / 32; ++k) {
+      tl += s_red[0][k];
+      tr += s_red[1][k];
+    }
+    cnt[blockIdx.x] = make_int2(tl, tr);
+  }
+}
+
+__global__ void __launch_bounds__(kBigThreads)
+    k_emit_big(EmitArgs E, const int32_t *__restrict__ big_list, int slices, const int2 *__restrict__ cnt) {
   __shared__ int s_warp[2][kBigThreads / 32];
   __shared__ int s_run[2];
-  int const j = big_list[blockIdx.x];
+  int const first = (blockIdx.x / slices) * slices, g = blockIdx.x - first;
+  int const j = big_list[blockIdx.x / slices];
   int const n = E.L.count[j];
   int const axis = E.L.axis[j];
   int const rb = E.L.begin[j];
   int const tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  int b, e;
+  big_slice(n, slices, g, &b, &e);
   if (axis < 0) {
     uint4 const sc = E.L.scan[j];
     int64_t const off = E.leaf_base + sc.y;
-    if (tid == 0)
+    if (g == 0 && tid == 0)
       E.nodes[E.level_base + j] = make_uint2(static_cast<uint32_t>(off),
                                              (static_cast<uint32_t>(n) << 2) | kKdLeafTag);
-    for (int r = tid; r < n; r += kBigThreads) E.leaf_refs[off + r] = E.R.tri[rb + r];
+    for (int r = b + tid; r < e; r += kBigThreads) E.leaf_refs[off + r] = E.R.tri[rb + r];
     return;
   }
   float const plane = E.L.plane[j];
-  if (tid == 0) {
-    write_split_node(E, j, axis, plane);
-    s_run[0] = s_run[1] = 0;
+  if (g == 0 && tid == 0) write_split_node(E, j, axis, plane);
+  if (w == 0) {
+    // references of the node's earlier slices
+    int pl = 0, pr = 0;
+    for (int k = lane; k < g; k += 32) {
+      int2 const c = cnt[first + k];
+      pl += c.x;
+      pr += c.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      pl += __shfl_down_sync(0xffffffffu, pl, o);
+      pr += __shfl_down_sync(0xffffffffu, pr, o);
+    }
+    if (lane == 0) {
+      s_run[0] = pl;
+      s_run[1] = pr;
+    }
   }
   __syncthreads();
   int const lbase = static_cast<int>(E.L.scan[j].z);
   int const rbase = lbase + E.L.nl[j];
-  for (int r0 = 0; r0 < n; r0 += kBigThreads) {
+  for (int r0 = b; r0 < e; r0 += kBigThreads) {
     int const r = r0 + tid;
     bool l = false, rr = false;
-    if (r < n) classify_ref(E.R.lo[axis][rb + r], E.R.hi[axis][rb + r], plane, &l, &rr);
+    if (r < e) classify_ref(E.R.lo[axis][rb + r], E.R.hi[axis][rb + r], plane, &l, &rr);
     unsigned const ml = __ballot_sync(0xffffffffu, l);
     unsigned const mr = __ballot_sync(0xffffffffu, rr);
     if (lane == 0) {
@@ -744,6 +814,7 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
   DevBuf<uint2> nodes;
   DevBuf<int32_t> leaf_refs;
   DevBuf<int32_t> big_list, small_i32;
+  DevBuf<int2> big_cnt;
   DevBuf<uint4> block_sums, grand;
   for (int q = 0; q < 2; ++q) {
     refs[q].tri.st = st;
@@ -756,6 +827,7 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
   nodes.st = st;
   leaf_refs.st = st;
   big_list.st = small_i32.st = st;
+  big_cnt.st = st;
   block_sums.st = grand.st = st;
   XYZ_BUILD_TRY(refs[0].reserve(std::max(1, n)));
   XYZ_BUILD_TRY(lv[0].reserve(1));
@@ -829,7 +901,13 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
     E.leaf_base = leaf_total;
     E.m = m;
     k_emit_small<<<grid_for(int64_t{m} * 32, 32 * kWarpsPerBlock, dev), 32 * kWarpsPerBlock, 0, st>>>(E, A);
-    if (n_big > 0) k_emit_big<<<n_big, kBigThreads, 0, st>>>(E, big_list.p);
+    if (n_big > 0) {
+      // slices per big node: up to 128, about 1,024 CTAs per launch in all
+      int const slices = std::max(1, std::min(kBigSlicesMax, kBigSliceBudget / n_big));
+      XYZ_BUILD_TRY(big_cnt.reserve(int64_t{n_big} * slices));
+      k_emit_big_count<<<n_big * slices, kBigThreads, 0, st>>>(E, big_list.p, slices, big_cnt.p);
+      k_emit_big<<<n_big * slices, kBigThreads, 0, st>>>(E, big_list.p, slices, big_cnt.p);
+    }
     XYZ_BUILD_TRY(cudaGetLastError());
     leaves += m - splits;
     empty += tot.w;
