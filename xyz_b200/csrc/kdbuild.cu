@@ -4,9 +4,10 @@
 // order, --fmad=false; integer histograms and scans are order independent).
 //
 // Per level (m nodes, R references, each node's references contiguous):
-//   classify   nodes with >= kBigRefs references are listed ("big"): one CTA
-//              each decides, up to 128 CTAs each (slices) emit; the rest get
-//              one warp each
+//   classify   nodes with >= kBigRefs references are listed ("big"): their
+//              histograms, left / right counts and emit run on up to 128 CTAs
+//              each (slices of the references), the SAH decision on one CTA
+//              each; the rest get one warp each
 //   decide     binned start/end histograms per axis in shared memory
 //              (shared-memory atomics), exclusive prefix per axis, SAH cost of
 //              every candidate plane, arg-min with the host's tie-break
@@ -243,12 +244,58 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock)
 }
 
 // ---- decide: one CTA per big node
+// Big nodes use `slices` CTAs each for their O(n) passes; CTA g of a node
+// takes the g-th contiguous slice of its references.
+__device__ __forceinline__ void big_slice(int n, int slices, int g, int *b, int *e) {
+  int const s = (n + slices - 1) / slices;
+  *b = min(n, g * s);
+  *e = min(n, *b + s);
+}
+
+constexpr int kHistWords = 3 * 2 * (kKdMaxBins + 1);
+
+// Start / end bin histograms of a big node, one slice per CTA, added into the
+// node's histogram in global memory (integer counts: the sum does not depend
+// on the order of the slices).
+__global__ void __launch_bounds__(kBigThreads) k_decide_big_hist(LevelArrays L, const int32_t *__restrict__ big_list,
+                                                                 RefArrays R, BuildArgs A, int slices,
+                                                                 uint32_t *__restrict__ gh) {
+  __shared__ uint32_t h[kHistWords];
+  int const ib = blockIdx.x / slices, g = blockIdx.x % slices;
+  int const j = big_list[ib];
+  int const n = L.count[j];
+  int const B = A.bins;
+  int const tid = threadIdx.x;
+  float4 const lo4 = L.blo[j], hi4 = L.bhi[j];
+  float const ext[3] = {hi4.x - lo4.x, hi4.y - lo4.y, hi4.z - lo4.z};
+  if (!(half_area3(ext[0], ext[1], ext[2]) > 0.0f)) return;  // k_decide_big makes it a leaf
+  for (int t = tid; t < kHistWords; t += kBigThreads) h[t] = 0u;
+  __syncthreads();
+  int b, e;
+  big_slice(n, slices, g, &b, &e);
+  int const rb = L.begin[j];
+  for (int a = 0; a < 3; ++a) {
+    if (!(ext[a] > 0.0f)) continue;
+    float const scale = static_cast<float>(B) / ext[a];
+    float const lo = comp4(lo4, a);
+    for (int r = b + tid; r < e; r += kBigThreads) {
+      int const b0 = bin_of(R.lo[a][rb + r], lo, scale, B);
+      int const b1 = bin_of(R.hi[a][rb + r], lo, scale, B);
+      atomicAdd(&h[(a * 2 + 0) * (kKdMaxBins + 1) + b0], 1u);
+      atomicAdd(&h[(a * 2 + 1) * (kKdMaxBins + 1) + b1], 1u);
+    }
+  }
+  __syncthreads();
+  for (int t = tid; t < kHistWords; t += kBigThreads)
+    if (h[t]) atomicAdd(&gh[static_cast<int64_t>(ib) * kHistWords + t], h[t]);
+}
+
 __global__ void __launch_bounds__(kBigThreads)
-    k_decide_big(LevelArrays L, const int32_t *__restrict__ big_list, RefArrays R, BuildArgs A) {
-  __shared__ uint32_t h[3 * 2 * (kKdMaxBins + 1)];
+    k_decide_big(LevelArrays L, const int32_t *__restrict__ big_list, BuildArgs A,
+                 const uint32_t *__restrict__ gh) {
+  __shared__ uint32_t h[kHistWords];
   __shared__ float s_cost[kBigThreads / 32];
   __shared__ int s_idx[kBigThreads / 32];
-  __shared__ int s_cnt[2];
   int const j = big_list[blockIdx.x];
   int const n = L.count[j];
   int const B = A.bins;
@@ -263,21 +310,8 @@ __global__ void __launch_bounds__(kBigThreads)
     }
     return;
   }
-  for (int t = tid; t < 3 * 2 * (kKdMaxBins + 1); t += kBigThreads) h[t] = 0u;
-  if (tid < 2) s_cnt[tid] = 0;
-  __syncthreads();
-  int const rb = L.begin[j];
-  for (int a = 0; a < 3; ++a) {
-    if (!(ext[a] > 0.0f)) continue;
-    float const scale = static_cast<float>(B) / ext[a];
-    float const lo = comp4(lo4, a);
-    for (int r = tid; r < n; r += kBigThreads) {
-      int const b0 = bin_of(R.lo[a][rb + r], lo, scale, B);
-      int const b1 = bin_of(R.hi[a][rb + r], lo, scale, B);
-      atomicAdd(&h[(a * 2 + 0) * (kKdMaxBins + 1) + b0], 1u);
-      atomicAdd(&h[(a * 2 + 1) * (kKdMaxBins + 1) + b1], 1u);
-    }
-  }
+  // the node's histograms, summed over its slices by k_decide_big_hist
+  for (int t = tid; t < kHistWords; t += kBigThreads) h[t] = gh[static_cast<int64_t>(blockIdx.x) * kHistWords + t];
   __syncthreads();
   if (tid < 6) {
     uint32_t *row = h + tid * (kKdMaxBins + 1);
@@ -334,30 +368,10 @@ __global__ void __launch_bounds__(kBigThreads)
     candidate_cost(A, h, best_c, n, ext, lo4, hi4, sa, &plane, &nl_bin);
     axis = best_c / (B - 1);
   }
-  if (axis >= 0) {
-    int nl = 0, nr = 0;
-    for (int r = tid; r < n; r += kBigThreads) {
-      bool l, rr;
-      classify_ref(R.lo[axis][rb + r], R.hi[axis][rb + r], plane, &l, &rr);
-      nl += l;
-      nr += rr;
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      nl += __shfl_xor_sync(0xffffffffu, nl, off);
-      nr += __shfl_xor_sync(0xffffffffu, nr, off);
-    }
-    if ((tid & 31) == 0) {
-      atomicAdd(&s_cnt[0], nl);
-      atomicAdd(&s_cnt[1], nr);
-    }
-    __syncthreads();
-  }
+  // exact left / right counts: k_emit_big_count per slice, k_big_totals per node
   if (tid == 0) {
     L.axis[j] = axis;
     L.plane[j] = plane;
-    L.nl[j] = axis >= 0 ? s_cnt[0] : 0;
-    L.nr[j] = axis >= 0 ? s_cnt[1] : 0;
   }
 }
 
@@ -536,27 +550,23 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_emit_small(EmitArgs E, 
 // of the node's earlier slices and keeps the order within the slice, so the
 // children receive the parent's references in the parent's order, as from a
 // single CTA.
-__device__ __forceinline__ void big_slice(int n, int slices, int g, int *b, int *e) {
-  int const s = (n + slices - 1) / slices;
-  *b = min(n, g * s);
-  *e = min(n, *b + s);
-}
 
 __global__ void __launch_bounds__(kBigThreads)
-    k_emit_big_count(EmitArgs E, const int32_t *__restrict__ big_list, int slices, int2 *__restrict__ cnt) {
+    k_emit_big_count(LevelArrays L, RefArrays R, const int32_t *__restrict__ big_list, int slices,
+                     int2 *__restrict__ cnt) {
   __shared__ int s_red[2][kBigThreads / 32];
   int const j = big_list[blockIdx.x / slices], g = blockIdx.x % slices;
-  int const axis = E.L.axis[j];
+  int const axis = L.axis[j];
   if (axis < 0) return;  // leaf: its references are copied, not counted
-  int const n = E.L.count[j], rb = E.L.begin[j];
-  float const plane = E.L.plane[j];
+  int const n = L.count[j], rb = L.begin[j];
+  float const plane = L.plane[j];
   int b, e;
   big_slice(n, slices, g, &b, &e);
   int const tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   int cl = 0, cr = 0;
   for (int r = b + tid; r < e; r += kBigThreads) {
     bool l = false, rr = false;
-    classify_ref(E.R.lo[axis][rb + r], E.R.hi[axis][rb + r], plane, &l, &rr);
+    classify_ref(R.lo[axis][rb + r], R.hi[axis][rb + r], plane, &l, &rr);
     cl += l;
     cr += rr;
   }
@@ -576,6 +586,29 @@ __global__ void __launch_bounds__(kBigThreads)
       tr += s_red[1][k];
     }
     cnt[blockIdx.x] = make_int2(tl, tr);
+  }
+}
+
+// A big node's exact left / right reference counts: the sum of its slices'.
+__global__ void k_big_totals(LevelArrays L, const int32_t *__restrict__ big_list, int slices,
+                             const int2 *__restrict__ cnt) {
+  int const j = big_list[blockIdx.x];
+  int const lane = threadIdx.x;
+  bool const split = L.axis[j] >= 0;
+  int nl = 0, nr = 0;
+  if (split)
+    for (int k = lane; k < slices; k += 32) {
+      int2 const c = cnt[blockIdx.x * slices + k];
+      nl += c.x;
+      nr += c.y;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    nl += __shfl_down_sync(0xffffffffu, nl, o);
+    nr += __shfl_down_sync(0xffffffffu, nr, o);
+  }
+  if (lane == 0) {
+    L.nl[j] = split ? nl : 0;
+    L.nr[j] = split ? nr : 0;
   }
 }
 
@@ -815,6 +848,7 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
   DevBuf<int32_t> leaf_refs;
   DevBuf<int32_t> big_list, small_i32;
   DevBuf<int2> big_cnt;
+  DevBuf<uint32_t> big_hist;
   DevBuf<uint4> block_sums, grand;
   for (int q = 0; q < 2; ++q) {
     refs[q].tri.st = st;
@@ -827,7 +861,7 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
   nodes.st = st;
   leaf_refs.st = st;
   big_list.st = small_i32.st = st;
-  big_cnt.st = st;
+  big_cnt.st = big_hist.st = st;
   block_sums.st = grand.st = st;
   XYZ_BUILD_TRY(refs[0].reserve(std::max(1, n)));
   XYZ_BUILD_TRY(lv[0].reserve(1));
@@ -864,7 +898,19 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
     XYZ_BUILD_TRY(cudaStreamSynchronize(st));
     RefArrays const R = refs[cur].view();
     k_decide_small<<<grid_for(int64_t{m} * 32, 32 * kWarpsPerBlock, dev), 32 * kWarpsPerBlock, 0, st>>>(L, m, R, A);
-    if (n_big > 0) k_decide_big<<<n_big, kBigThreads, 0, st>>>(L, big_list.p, R, A);
+    // big nodes: sliced histograms, one CTA per node for the decision, sliced
+    // left / right counts (kept for the emit) and their per-node totals;
+    // slices per node: up to 128, about 1,024 CTAs per launch in all
+    int const slices = n_big > 0 ? std::max(1, std::min(kBigSlicesMax, kBigSliceBudget / n_big)) : 1;
+    if (n_big > 0) {
+      XYZ_BUILD_TRY(big_hist.reserve(int64_t{n_big} * kHistWords));
+      XYZ_BUILD_TRY(big_cnt.reserve(int64_t{n_big} * slices));
+      XYZ_BUILD_TRY(cudaMemsetAsync(big_hist.p, 0, sizeof(uint32_t) * n_big * kHistWords, st));
+      k_decide_big_hist<<<n_big * slices, kBigThreads, 0, st>>>(L, big_list.p, R, A, slices, big_hist.p);
+      k_decide_big<<<n_big, kBigThreads, 0, st>>>(L, big_list.p, A, big_hist.p);
+      k_emit_big_count<<<n_big * slices, kBigThreads, 0, st>>>(L, R, big_list.p, slices, big_cnt.p);
+      k_big_totals<<<n_big, 32, 0, st>>>(L, big_list.p, slices, big_cnt.p);
+    }
     XYZ_BUILD_TRY(cudaGetLastError());
     // flags + scan (twice if the reference budget is exceeded)
     uint4 tot = make_uint4(0, 0, 0, 0);
@@ -901,13 +947,7 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
     E.leaf_base = leaf_total;
     E.m = m;
     k_emit_small<<<grid_for(int64_t{m} * 32, 32 * kWarpsPerBlock, dev), 32 * kWarpsPerBlock, 0, st>>>(E, A);
-    if (n_big > 0) {
-      // slices per big node: up to 128, about 1,024 CTAs per launch in all
-      int const slices = std::max(1, std::min(kBigSlicesMax, kBigSliceBudget / n_big));
-      XYZ_BUILD_TRY(big_cnt.reserve(int64_t{n_big} * slices));
-      k_emit_big_count<<<n_big * slices, kBigThreads, 0, st>>>(E, big_list.p, slices, big_cnt.p);
-      k_emit_big<<<n_big * slices, kBigThreads, 0, st>>>(E, big_list.p, slices, big_cnt.p);
-    }
+    if (n_big > 0) k_emit_big<<<n_big * slices, kBigThreads, 0, st>>>(E, big_list.p, slices, big_cnt.p);
     XYZ_BUILD_TRY(cudaGetLastError());
     leaves += m - splits;
     empty += tot.w;
