@@ -119,6 +119,8 @@ def reference_lib():
     """The reference's own renderer built from its sources (oracle/_ref), else
     the C restatement (oracle/_port)."""
     from oracle import refbind
+    if refbind.fast_ref_available():
+        return refbind.RefLib(pinhole=True, fast=True), "reference"
     if refbind.ref_available(pinhole=True):
         return refbind.RefLib(pinhole=True), "reference"
     if not refbind.port_available():
@@ -165,6 +167,7 @@ def cpu_baseline(sd, target_s=12.0):
     rows, spp = cpu_plan(lib, threads, target_s)
     v, dt = cpu_sample(lib, threads, rows, spp, 0)
     return {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": kind,
+            "build": getattr(lib, "build", "-O2"),
             "sample": f"{spp} spp over {rows} of 1024 rows (centre band) of the same scene and "
                       f"camera, {rows * W_PIX * spp} paths in {dt:.1f} s; tree build {build_s:.1f} s untimed"}
 
@@ -191,6 +194,7 @@ def run_reference_arm(args, rank):
         "data": "synthetic (seeded scene generator)", "config": workload_config(),
         "impl": "reference",
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": kind,
+                         "build": getattr(lib, "build", "-O2"),
                          "sample": f"each step: {spp} spp over {rows} of 1024 rows (centre band), "
                                    f"{rows * W_PIX * spp} paths; tree build {build_s:.1f} s untimed"},
         "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -40,6 +40,27 @@ def _ref_path(pinhole: bool) -> str:
     return os.path.join(REF_DIR, "libxyzref_pinhole.so" if pinhole else "libxyzref_thinlens.so")
 
 
+FAST_REF_PATH = os.path.join(REF_DIR, "libxyzref_pinhole_o3.so")
+
+
+def host_has_x86_64_v3() -> bool:
+    """True when this host's CPU runs x86-64-v3 code (AVX2, FMA, BMI2), which
+    the -O3 timing build of the reference (libxyzref_pinhole_o3.so) needs."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    fl = set(line.split(":", 1)[1].split())
+                    return {"avx2", "fma", "bmi2", "movbe"} <= fl
+    except OSError:
+        pass
+    return False
+
+
+def fast_ref_available() -> bool:
+    return os.path.exists(FAST_REF_PATH) and host_has_x86_64_v3()
+
+
 def port_available() -> bool:
     return os.path.exists(os.path.join(PORT_DIR, "libxyzport.so"))
 
@@ -103,8 +124,12 @@ class _Common:
 class RefLib(_Common):
     prefix = "xyzref_"
 
-    def __init__(self, pinhole: bool = True):
-        path = _ref_path(pinhole)
+    def __init__(self, pinhole: bool = True, fast: bool = False):
+        """fast: the -O3 x86-64-v3 timing build (pinhole only; same IEEE
+        arithmetic as the parity build)."""
+        if fast and not pinhole:
+            raise ValueError("the timing build of the reference is the pinhole one")
+        path = FAST_REF_PATH if fast else _ref_path(pinhole)
         if not os.path.exists(path):
             raise FileNotFoundError(f"reference oracle not built: {path} (run make -C oracle)")
         self.lib = C.CDLL(path)
@@ -123,6 +148,7 @@ class RefLib(_Common):
         L.xyzref_max_threads.restype = C.c_int
         self.pinhole = bool(L.xyzref_is_pinhole())
         self.kind = "reference"
+        self.build = "-O3 -march=x86-64-v3" if fast else "-O2"
 
     def _set_path(self, kmax, rr_threshold, rr_start):
         if rr_start != 1:

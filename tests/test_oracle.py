@@ -84,3 +84,22 @@ def test_port_options_rr_start_changes_only_when_enabled():
     assert not np.array_equal(a, b)
     # unbiased either way: means agree loosely
     assert abs(a.mean() - b.mean()) / a.mean() < 0.15
+
+
+def test_reference_timing_build_renders_the_parity_build_film():
+    """The -O3 x86-64-v3 build that the CPU baseline times keeps IEEE
+    arithmetic without contraction, so it renders bit for bit what the parity
+    build renders (same work, same branches)."""
+    from oracle import refbind
+    if not (refbind.ref_available(True) and refbind.fast_ref_available()):
+        pytest.skip("reference timing build not built or CPU without x86-64-v3")
+    from xyz_b200 import scenes
+    slow, fast = refbind.RefLib(pinhole=True), refbind.RefLib(pinhole=True, fast=True)
+    sd = scenes.spheres_scene(level=2, n_spheres=3, seed=4)
+    films = []
+    for L in (slow, fast):
+        L.scene_create(sd)
+        L.set_camera(sd.camera, 40, 30)
+        L.set_path_params(max_depth=10)
+        films.append(L.render(3, seed=5, nthreads=2))
+    assert np.array_equal(films[0], films[1])

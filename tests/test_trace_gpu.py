@@ -94,9 +94,39 @@ def test_tree_structure_invariants(builder):
     assert parents[0] == 0 and (parents[1:] == 1).all()
 
 
-def test_device_tree_equals_host_tree():
+def _triangle_soup(n, seed):
+    """n random small triangles in a unit box: one flat root node of n
+    references (n = 2,050 is just above a multiple of the builder's 128 slices,
+    so a big node's last slices hold one reference or none)."""
     from xyz_b200 import scenes
-    sd = scenes.spheres_scene(level=4, n_spheres=3, seed=2)
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-1.0, 1.0, (n, 1, 3))
+    pos = (c + rng.normal(scale=0.05, size=(n, 3, 3))).reshape(-1, 3).astype(np.float32)
+    tris = np.arange(3 * n, dtype=np.int32).reshape(n, 3)
+    mat = np.zeros(n, np.int32)
+    mat[:2] = 1
+    sd = scenes.SceneData(pos, tris, mat, np.array([[0.5] * 3, [0.0] * 3], np.float32),
+                          np.array([0, 1], np.int32), np.ones(3, np.float32))
+    return sd
+
+
+@pytest.mark.parametrize("case", ["spheres-l4x3", "spheres-l6x4", "soup-2050", "soup-4099",
+                                  "spheres-1M"])
+def test_device_tree_equals_host_tree(case):
+    """The device builder (sliced histograms and counts for big nodes) builds
+    the host builder's tree exactly: on a 15k-triangle mesh; on 328k
+    triangles, whose upper levels hold many big nodes sharing the slices; on
+    flat soups whose root has 2,050 / 4,099 references (empty and one-element
+    trailing slices); and on the 984,322-triangle benchmark scene."""
+    from xyz_b200 import scenes
+    if case == "spheres-l4x3":
+        sd = scenes.spheres_scene(level=4, n_spheres=3, seed=2)
+    elif case == "spheres-l6x4":
+        sd = scenes.spheres_scene(level=6, n_spheres=4, seed=5)
+    elif case.startswith("soup"):
+        sd = _triangle_soup(int(case.split("-")[1]), seed=3)
+    else:
+        sd = scenes.spheres_scene(level=7, n_spheres=3, seed=0)
     with _scene(sd, "host") as a, _scene(sd, "device") as b:
         na, ra = a.tree()
         nb, rb = b.tree()

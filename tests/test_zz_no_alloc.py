@@ -9,6 +9,16 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+def _render_pair(s, c):
+    import torch
+    ref = s.render(c["cam"], c["W"], c["H"], c["spp"], seed=c["seed"], max_depth=c["depth"])
+    film = torch.full((c["H"], c["W"], 3), float("nan"), device="cuda")
+    s.render_noalloc(c["cam"], c["W"], c["H"], c["spp"], film, seed=c["seed"],
+                     max_depth=c["depth"], wave_paths=c.get("wave_paths", 0))
+    torch.cuda.synchronize()
+    return film, ref
+
+
 def test_noalloc_render_equals_render_on_two_calls_in_a_row():
     import torch
     from xyz_b200 import api, scenes
@@ -20,13 +30,27 @@ def test_noalloc_render_equals_render_on_two_calls_in_a_row():
              dict(cam=thin, W=40, H=30, spp=2, seed=9, depth=6)]
     with api.Scene(sd) as s:
         for c in cases:
-            ref = s.render(c["cam"], c["W"], c["H"], c["spp"], seed=c["seed"], max_depth=c["depth"])
-            film = torch.full((c["H"], c["W"], 3), float("nan"), device="cuda")
-            s.render_noalloc(c["cam"], c["W"], c["H"], c["spp"], film, seed=c["seed"],
-                             max_depth=c["depth"])
-            torch.cuda.synchronize()
+            film, ref = _render_pair(s, c)
             # per-path results do not depend on the wave size: identical films
             assert torch.equal(film, ref)
+
+
+def test_noalloc_render_splits_pixels_and_samples_over_waves():
+    """Calls larger than one wave of the fixed array: the image is cut into
+    runs of pixels (more pixels than a wave holds), into runs of samples (few
+    pixels, many samples), or both (a small explicit wave size); every film
+    equals xyzgpu_render's, and a second call in a row still does."""
+    import torch
+    from xyz_b200 import api, scenes
+    sd = scenes.cornell_box(pinhole=True)
+    cases = [dict(cam=sd.camera, W=320, H=240, spp=1, seed=5, depth=8),     # 76,800 pixels: 2 pixel runs
+             dict(cam=sd.camera, W=64, H=64, spp=40, seed=6, depth=8),      # 16 + 16 + 8 samples
+             dict(cam=sd.camera, W=64, H=48, spp=6, seed=7, depth=8, wave_paths=1000),  # 4 x 6 waves
+             dict(cam=sd.camera, W=64, H=48, spp=6, seed=7, depth=8, wave_paths=1000)]
+    with api.Scene(sd) as s:
+        for c in cases:
+            film, ref = _render_pair(s, c)
+            assert torch.equal(film, ref), c
 
 
 def test_noalloc_render_rejects_sizes_beyond_its_limits():

@@ -947,6 +947,13 @@ int kd_build_device(SceneImpl &s, const float4 *d_tri, int n, const BuildConfig 
     E.leaf_base = leaf_total;
     E.m = m;
     k_emit_small<<<grid_for(int64_t{m} * 32, 32 * kWarpsPerBlock, dev), 32 * kWarpsPerBlock, 0, st>>>(E, A);
+    // big_cnt was written by k_emit_big_count at decision time, before the
+    // flag / scan passes, and holds valid per-slice counts only for nodes that
+    // decided to split (axis >= 0); leaves never have theirs written.  The
+    // second k_flags pass (reference budget exceeded) only turns nodes into
+    // leaves (axis = -1), and k_emit_big takes its leaf branch for those
+    // without reading cnt, so the counts stay valid for every node that reads
+    // them here.
     if (n_big > 0) k_emit_big<<<n_big * slices, kBigThreads, 0, st>>>(E, big_list.p, slices, big_cnt.p);
     XYZ_BUILD_TRY(cudaGetLastError());
     leaves += m - splits;

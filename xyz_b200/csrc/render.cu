@@ -11,6 +11,40 @@ namespace xyzgpu {
 namespace {
 constexpr int64_t kMaxDefaultWave = int64_t{1} << 26;
 constexpr int64_t kMaxGuidedWave = int64_t{1} << 23;
+
+// Grids of one full wave of resident CTAs per kernel variant on a device (the
+// grid-stride loops give every CTA an equal share, so a grid larger than what
+// fits at once would run a second, tail wave).  Sized once per device and
+// published under a mutex only when complete, so threads rendering on several
+// devices never see a partly filled entry or another device's grids.
+struct Grids {
+  int raygen, trace_e, trace_s, trace_s_adj, trace_s_guide;
+  int shade, shade_adj, shade_guide, shade_sp, film;
+};
+
+Grids wave_grids(int device) {
+  static std::mutex mu;
+  static Grids table[64];
+  static bool ready[64] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  int const d = device & 63;
+  if (!ready[d]) {
+    Grids g;
+    g.raygen = occupancy_grid(k_raygen<false>, device);
+    g.trace_e = occupancy_grid(k_trace_queue<false, false>, device);
+    g.trace_s = occupancy_grid(k_trace_queue<true, false>, device);
+    g.trace_s_adj = occupancy_grid(k_trace_queue<true, false, kModeAdjoint>, device);
+    g.trace_s_guide = occupancy_grid(k_trace_queue<true, false, kModeGuided>, device);
+    g.shade = occupancy_grid(k_shade<kModePlain>, device);
+    g.shade_adj = occupancy_grid(k_shade<kModeAdjoint>, device);
+    g.shade_guide = occupancy_grid(k_shade<kModeGuided>, device);
+    g.shade_sp = occupancy_grid(k_shade_spectral, device);
+    g.film = occupancy_grid(k_film, device);
+    table[d] = g;
+    ready[d] = true;
+  }
+  return table[d];
+}
 }  // namespace
 
 extern const int64_t kBytesPerPath = 3 * sizeof(float4) + sizeof(uint32_t) +  // beta, radiance, hits, misc
@@ -172,23 +206,7 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
     }
   } ltot_guard{ltot, st};
 
-  // Grids of one full wave of resident CTAs per kernel variant (the
-  // grid-stride loops give every CTA an equal share, so a grid larger than
-  // what fits at once would run a second, tail wave).
-  static int g_raygen = 0, g_trace_e = 0, g_trace_s = 0, g_shade = 0, g_film = 0, g_shade_sp = 0;
-  static int g_shade_adj = 0, g_shade_guide = 0, g_trace_s_adj = 0, g_trace_s_guide = 0;
-  if (!g_raygen) {
-    g_raygen = occupancy_grid(k_raygen<false>, s.device);
-    g_trace_e = occupancy_grid(k_trace_queue<false, false>, s.device);
-    g_trace_s = occupancy_grid(k_trace_queue<true, false>, s.device);
-    g_trace_s_adj = occupancy_grid(k_trace_queue<true, false, kModeAdjoint>, s.device);
-    g_trace_s_guide = occupancy_grid(k_trace_queue<true, false, kModeGuided>, s.device);
-    g_shade = occupancy_grid(k_shade<kModePlain>, s.device);
-    g_shade_adj = occupancy_grid(k_shade<kModeAdjoint>, s.device);
-    g_shade_guide = occupancy_grid(k_shade<kModeGuided>, s.device);
-    g_shade_sp = occupancy_grid(k_shade_spectral, s.device);
-    g_film = occupancy_grid(k_film, s.device);
-  }
+  Grids const G = wave_grids(s.device);
   int const prof = rp.profile;
   bool const spectral = rp.spectral != XYZGPU_SPECTRAL_OFF;
   bool const timing = prof == XYZGPU_PROFILE_TIMING;
@@ -272,7 +290,7 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       XYZ_CUDA_TRY(cudaMemsetAsync(wv.counts, 0, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t), st));
       if (A.train_bounces > 0)
         XYZ_CUDA_TRY(cudaMemsetAsync(A.records, 0, static_cast<size_t>(A.npaths) * A.train_bounces * 16 * sizeof(float), st));
-      int const gr = static_cast<int>(std::min<int64_t>(g_raygen, (A.npaths + kThreads - 1) / kThreads));
+      int const gr = static_cast<int>(std::min<int64_t>(G.raygen, (A.npaths + kThreads - 1) / kThreads));
 #define XYZ_MARK(cls, start)              \
   do {                                    \
     int const m_ = mark((cls), (start));  \
@@ -288,9 +306,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
         for (int b = 0; b < iters; ++b) {
           XYZ_MARK(1, true);
           if (counting)
-            k_trace_queue<false, true><<<g_trace_e, kThreads, 0, st>>>(A, b, pc);
+            k_trace_queue<false, true><<<G.trace_e, kThreads, 0, st>>>(A, b, pc);
           else
-            k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, pc);
+            k_trace_queue<false, false><<<G.trace_e, kThreads, 0, st>>>(A, b, pc);
           XYZ_MARK(1, false);
           // (the last bounce only meets the depth cap: no sampling, no inference;
           // beyond guide_bounces the guided kernels sample Lambert alone)
@@ -307,23 +325,23 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
           }
           XYZ_MARK(2, true);
           if (spectral)
-            k_shade_spectral<<<g_shade_sp, kThreads, 0, st>>>(A, b);
+            k_shade_spectral<<<G.shade_sp, kThreads, 0, st>>>(A, b);
           else if (guide)
-            k_shade<kModeGuided><<<g_shade_guide, kThreads, 0, st>>>(A, b);
+            k_shade<kModeGuided><<<G.shade_guide, kThreads, 0, st>>>(A, b);
           else if (replay)
-            k_shade<kModeAdjoint><<<g_shade_adj, kThreads, 0, st>>>(A, b);
+            k_shade<kModeAdjoint><<<G.shade_adj, kThreads, 0, st>>>(A, b);
           else
-            k_shade<kModePlain><<<g_shade, kThreads, 0, st>>>(A, b);
+            k_shade<kModePlain><<<G.shade, kThreads, 0, st>>>(A, b);
           XYZ_MARK(2, false);
           XYZ_MARK(3, true);
           if (counting)
-            k_trace_queue<true, true><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
+            k_trace_queue<true, true><<<G.trace_s, kThreads, 0, st>>>(A, b, pc);
           else if (replay)
-            k_trace_queue<true, false, kModeAdjoint><<<g_trace_s_adj, kThreads, 0, st>>>(A, b, pc);
+            k_trace_queue<true, false, kModeAdjoint><<<G.trace_s_adj, kThreads, 0, st>>>(A, b, pc);
           else if (guide)
-            k_trace_queue<true, false, kModeGuided><<<g_trace_s_guide, kThreads, 0, st>>>(A, b, pc);
+            k_trace_queue<true, false, kModeGuided><<<G.trace_s_guide, kThreads, 0, st>>>(A, b, pc);
           else
-            k_trace_queue<true, false><<<g_trace_s, kThreads, 0, st>>>(A, b, pc);
+            k_trace_queue<true, false><<<G.trace_s, kThreads, 0, st>>>(A, b, pc);
           XYZ_MARK(3, false);
           launches += 3;
         }
@@ -331,9 +349,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       };
       int const pr = pass(false);
       if (pr) return pr;
-      int const gf = static_cast<int>(std::min<int64_t>(g_film, (A.npix + kThreads - 1) / kThreads));
+      int const gf = static_cast<int>(std::min<int64_t>(G.film, (A.npix + kThreads - 1) / kThreads));
       if (adj) {
-        int const gs = static_cast<int>(std::min<int64_t>(g_film, (A.npaths + kThreads - 1) / kThreads));
+        int const gs = static_cast<int>(std::min<int64_t>(G.film, (A.npaths + kThreads - 1) / kThreads));
         k_adj_stash<<<gs, kThreads, 0, st>>>(A);
         ++launches;
         XYZ_CUDA_TRY(cudaMemsetAsync(wv.counts, 0, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t), st));
@@ -463,23 +481,38 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 namespace {
 
 std::mutex g_noalloc_mu;
-void *g_noalloc_base[64] = {nullptr};
 
-// Device address of g_noalloc_scratch on `device` (which must be current).
-// The first call on a device looks the symbol up; later calls reuse it.
-int noalloc_scratch(int device, unsigned char **out) {
+// Per device: the array's device address and the launch grids of the five
+// kernels (occupancy x SM count of that device).  An entry is published, under
+// g_noalloc_mu, only once all of its fields are set.
+struct NoAllocDevice {
+  unsigned char *base;
+  int raygen, trace_e, trace_s, shade, film;
+};
+NoAllocDevice g_noalloc_dev[64] = {};
+
+// Set-up of `device` (which must be current): the first call on a device looks
+// the symbol up and sizes the grids; later calls reuse them.
+int noalloc_device(int device, NoAllocDevice *out) {
   if (device < 0 || device >= 64)
     return set_error(XYZGPU_E_LIMIT, "render_noalloc: device ordinal %d is beyond 63", device);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_base[device]) {
+  if (!g_noalloc_dev[device].base) {
     void *p = nullptr;
     cudaError_t const e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr)
       return set_error(XYZGPU_E_CUDA, "render_noalloc: cudaGetSymbolAddress failed: %s",
                        cudaGetErrorString(e));
-    g_noalloc_base[device] = p;
+    NoAllocDevice d;
+    d.raygen = occupancy_grid(k_raygen<false>, device);
+    d.trace_e = occupancy_grid(k_trace_queue<false, false>, device);
+    d.trace_s = occupancy_grid(k_trace_queue<true, false>, device);
+    d.shade = occupancy_grid(k_shade<kModePlain>, device);
+    d.film = occupancy_grid(k_film, device);
+    d.base = static_cast<unsigned char *>(p);
+    g_noalloc_dev[device] = d;
   }
-  *out = static_cast<unsigned char *>(g_noalloc_base[device]);
+  *out = g_noalloc_dev[device];
   return XYZGPU_OK;
 }
 
@@ -500,9 +533,10 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
     return set_error(XYZGPU_E_LIMIT, "render_noalloc: max_depth %d exceeds the maximum of %d",
                      rp.max_depth, kNoAllocDepth);
   XYZ_CUDA_TRY(cudaSetDevice(s.device));
-  unsigned char *base = nullptr;
-  int rc = noalloc_scratch(s.device, &base);
+  NoAllocDevice dev;
+  int rc = noalloc_device(s.device, &dev);
   if (rc) return rc;
+  unsigned char *const base = dev.base;
 
   WaveArgs A;
   std::memset(&A, 0, sizeof(A));
@@ -537,14 +571,6 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
   A.rr_threshold = rp.rr_threshold;
   A.seed = rp.seed;
 
-  static int g_raygen = 0, g_trace_e = 0, g_trace_s = 0, g_shade = 0, g_film = 0;
-  if (!g_raygen) {
-    g_raygen = occupancy_grid(k_raygen<false>, s.device);
-    g_trace_e = occupancy_grid(k_trace_queue<false, false>, s.device);
-    g_trace_s = occupancy_grid(k_trace_queue<true, false>, s.device);
-    g_shade = occupancy_grid(k_shade<kModePlain>, s.device);
-    g_film = occupancy_grid(k_film, s.device);
-  }
   int64_t const npix_total = static_cast<int64_t>(rp.width) * rp.height;
   int64_t const cap = rp.wave_paths > 0 ? rp.wave_paths : kNoAllocPaths;
   int const iters = rp.max_depth;
@@ -563,14 +589,14 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
       A.npaths = A.npix * ns;
       // queue lengths and work counters from the previous wave or call
       XYZ_CUDA_TRY(cudaMemsetAsync(A.counts, 0, kNoAllocCounts, st));
-      int const gr = static_cast<int>(std::min<int64_t>(g_raygen, (A.npaths + kThreads - 1) / kThreads));
+      int const gr = static_cast<int>(std::min<int64_t>(dev.raygen, (A.npaths + kThreads - 1) / kThreads));
       k_raygen<false><<<gr, kThreads, 0, st>>>(A);
       for (int b = 0; b < iters; ++b) {
-        k_trace_queue<false, false><<<g_trace_e, kThreads, 0, st>>>(A, b, tally + 8);
-        k_shade<kModePlain><<<g_shade, kThreads, 0, st>>>(A, b);
-        k_trace_queue<true, false><<<g_trace_s, kThreads, 0, st>>>(A, b, tally + 8);
+        k_trace_queue<false, false><<<dev.trace_e, kThreads, 0, st>>>(A, b, tally + 8);
+        k_shade<kModePlain><<<dev.shade, kThreads, 0, st>>>(A, b);
+        k_trace_queue<true, false><<<dev.trace_s, kThreads, 0, st>>>(A, b, tally + 8);
       }
-      int const gf = static_cast<int>(std::min<int64_t>(g_film, (A.npix + kThreads - 1) / kThreads));
+      int const gf = static_cast<int>(std::min<int64_t>(dev.film, (A.npix + kThreads - 1) / kThreads));
       k_film<<<gf, kThreads, 0, st>>>(A, film);
       XYZ_CUDA_TRY(cudaGetLastError());
     }
