@@ -341,19 +341,22 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
                 max_seconds: float = 30.0, guide_cfg=None, variants=(), repeats: int = 2):
     """Time to relative MSE 0.01, guided vs plain, on the indirect-lit room
     (196,146 triangles; light only through a 0.1 m gap), 1024 x 1024 camera,
-    max depth 10, Russian roulette 0.2.  The error is measured on a band of
-    `band` image rows through the image centre (both tracers render that band),
-    against a `ref_spp` plain render of the band (float64 accumulation),
+    max depth 10, Russian roulette 0.2.  The error is measured on `band` image
+    rows spread evenly over the frame (rows 16, 48, ..., 1008 for 32: every
+    32nd row; both tracers render exactly those rows of the full image, the
+    same pixels and paths as a full render), against a `ref_spp` plain render
+    of those rows (float64 accumulation),
     relMSE = mean((Y - Y_ref)^2 / (Y_ref^2 + 1e-2)) with the image exposed so
-    that the band's mean reference Y is 1, minus the reference's own share of
+    that the rows' mean reference Y is 1, minus the reference's own share of
     that error (estimated from the difference of its two independent halves
     A and B: var(Y_ref) = E[(A - B)^2] / 4).  Both tracers render passes of
     `pass_spp` until the error reaches 0.01; each pass is timed with CUDA
     events around the render call (the error evaluation is not timed).  The
-    reported time is robust to host-side launch stalls of the shared machine:
-    the number of passes times the median pass time (training and rendering
-    passes of the guided tracer separately); the plain sum of the pass times
-    is reported beside it.  The guided tracer trains during the first 25 % of
+    reported time is the sum of the pass times (the guided tracer's training
+    passes included); passes x median pass time is reported beside it.  Each
+    tracer's buffers are allocated before its first timed pass (the guide's by
+    xyzgpu_guide_reserve, as the plain tracer's wave buffers are by the
+    untimed warm-up).  The guided tracer trains during the first 25 % of
     a planned `plan_spp` (Adam steps after every training pass); as in path
     guiding practice the training passes' samples, drawn while the guide is
     still immature, are left out of the image, but their time counts.  Plain
@@ -365,7 +368,9 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
     import torch
     from xyz_b200 import api, scenes
     W = H = 1024
-    rows = (H // 2 - band // 2, H // 2 + band // 2)
+    step = H // band
+    rows = (step // 2, H, step)
+    row_list = list(range(*rows))
     depth = 10
     sd = scenes.occluded_room()
     cam = scenes.Camera.with_fov(*GUIDE_CAMERA, pinhole=True)
@@ -377,7 +382,7 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
         t0 = time.perf_counter()
         for k in range(0, ref_spp, chunk):
             f = s.render(cam, W, H, chunk, seed=99, spp_offset=k, max_depth=depth, rows=rows)
-            halves[(k // chunk) & 1] += f[rows[0]:rows[1]].double()
+            halves[(k // chunk) & 1] += f[row_list].double()
         torch.cuda.synchronize()
         ref_s = time.perf_counter() - t0
         a, b = (h[..., 1] / (ref_spp // 2) for h in halves)
@@ -402,18 +407,20 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
                 p += 1
                 if p <= train_passes:
                     continue
-                acc += film[rows[0]:rows[1]].double()
+                acc += film[row_list].double()
                 e = relmse(acc / ((p - train_passes) * pass_spp))
                 tr, rd = times[:train_passes], times[train_passes:]
                 robust = len(tr) * (statistics.median(tr) if tr else 0.0) + len(rd) * (statistics.median(rd) if rd else 0.0)
+                total = sum(times)
                 out = {"spp": p * pass_spp, "image_spp": (p - train_passes) * pass_spp, "relmse": round(e, 5),
-                       "passes": p,
+                       "passes": p, "training_passes": train_passes,
+                       "training_seconds": round(sum(tr), 4),
                        "median_pass_ms": round(statistics.median(rd if rd else tr) * 1e3, 3),
-                       "sum_of_pass_seconds": round(sum(times), 3)}
+                       "passes_times_median_seconds": round(robust, 3)}
                 if e <= 0.01:
-                    return {"seconds": round(robust, 3), "reached": True} | out
-                if sum(times) > max_seconds:
-                    return {"seconds": round(robust * e / 0.01, 3), "reached": False} | out
+                    return {"seconds": round(total, 3), "reached": True} | out
+                if total > max_seconds:
+                    return {"seconds": round(total * e / 0.01, 3), "reached": False} | out
 
         def plain_pass(p, film):
             s.render(cam, W, H, pass_spp, seed=1, spp_offset=p * pass_spp, max_depth=depth, film=film, rows=rows)
@@ -421,11 +428,14 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
         # untimed warm-up of both tracers (module loading, first-use allocations)
         s.render(cam, W, H, pass_spp, seed=7, max_depth=depth, rows=rows)
         with api.Guide(s, **cfg) as g0:
+            g0.reserve(W * band * pass_spp, train=True)
             g0.render(cam, W, H, pass_spp, seed=7, max_depth=depth, rows=rows, train=True)
         torch.cuda.synchronize()
         def guided_run(gcfg, gplan):
             train_passes = max(1, (gplan // 4) // pass_spp)
             with api.Guide(s, **gcfg) as g:
+                g.reserve(W * band * pass_spp, train=True)
+
                 def guided_pass(p, film):
                     g.render(cam, W, H, pass_spp, seed=1, spp_offset=p * pass_spp, max_depth=depth, film=film,
                              rows=rows, train=p < train_passes)
@@ -469,8 +479,10 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
                     "guided_spp": [r[0]["spp"] for r in guideds]},
            "reference": {"spp": ref_spp, "seconds": round(ref_s, 2), "own_relmse": round(ref_noise, 5),
                          "tracer": "plain GPU path tracer, float64 sums"},
-           "config": f"occluded room, 196,146 triangles, 1024x1024 camera, rows {rows[0]}-{rows[1]}, max depth 10, "
-                     f"Russian roulette 0.2, passes of {pass_spp} spp, exposure: band mean Y = 1"}
+           "time": "sum of the CUDA-event times of every pass (training passes included)",
+           "config": f"occluded room, 196,146 triangles, 1024x1024 camera, {band} rows spread over the frame "
+                     f"(rows {rows[0]}, {rows[0] + rows[2]}, ..., {row_list[-1]}), max depth 10, "
+                     f"Russian roulette 0.2, passes of {pass_spp} spp, exposure: mean reference Y = 1"}
     if more:
         out["variants"] = more
     return out

@@ -170,6 +170,9 @@ typedef struct {
   int hero_wavelengths;    /* 1..4 wavelengths per path in the spectral modes */
   int row_begin, row_end;  /* render only image rows [row_begin, row_end) (a band of the same
                               image: same pixels, same paths); 0, 0 = all rows */
+  int row_step;            /* with a band: render only rows row_begin + k * row_step (0 or 1:
+                              every row of the band); rows not rendered hold zero (or keep
+                              their values when accumulating), as outside a band */
 } xyzgpu_render_params;
 
 /* Film modes.  OFF: throughput and albedo are CIE XYZ triples, the estimator of
@@ -414,19 +417,103 @@ int xyzgpu_guide_train_step(xyzgpu_guide guide, const float *records, int n, voi
  * (a mixture per queue entry), shading and shadow rays.  train != 0: the first
  * train_bounces vertices of every path also leave training records (point,
  * sampled direction, incident-radiance weight), and after each wave the guide
- * takes steps_per_pass Adam steps on them (synchronises `stream`).  Russian
+ * takes steps_per_pass Adam steps on them.  Russian
  * roulette tests the throughput the path would have with Lambert sampling (the
  * throughput times the product of the guide / Lambert density ratios): the
  * guide sends paths towards bright regions with a high pdf, i.e. a low
- * throughput, which roulette on the throughput itself would end. */
+ * throughput, which roulette on the throughput itself would end.  A training
+ * wave's records, Adam steps and bookkeeping run on the device as one CUDA
+ * graph (captured on a private stream the first time a wave of that size
+ * trains), so training enqueues no host synchronisation. */
 int xyzgpu_render_guided(xyzgpu_guide guide, const xyzgpu_camera *camera,
                          const xyzgpu_render_params *rp, int train, float *film, void *stream);
+
+/* Allocates the guided-wave buffers now - the mixtures (80 B per path) and,
+ * with train, the training records and rows (520 B per path at 5 training
+ * bounces) - for waves of up to wave_paths paths (at most 2^23, the guided
+ * wave size), so that xyzgpu_render_guided calls whose waves fit allocate
+ * nothing (else the first such call allocates them).  No counterpart in the
+ * reference.  Synchronises `stream`. */
+int xyzgpu_guide_reserve(xyzgpu_guide guide, int64_t wave_paths, int train, void *stream);
 
 typedef struct {
   uint64_t adam_steps, trained_records;
 } xyzgpu_guide_stats;
 
 int xyzgpu_guide_stats_get(xyzgpu_guide guide, xyzgpu_guide_stats *out);
+
+/* ---- Film output.  Post-processing on the device of a film as xyzgpu_render
+ * leaves it (W * H XYZ sums, row 0 at the bottom, device memory), and the
+ * files around it. */
+
+/* Radiance RGBE pixels of ImageFilm::SaveAsHdr (xyz/core/imagefilm_hdr.cpp:
+ * 124-183): pixel = film * scale (scale = 1 / spp), converted to CCIR 601-1 RGB
+ * (a non-finite pixel becomes 0) and encoded as hdr_encode does (:14-31);
+ * out: W * H * 4 bytes (device) in file order, scanlines from the top image
+ * row down.  xyze != 0: the reference's CONFIG_HDR_STRICT output, XYZ encoded
+ * directly, scanlines from the bottom row up. */
+int xyzgpu_film_encode_rgbe(const float *film, int width, int height, float scale, int xyze, uint8_t *out,
+                            void *stream);
+
+/* Writes a Radiance .hdr file (header and run-length scanlines, the format of
+ * imagefilm_hdr.cpp:46-183) from the host copy of xyzgpu_film_encode_rgbe's
+ * output. */
+int xyzgpu_hdr_write(const char *path, const uint8_t *rgbe, int width, int height, int xyze);
+
+/* Tone operators of the reference's float2bmp tool (float2bmp/main.cpp:80-118)
+ * applied per channel: FILM 1 - exp(-exposure L) (the one the tool uses),
+ * LINEAR exposure L, REINHARD exposure L / (1 + L), REINHARD_WHITE
+ * exposure L (1 + L / white^2) / (1 + L); then L^(src_gamma / dst_gamma) and
+ * the 8-bit quantisation min(255, floor(256 v)) for v in (0, 1). */
+#define XYZGPU_TONEMAP_FILM 0
+#define XYZGPU_TONEMAP_LINEAR 1
+#define XYZGPU_TONEMAP_REINHARD 2
+#define XYZGPU_TONEMAP_REINHARD_WHITE 3
+typedef struct {
+  float scale;       /* film multiplier (1 / spp) */
+  int op;            /* XYZGPU_TONEMAP_* */
+  float exposure;    /* (1, the tool's default) */
+  float white;       /* REINHARD_WHITE: white point; <= 0: the image's maximum of
+                        0.6069 c0 + 0.1735 c1 + 0.2003 c2, as the tool computes it */
+  float dst_gamma;   /* 2.2 */
+  float src_gamma;   /* 1.0 */
+  int rgb;           /* 0: the film's channels as they are (the tool reads the
+                        reference's .pfm, which holds XYZ); 1: CCIR 601-1 RGB */
+} xyzgpu_tonemap_params;
+
+void xyzgpu_tonemap_params_default(xyzgpu_tonemap_params *tp);
+
+/* 24-bit BMP pixel rows (device): rows from the bottom, bytes blue, green, red
+ * = tone-mapped channels 2, 1, 0 (the tool's order), each row padded to a
+ * multiple of 4 bytes.  scratch_white: one device word, needed only for
+ * REINHARD_WHITE with white <= 0. */
+int xyzgpu_film_tonemap(const float *film, int width, int height, const xyzgpu_tonemap_params *tp, uint8_t *out,
+                        unsigned int *scratch_white, void *stream);
+
+/* Writes a 24-bit BMP file (the header of float2bmp/main.cpp:131-144) from the
+ * host copy of xyzgpu_film_tonemap's output. */
+int xyzgpu_bmp_write(const char *path, const uint8_t *bgr, int width, int height);
+
+/* Host-film forms: the film (host, W * H * 3 sums) is uploaded, encoded or
+ * tone-mapped by the kernels above and written (synchronous; allocates device
+ * memory for the call).  save_hdr is the reference's ImageFilm::SaveAsHdr with
+ * mpp = spp; save_bmp is float2bmp applied to the film. */
+int xyzgpu_film_save_hdr(const char *path, const float *film, int width, int height, float spp, int xyze);
+int xyzgpu_film_save_bmp(const char *path, const float *film, int width, int height,
+                         const xyzgpu_tonemap_params *tp);
+
+/* Resumable render checkpoint (no counterpart in the reference, whose periodic
+ * .pfm dump, xyz/integrator/integrator.cpp:140-160, keeps the image but not
+ * the means to continue it): the film sums (host memory, W * H * 3 floats),
+ * the number of samples per pixel done and the render parameters, with a
+ * checksum of the film.  To resume, load, then render with
+ * spp_offset = spp_done and accumulate = 1 into the loaded film: the film
+ * kernels add each path's sample into the pixel in sample order, so the
+ * resumed film is bit-identical to an uninterrupted render.  The file is
+ * written under a temporary name and renamed, so a crash never leaves a
+ * half-written checkpoint.  load with film = NULL reads only the header. */
+int xyzgpu_checkpoint_save(const char *path, const xyzgpu_render_params *rp, int spp_done, const float *film);
+int xyzgpu_checkpoint_load(const char *path, xyzgpu_render_params *rp, int *spp_done, float *film);
 
 /* Host evaluation of the random stream defined above (for tests). */
 float xyzgpu_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim);

@@ -82,7 +82,10 @@ class ImageFilm {
 
   // ".pfm": raw XYZ / spp, non-finite pixels written as 0
   // (ImageFilm::SaveAsPfm, imagefilm.cpp:153-206); ".float": CCIR 601-1 RGB /
-  // spp with negatives clamped to 0 (ImageFilm::SaveAsFloat, :108-151).
+  // spp with negatives clamped to 0 (ImageFilm::SaveAsFloat, :108-151);
+  // ".hdr": Radiance RGBE (ImageFilm::SaveAsHdr, imagefilm_hdr.cpp:124-183,
+  // pixels encoded on the GPU); ".bmp": the float2bmp tool's film tone map of
+  // XYZ / spp (float2bmp/main.cpp, on the GPU).
   bool Save(const std::string &filename, float spp) const {
     auto ends = [&](const char *sfx) {
       size_t const n = std::char_traits<char>::length(sfx);
@@ -90,7 +93,25 @@ class ImageFilm {
     };
     if (ends(".pfm")) return SaveAsPfm(filename, spp);
     if (ends(".float")) return SaveAsFloat(filename, spp);
+    if (ends(".hdr")) return xyzgpu_film_save_hdr(filename.c_str(), m_.data(), w_, h_, spp, 0) == XYZGPU_OK;
+    if (ends(".bmp")) {
+      xyzgpu_tonemap_params tp;
+      xyzgpu_tonemap_params_default(&tp);
+      tp.scale = 1.0f / spp;
+      return xyzgpu_film_save_bmp(filename.c_str(), m_.data(), w_, h_, &tp) == XYZGPU_OK;
+    }
     return false;
+  }
+
+  // Resumable checkpoint: the sums, the samples done and the parameters that
+  // made them (xyzgpu_checkpoint_save / _load).
+  bool SaveCheckpoint(const std::string &filename, const xyzgpu_render_params &rp, int spp_done) const {
+    return xyzgpu_checkpoint_save(filename.c_str(), &rp, spp_done, m_.data()) == XYZGPU_OK;
+  }
+  bool LoadCheckpoint(const std::string &filename, xyzgpu_render_params *rp, int *spp_done) {
+    if (xyzgpu_checkpoint_load(filename.c_str(), rp, spp_done, nullptr) != XYZGPU_OK) return false;
+    Resize(rp->width, rp->height);
+    return xyzgpu_checkpoint_load(filename.c_str(), rp, spp_done, m_.data()) == XYZGPU_OK;
   }
 
  private:
@@ -192,10 +213,9 @@ class Scene {
     return st.light_area;
   }
 
-  // Scene::EvalutePathTracing for every pixel and `spp` samples starting at
-  // sample index `first_sample`, added to `film` (host memory).
-  void EvalutePathTracing(ImageFilm *film, int first_sample, int spp, uint64_t seed, int max_depth = 15,
-                          int rr_start_depth = 1, float rr_threshold = 0.2f) const {
+  // The render parameters of EvalutePathTracing's call (host film, added to).
+  xyzgpu_render_params Params(int first_sample, int spp, uint64_t seed, int max_depth = 15, int rr_start_depth = 1,
+                              float rr_threshold = 0.2f) const {
     xyzgpu_render_params rp;
     xyzgpu_render_params_default(&rp);
     rp.width = width_;
@@ -208,6 +228,14 @@ class Scene {
     rp.seed = seed;
     rp.film_location = XYZGPU_FILM_HOST;
     rp.accumulate = 1;
+    return rp;
+  }
+
+  // Scene::EvalutePathTracing for every pixel and `spp` samples starting at
+  // sample index `first_sample`, added to `film` (host memory).
+  void EvalutePathTracing(ImageFilm *film, int first_sample, int spp, uint64_t seed, int max_depth = 15,
+                          int rr_start_depth = 1, float rr_threshold = 0.2f) const {
+    xyzgpu_render_params const rp = Params(first_sample, spp, seed, max_depth, rr_start_depth, rr_threshold);
     if (film->width() != width_ || film->height() != height_) film->Resize(width_, height_);
     check(xyzgpu_render(handle(), &camera_.desc(), &rp, film->data(), nullptr));
   }
@@ -238,14 +266,38 @@ class PathTracer {
   float rr_threshold = 0.2f;
   uint64_t seed = 0;
 
+  // checkpoint: if not empty, the film, the samples done and the parameters
+  // are saved there after every pass (xyzgpu_checkpoint_save), and run()
+  // starts from that file when it exists and matches this render (same image
+  // size, seed, depth and roulette), so a stopped render continues where it
+  // stopped with the film it would have had.
+  std::string checkpoint;
+
   int run(const Scene &scene, ImageFilm *film, int total_spp, int interval,
           const std::function<bool(const ImageFilm &, int)> &on_pass = {}) const {
     film->Resize(scene.GetWidth(), scene.GetHeight());
     int done = 0;
+    if (!checkpoint.empty()) {
+      xyzgpu_render_params saved;
+      int saved_done = 0;
+      ImageFilm loaded;
+      xyzgpu_render_params const want = scene.Params(0, 0, seed, max_depth, rr_start_depth, rr_threshold);
+      if (loaded.LoadCheckpoint(checkpoint, &saved, &saved_done) && saved.width == want.width &&
+          saved.height == want.height && saved.seed == want.seed && saved.max_depth == want.max_depth &&
+          saved.rr_start_depth == want.rr_start_depth && saved.rr_threshold == want.rr_threshold &&
+          saved_done <= total_spp) {
+        *film = std::move(loaded);
+        done = saved_done;
+      }
+    }
     while (done < total_spp) {
       int const n = std::min(interval, total_spp - done);
       scene.EvalutePathTracing(film, done, n, seed, max_depth, rr_start_depth, rr_threshold);
       done += n;
+      if (!checkpoint.empty() &&
+          !film->SaveCheckpoint(checkpoint, scene.Params(0, done, seed, max_depth, rr_start_depth, rr_threshold),
+                                done))
+        throw Error(XYZGPU_E_INVALID, "PathTracer: cannot write checkpoint " + checkpoint);
       if (on_pass && !on_pass(*film, done)) break;
     }
     return done;

@@ -53,6 +53,8 @@
 #define _ftprintf_s fprintf
 #define _stprintf_s snprintf
 #define _tcscpy_s(d, n, s) std::strncpy((d), (s), (n))
+// MSVC CRT's _finite (xyz/core/imagefilm_hdr.cpp:165)
+inline int _finite(double x) { return std::isfinite(x) ? 1 : 0; }
 
 #define HI_TO_STRING(x) #x
 #define HI_ARRAYS_LENGTH(ary) (sizeof(ary) / sizeof(ary[0]))

@@ -34,6 +34,10 @@ class basic_vector4 {
   typedef T value_type;
   explicit basic_vector4(T a = T()) : v_{a, a, a, a} {}
   basic_vector4(T a, T b, T c, T d) : v_{a, b, c, d} {}
+  basic_vector4 &operator=(T a) {  // `dst = 0` of imagefilm_hdr.cpp:20
+    v_[0] = v_[1] = v_[2] = v_[3] = a;
+    return *this;
+  }
   T *data() { return v_; }
   T const *data() const { return v_; }
   T &operator[](std::size_t i) { return v_[i]; }

@@ -208,6 +208,9 @@ class PortLib(_Common):
         L.xyzo_scene_set_spectra.argtypes = [C.c_void_p, C.c_void_p]
         L.xyzo_set_spectral.argtypes = [C.c_int, C.c_int]
         L.xyzo_set_materials.argtypes = [C.c_void_p, C.c_void_p]
+        L.xyzo_encode_rgbe.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p]
+        L.xyzo_tonemap.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float,
+                                   C.c_float, C.c_float, C.c_int, C.c_void_p]
         L.xyzo_adjoint.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_int]
         self.kind = "port"
@@ -215,6 +218,27 @@ class PortLib(_Common):
 
     def _set_path(self, kmax, rr_threshold, rr_start):
         self.lib.xyzo_set_path_params(kmax, rr_threshold, rr_start)
+
+    def encode_rgbe(self, film, scale: float, xyze: bool = False):
+        """Pixels of the reference's .hdr writer, (H, W, 4) uint8 in file order."""
+        film = _f(film)
+        H, W = film.shape[:2]
+        out = np.zeros((H, W, 4), np.uint8)
+        self.lib.xyzo_encode_rgbe(film.ctypes.data_as(C.c_void_p), W, H, C.c_float(scale), int(xyze),
+                                  out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def tonemap(self, film, scale: float = 1.0, op: int = 0, exposure: float = 1.0, white: float = 0.0,
+                dst_gamma: float = 2.2, src_gamma: float = 1.0, rgb: bool = False):
+        """float2bmp's tone operators: BMP rows (H, stride) uint8, rows from the bottom."""
+        film = _f(film)
+        H, W = film.shape[:2]
+        stride = (3 * W + 3) & ~3
+        out = np.zeros((H, stride), np.uint8)
+        self.lib.xyzo_tonemap(film.ctypes.data_as(C.c_void_p), W, H, C.c_float(scale), op, C.c_float(exposure),
+                              C.c_float(white), C.c_float(dst_gamma), C.c_float(src_gamma), int(rgb),
+                              out.ctypes.data_as(C.c_void_p))
+        return out
 
     def set_camera(self, cam, width: int, height: int):
         eye = _f(cam.eye)
@@ -357,3 +381,26 @@ class TwinLib:
         film = np.zeros((self.height, self.width, 3), np.float32)
         self.lib.xyztwin_render(s0, spp, C.c_ulonglong(seed), film.ctypes.data_as(C.c_void_p), nthreads)
         return film
+
+
+FILM_REF_PATH = os.path.join(REF_DIR, "xyzref_hdr")
+
+
+def ref_film_available() -> bool:
+    return os.path.exists(FILM_REF_PATH)
+
+
+class RefFilmLib:
+    """The reference's Radiance writer, ImageFilm::SaveAsHdr, built from its
+    sources into the program oracle/_ref/xyzref_hdr (run in its own process)."""
+
+    def save_hdr(self, path: str, film, spp: float):
+        import subprocess
+        film = _f(film)
+        H, W = film.shape[:2]
+        raw = path + ".film.f32"
+        film.tofile(raw)
+        try:
+            subprocess.run([FILM_REF_PATH, raw, str(W), str(H), repr(float(spp)), path], check=True)
+        finally:
+            os.remove(raw)

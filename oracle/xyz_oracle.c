@@ -1172,3 +1172,102 @@ void xyzo_adjoint(int s0, int spp, uint64_t seed, const float *dfilm, double *g_
   j.g_em = g_em;
   run_job(&j, nthreads);
 }
+
+/* ------------------------------------------------------------------ film output
+ * CCIR601_1_XYZ2RGB (libhi/hi/image/color_space.hpp:69-79) in float. */
+static void ccir601_xyz2rgb(const float xyz[3], float rgb[3]) {
+  rgb[0] = 1.9104f * xyz[0] - 0.5338f * xyz[1] - 0.2891f * xyz[2];
+  rgb[1] = -0.9844f * xyz[0] + 1.9985f * xyz[1] - 0.0279f * xyz[2];
+  rgb[2] = 0.0585f * xyz[0] - 0.1187f * xyz[1] + 0.9017f * xyz[2];
+}
+
+/* static_cast<unsigned char>(float) as the reference's x86-64 build performs it:
+ * truncation towards zero to a 32-bit integer, low byte kept. */
+static unsigned char byte_of(float v) { return (unsigned char)(unsigned int)(int)v; }
+
+/* hdr_encode (xyz/core/imagefilm_hdr.cpp:14-31). */
+static void rgbe_of(const float c[3], unsigned char out[4]) {
+  float d = c[0] > c[1] ? c[0] : c[1];
+  d = d > c[2] ? d : c[2];
+  if ((double)d <= 1e-32) {
+    out[0] = out[1] = out[2] = out[3] = 0;
+    return;
+  }
+  int e;
+  float const m = frexpf(d, &e);
+  float const f = (float)((double)m * 255.9999 / (double)d);
+  out[0] = byte_of(c[0] * f);
+  out[1] = byte_of(c[1] * f);
+  out[2] = byte_of(c[2] * f);
+  out[3] = (unsigned char)(e + 128);
+}
+
+/* The pixels of ImageFilm::SaveAsHdr (imagefilm_hdr.cpp:124-183) in file order:
+ * film * scale, CCIR 601-1 RGB with non-finite pixels as 0, scanlines from the
+ * top row down; xyze: XYZ, scanlines from the bottom row up (CONFIG_HDR_STRICT). */
+void xyzo_encode_rgbe(const float *film, int W, int H, float scale, int xyze, unsigned char *out) {
+  for (int row = 0; row < H; ++row) {
+    int const y = xyze ? row : H - 1 - row;
+    for (int x = 0; x < W; ++x) {
+      const float *f = film + 3 * ((size_t)y * W + x);
+      float xyz[3] = {f[0] * scale, f[1] * scale, f[2] * scale}, c[3];
+      if (xyze) {
+        c[0] = xyz[0], c[1] = xyz[1], c[2] = xyz[2];
+      } else {
+        ccir601_xyz2rgb(xyz, c);
+        if (!isfinite(c[0]) || !isfinite(c[1]) || !isfinite(c[2])) c[0] = c[1] = c[2] = 0.0f;
+      }
+      rgbe_of(c, out + 4 * ((size_t)row * W + x));
+    }
+  }
+}
+
+/* tonemap() and clamp() of float2bmp/main.cpp:69-118 with the operator chosen
+ * at run time (0 film 1 - exp(-e L), the tool's; 1 linear; 2 Reinhard; 3
+ * Reinhard with white). */
+static unsigned char tone_one(float light, int op, float exposure, float white, float gamma) {
+  if (light <= 0) return 0;
+  float v;
+  switch (op) {
+    case 1: v = exposure * light; break;
+    case 2: v = exposure * light / (1 + light); break;
+    case 3: v = exposure * light * (1 + light / (white * white)) / (1 + light); break;
+    default: v = 1.0f - expf(-exposure * light); break;
+  }
+  v = powf(v, gamma);
+  if (v <= 0) return 0;
+  if (v >= 1) return 255;
+  return (unsigned char)(v * 256);
+}
+
+/* float2bmp's image loop (main.cpp:186-214): white <= 0 takes the maximum of
+ * 0.6069 c0 + 0.1735 c1 + 0.2003 c2; BGR bytes, rows from the bottom padded to
+ * 4 bytes. */
+void xyzo_tonemap(const float *film, int W, int H, float scale, int op, float exposure, float white,
+                  float dst_gamma, float src_gamma, int rgb, unsigned char *out) {
+  size_t const n = (size_t)W * H, stride = ((size_t)3 * W + 3) & ~(size_t)3;
+  float const gamma = src_gamma / dst_gamma;
+  if (op == 3 && !(white > 0)) {
+    white = 0;
+    for (size_t p = 0; p < n; ++p) {
+      float c[3] = {film[3 * p] * scale, film[3 * p + 1] * scale, film[3 * p + 2] * scale};
+      if (rgb) {
+        float const xyz[3] = {c[0], c[1], c[2]};
+        ccir601_xyz2rgb(xyz, c);
+      }
+      float const l = 0.6069f * c[0] + 0.1735f * c[1] + 0.2003f * c[2];
+      if (white < l) white = l;
+    }
+  }
+  for (size_t p = 0; p < n; ++p) {
+    float c[3] = {film[3 * p] * scale, film[3 * p + 1] * scale, film[3 * p + 2] * scale};
+    if (rgb) {
+      float const xyz[3] = {c[0], c[1], c[2]};
+      ccir601_xyz2rgb(xyz, c);
+    }
+    unsigned char *o = out + (p / W) * stride + 3 * (p % W);
+    o[2] = tone_one(c[0], op, exposure, white, gamma);
+    o[1] = tone_one(c[1], op, exposure, white, gamma);
+    o[0] = tone_one(c[2], op, exposure, white, gamma);
+  }
+}

@@ -2,12 +2,15 @@
 // the way the reference's shell drives xyz::Scene and PathTracer
 // (xyz/core/shell.cpp:204-497: load, set eye/at/dim, ren).
 //
-//   xyz_render <scene_dir> <out.pfm> <spp> <interval> <seed> <max_depth> [--guided]
+//   xyz_render <scene_dir> <out> <spp> <interval> <seed> <max_depth>
+//              [--guided | --checkpoint <file>]
 //       scene_dir holds positions.f32 triangles.i32 material.i32 albedo.f32
 //       is_light.i32 power.f32 camera.f32 (eye, at, film, focal, F, pinhole)
-//       dims.i32 (W, H) and, optionally, normals.f32; writes the film / spp as
-//       PFM after every pass and prints "passes N spp S sum X"; --guided renders
-//       with GuidedPathTracer (the first quarter of the samples train the guide).
+//       dims.i32 (W, H) and, optionally, normals.f32; writes the film / spp to
+//       `out` (.pfm, .float, .hdr or .bmp) after every pass and prints
+//       "passes N spp S sum X"; --guided renders with GuidedPathTracer (the
+//       first quarter of the samples train the guide); --checkpoint saves the
+//       render after every pass and resumes from the file if it exists.
 //   xyz_render --film-selftest <out.pfm> <out.float>
 //       writes a synthetic 3 x 2 film with both writers (no GPU needed).
 #include <cstdio>
@@ -44,8 +47,11 @@ int main(int argc, char **argv) {
     return ok ? 0 : 1;
   }
   bool const guided = argc == 8 && std::string(argv[7]) == "--guided";
-  if (argc != 7 && !guided) {
-    std::fprintf(stderr, "usage: xyz_render <scene_dir> <out.pfm> <spp> <interval> <seed> <max_depth> [--guided]\n");
+  bool const ckpt = argc == 9 && std::string(argv[7]) == "--checkpoint";
+  if (argc != 7 && !guided && !ckpt) {
+    std::fprintf(stderr,
+                 "usage: xyz_render <scene_dir> <out> <spp> <interval> <seed> <max_depth> "
+                 "[--guided | --checkpoint <file>]\n");
     return 2;
   }
   std::string const dir = argv[1];
@@ -86,6 +92,7 @@ int main(int argc, char **argv) {
       xyzgpu::PathTracer pt;                                 // ren
       pt.seed = std::strtoull(argv[5], nullptr, 10);
       pt.max_depth = std::atoi(argv[6]);
+      if (ckpt) pt.checkpoint = argv[8];
       spp = pt.run(scene, &film, std::atoi(argv[3]), std::atoi(argv[4]), on_pass);
     }
     double sum = 0.0;

@@ -51,3 +51,58 @@ def grazing_mask(sd, org, d, tri, f, g, eps=1e-4):
     cosang = np.abs((n * d).sum(axis=1))
     m[hit] |= cosang[hit] < 1e-3
     return m
+
+
+def read_hdr(path):
+    """Radiance .hdr reader (header, then flat or run-length scanlines):
+    returns (header lines, (rows, W, 4) uint8 in file order)."""
+    data = open(path, "rb").read()
+    end = data.index(b"\n\n")
+    head = data[:end].decode().split("\n")
+    nl = data.index(b"\n", end + 2)
+    res = data[end + 2:nl].decode().split()
+    H, W = int(res[1]), int(res[3])
+    pos = nl + 1
+    img = np.zeros((H, W, 4), np.uint8)
+    for r in range(H):
+        if 8 <= W <= 0x7FFF:
+            assert data[pos] == 2 and data[pos + 1] == 2 and (data[pos + 2] << 8 | data[pos + 3]) == W
+            pos += 4
+            for c in range(4):
+                x = 0
+                while x < W:
+                    code = data[pos]
+                    pos += 1
+                    if code > 128:
+                        n = code - 128
+                        img[r, x:x + n, c] = data[pos]
+                        pos += 1
+                    else:
+                        n = code
+                        assert n > 0
+                        img[r, x:x + n, c] = np.frombuffer(data[pos:pos + n], np.uint8)
+                        pos += n
+                    x += n
+                assert x == W
+        else:
+            img[r] = np.frombuffer(data[pos:pos + 4 * W], np.uint8).reshape(W, 4)
+            pos += 4 * W
+    assert pos == len(data)
+    return head + [" ".join(res)], img
+
+
+def sample_films(seed=0):
+    """Films (H, W, 3) of XYZ sums for the output formats: smooth, saturated
+    (negative RGB components), dark, very bright, with zeros and a NaN."""
+    rng = np.random.default_rng(seed)
+    H, W = 19, 37
+    base = rng.uniform(0.0, 2.0, (H, W, 3)).astype(np.float32)
+    base[0] = 0.0
+    base[1, :, 0] = rng.uniform(0.0, 0.05, W)         # saturated: X small, Y large
+    base[1, :, 1] = rng.uniform(1.0, 3.0, W)
+    base[2] *= np.float32(1e-6)
+    base[3] *= np.float32(1e4)
+    base[4, :5] = [0.7, 0.7, 0.7]                      # a run of equal pixels
+    base[5, 3] = np.nan
+    base[6, 7] = [-1.0, 0.5, 0.2]
+    return base

@@ -110,3 +110,48 @@ def test_cpp_guided_path_tracer(tmp_path):
         plain = plain.cpu().numpy() / 64
     assert np.isfinite(img).all() and (img >= 0).all()
     assert abs(img.mean() / plain.mean() - 1.0) < 0.05
+
+
+def _write_scene(sd, d, W=64, H=48):
+    d.mkdir()
+    sd.positions.astype("<f4").tofile(d / "positions.f32")
+    sd.tris.astype("<i4").tofile(d / "triangles.i32")
+    sd.tri_mat.astype("<i4").tofile(d / "material.i32")
+    sd.albedo_xyz.astype("<f4").tofile(d / "albedo.f32")
+    sd.is_light.astype("<i4").tofile(d / "is_light.i32")
+    sd.light_power_xyz.astype("<f4").tofile(d / "power.f32")
+    c = sd.camera
+    np.array(list(c.eye) + list(c.at) + [c.film_size, c.focal_length, c.f_number, float(c.pinhole)],
+             "<f4").tofile(d / "camera.f32")
+    np.array([W, H], "<i4").tofile(d / "dims.i32")
+
+
+@pytest.mark.gpu
+def test_cpp_path_tracer_resumes_from_its_checkpoint(tmp_path):
+    """PathTracer with a checkpoint: a render stopped after 6 of 12 samples and
+    run again continues from the file, and its film is the uninterrupted
+    render's film bit for bit; the .hdr and .bmp outputs come from the GPU."""
+    from tests.helpers import read_hdr
+    from xyz_b200 import scenes
+    exe = _compile(tmp_path)
+    sd = scenes.cornell_box(pinhole=True)
+    d = tmp_path / "scene"
+    _write_scene(sd, d)
+    ck = str(tmp_path / "r.ckpt")
+    a, b = str(tmp_path / "a.pfm"), str(tmp_path / "b.pfm")
+    r = subprocess.run([exe, str(d), b, "6", "3", "21", "8", "--checkpoint", ck], check=True,
+                       capture_output=True, text=True)
+    assert "passes 2 spp 6" in r.stdout
+    r = subprocess.run([exe, str(d), b, "12", "3", "21", "8", "--checkpoint", ck], check=True,
+                       capture_output=True, text=True)
+    assert "passes 2 spp 12" in r.stdout, r.stdout     # resumed at 6: two more passes
+    subprocess.run([exe, str(d), a, "12", "3", "21", "8"], check=True, capture_output=True)
+    assert np.array_equal(read_pfm(a), read_pfm(b))
+    h = str(tmp_path / "c.hdr")
+    subprocess.run([exe, str(d), h, "4", "4", "21", "8"], check=True, capture_output=True)
+    head, px = read_hdr(h)
+    assert head[-1] == "-Y 48 +X 64" and px[..., 3].max() > 0
+    bm = str(tmp_path / "c.bmp")
+    subprocess.run([exe, str(d), bm, "4", "4", "21", "8"], check=True, capture_output=True)
+    raw = open(bm, "rb").read()
+    assert raw[:2] == b"BM" and len(raw) == 54 + 64 * 3 * 48

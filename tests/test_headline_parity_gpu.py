@@ -57,14 +57,20 @@ def _three_sigma(ma, va, mb, vb):
 
 
 # ------------------------------------------------------------------ C1
-def _c1_port(sd):
+@pytest.fixture
+def c1_port():
+    """The oracle set up for the Cornell configuration (its spectral mode is
+    process-wide state of the oracle library: reset when the test ends)."""
+    from xyz_b200 import scenes
+    sd = scenes.cornell_box(pinhole=True)
     P = ensure_port()
     P.scene_create(sd)
     P.set_spectra(sd.albedo_spd, sd.light_power_spd)
     P.set_spectral(2, C1["hero"])
     P.set_camera(sd.camera, C1["W"], C1["H"])
     P.set_path_params(max_depth=C1["max_depth"], rr_start=C1["rr_start_depth"])
-    return P
+    yield sd, P
+    P.set_spectral(0, 1)
 
 
 def _c1_gpu(s, sd, spp, seed, spp_offset=0):
@@ -73,10 +79,9 @@ def _c1_gpu(s, sd, spp, seed, spp_offset=0):
                     spectral=C1["spectral"], hero_wavelengths=C1["hero"]).cpu().numpy()
 
 
-def test_c1_cornell_same_streams_matches_oracle():
-    from xyz_b200 import api, scenes
-    sd = scenes.cornell_box(pinhole=True)
-    P = _c1_port(sd)
+def test_c1_cornell_same_streams_matches_oracle(c1_port):
+    from xyz_b200 import api
+    sd, P = c1_port
     ref = P.render(C1["spp"], seed=C1["seed"], nthreads=0)
     with api.Scene(sd) as s:
         film = _c1_gpu(s, sd, C1["spp"], C1["seed"])
@@ -86,10 +91,9 @@ def test_c1_cornell_same_streams_matches_oracle():
     assert abs(film.sum() - ref.sum()) / ref.sum() < 5e-3
 
 
-def test_c1_cornell_per_pixel_three_sigma_on_independent_streams():
-    from xyz_b200 import api, scenes
-    sd = scenes.cornell_box(pinhole=True)
-    P = _c1_port(sd)
+def test_c1_cornell_per_pixel_three_sigma_on_independent_streams(c1_port):
+    from xyz_b200 import api
+    sd, P = c1_port
     mo, vo = _per_sample_stats(lambda k: P.render(1, seed=1, s0=k, nthreads=0), C1["spp"])
     with api.Scene(sd) as s:
         mg, vg = _per_sample_stats(lambda k: _c1_gpu(s, sd, 1, C1["seed"], spp_offset=k), C1["spp"])
@@ -113,6 +117,7 @@ def c2():
     sd = scenes.spheres_scene(level=7, n_spheres=3, seed=0)
     assert sd.n_tris == 984322
     P = ensure_port()
+    P.set_spectral(0, 1)   # the XYZ estimator (the oracle's mode is process-wide)
     P.scene_create(sd)
     P.set_camera(sd.camera, C2["W"], C2["H"])
     P.set_path_params(max_depth=C2["max_depth"])

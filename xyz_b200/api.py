@@ -39,6 +39,9 @@ EXPORTED = [
     "xyzgpu_guide_config_default", "xyzgpu_guide_create", "xyzgpu_guide_destroy",
     "xyzgpu_guide_get_params", "xyzgpu_guide_set_params", "xyzgpu_guide_forward",
     "xyzgpu_guide_gradient", "xyzgpu_guide_train_step", "xyzgpu_render_guided", "xyzgpu_guide_stats_get",
+    "xyzgpu_guide_reserve", "xyzgpu_film_encode_rgbe", "xyzgpu_hdr_write", "xyzgpu_tonemap_params_default",
+    "xyzgpu_film_tonemap", "xyzgpu_bmp_write", "xyzgpu_checkpoint_save", "xyzgpu_checkpoint_load",
+    "xyzgpu_film_save_hdr", "xyzgpu_film_save_bmp",
 ]
 
 
@@ -84,7 +87,8 @@ class RenderParams(C.Structure):
                 ("max_depth", C.c_int), ("rr_start_depth", C.c_int), ("rr_threshold", C.c_float),
                 ("seed", C.c_uint64), ("film_location", C.c_int), ("accumulate", C.c_int),
                 ("wave_paths", C.c_int), ("profile", C.c_int), ("spectral", C.c_int),
-                ("hero_wavelengths", C.c_int), ("row_begin", C.c_int), ("row_end", C.c_int)]
+                ("hero_wavelengths", C.c_int), ("row_begin", C.c_int), ("row_end", C.c_int),
+                ("row_step", C.c_int)]
 
 SPECTRAL_MODES = {"off": 0, "xyz": 0, "binned": 1, "continuous": 2}
 
@@ -101,6 +105,14 @@ class GuideConfig(C.Structure):
 
 class GuideStats(C.Structure):
     _fields_ = [("adam_steps", C.c_uint64), ("trained_records", C.c_uint64)]
+
+
+class TonemapParams(C.Structure):
+    _fields_ = [("scale", C.c_float), ("op", C.c_int), ("exposure", C.c_float), ("white", C.c_float),
+                ("dst_gamma", C.c_float), ("src_gamma", C.c_float), ("rgb", C.c_int)]
+
+
+TONEMAP_OPS = {"film": 0, "linear": 1, "reinhard": 2, "reinhard_white": 3}
 
 
 class BatchJobDesc(C.Structure):
@@ -190,6 +202,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.xyzgpu_render_guided.argtypes = [C.c_void_p, C.POINTER(CameraDesc), C.POINTER(RenderParams), C.c_int,
                                        C.c_void_p, C.c_void_p]
     L.xyzgpu_guide_stats_get.argtypes = [C.c_void_p, C.POINTER(GuideStats)]
+    L.xyzgpu_guide_reserve.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+    L.xyzgpu_film_encode_rgbe.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
+    L.xyzgpu_hdr_write.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
+    L.xyzgpu_tonemap_params_default.argtypes = [C.POINTER(TonemapParams)]
+    L.xyzgpu_film_tonemap.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(TonemapParams), C.c_void_p,
+                                      C.c_void_p, C.c_void_p]
+    L.xyzgpu_bmp_write.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.c_int]
+    L.xyzgpu_checkpoint_save.argtypes = [C.c_char_p, C.POINTER(RenderParams), C.c_int, C.c_void_p]
+    L.xyzgpu_checkpoint_load.argtypes = [C.c_char_p, C.POINTER(RenderParams), C.POINTER(C.c_int), C.c_void_p]
     L.xyzgpu_build_params_default.argtypes = [C.POINTER(BuildParams)]
     L.xyzgpu_render_params_default.argtypes = [C.POINTER(RenderParams)]
     _LIB = L
@@ -238,7 +259,10 @@ def render_params(width: int, height: int, spp: int, *, seed: int = 0, spp_offse
     rp.spectral = SPECTRAL_MODES[spectral] if isinstance(spectral, str) else int(spectral)
     rp.hero_wavelengths = hero_wavelengths
     if rows is not None:
+        # (begin, end) or (begin, end, step): rows begin, begin + step, ... < end
         rp.row_begin, rp.row_end = int(rows[0]), int(rows[1])
+        if len(rows) > 2:
+            rp.row_step = int(rows[2])
     return rp
 
 
@@ -474,6 +498,71 @@ class Scene:
         return d_albedo, d_emission
 
 
+# ------------------------------------------------------------------ film output
+def encode_rgbe(film, scale: float, xyze: bool = False, stream=None):
+    """xyzgpu_film_encode_rgbe: the .hdr pixels of a CUDA film (H, W, 3) of
+    sums, as a CUDA uint8 tensor (H, W, 4) in file order."""
+    import torch
+    H, W = int(film.shape[0]), int(film.shape[1])
+    out = torch.empty((H, W, 4), dtype=torch.uint8, device=film.device)
+    _check(load_library().xyzgpu_film_encode_rgbe(film.contiguous().data_ptr(), W, H, float(scale), int(xyze),
+                                                  out.data_ptr(), _stream_ptr(stream)))
+    return out
+
+
+def write_hdr(path: str, rgbe, xyze: bool = False):
+    """xyzgpu_hdr_write from host pixels (H, W, 4) uint8 in file order."""
+    a = np.ascontiguousarray(rgbe.cpu().numpy() if hasattr(rgbe, "cpu") else rgbe, np.uint8)
+    _check(load_library().xyzgpu_hdr_write(path.encode(), a.ctypes.data, a.shape[1], a.shape[0], int(xyze)))
+
+
+def save_hdr(path: str, film, spp: float, xyze: bool = False):
+    """The reference's ImageFilm::SaveAsHdr for a CUDA film of sums: device
+    encode, host file."""
+    write_hdr(path, encode_rgbe(film, 1.0 / spp, xyze), xyze)
+
+
+def tonemap(film, scale: float = 1.0, op="film", exposure: float = 1.0, white: float = 0.0,
+            dst_gamma: float = 2.2, src_gamma: float = 1.0, rgb: bool = False, stream=None):
+    """xyzgpu_film_tonemap: BMP pixel rows (H, stride) uint8 of a CUDA film."""
+    import torch
+    L = load_library()
+    H, W = int(film.shape[0]), int(film.shape[1])
+    tp = TonemapParams()
+    L.xyzgpu_tonemap_params_default(C.byref(tp))
+    tp.scale, tp.exposure, tp.white = float(scale), float(exposure), float(white)
+    tp.op = TONEMAP_OPS[op] if isinstance(op, str) else int(op)
+    tp.dst_gamma, tp.src_gamma, tp.rgb = float(dst_gamma), float(src_gamma), int(bool(rgb))
+    stride = (3 * W + 3) & ~3
+    out = torch.empty((H, stride), dtype=torch.uint8, device=film.device)
+    word = torch.zeros(1, dtype=torch.int32, device=film.device)
+    _check(L.xyzgpu_film_tonemap(film.contiguous().data_ptr(), W, H, C.byref(tp), out.data_ptr(), word.data_ptr(),
+                                 _stream_ptr(stream)))
+    return out
+
+
+def write_bmp(path: str, bgr, width: int, height: int):
+    a = np.ascontiguousarray(bgr.cpu().numpy() if hasattr(bgr, "cpu") else bgr, np.uint8)
+    _check(load_library().xyzgpu_bmp_write(path.encode(), a.ctypes.data, int(width), int(height)))
+
+
+def save_checkpoint(path: str, params: "RenderParams", spp_done: int, film):
+    """xyzgpu_checkpoint_save from a host film (H, W, 3) float32 of sums."""
+    a = np.ascontiguousarray(film.cpu().numpy() if hasattr(film, "cpu") else film, np.float32)
+    _check(load_library().xyzgpu_checkpoint_save(path.encode(), C.byref(params), int(spp_done), a.ctypes.data))
+
+
+def load_checkpoint(path: str):
+    """xyzgpu_checkpoint_load -> (RenderParams, spp_done, host film)."""
+    L = load_library()
+    rp = RenderParams()
+    done = C.c_int()
+    _check(L.xyzgpu_checkpoint_load(path.encode(), C.byref(rp), C.byref(done), None))
+    film = np.zeros((rp.height, rp.width, 3), np.float32)
+    _check(L.xyzgpu_checkpoint_load(path.encode(), C.byref(rp), C.byref(done), film.ctypes.data))
+    return rp, done.value, film
+
+
 def philox_u01(seed: int, pixel: int, sample: int, dim: int) -> float:
     return load_library().xyzgpu_philox_u01(seed, pixel, sample, dim)
 
@@ -626,6 +715,12 @@ class Guide:
         _check(_LIB.xyzgpu_guide_gradient(self.handle, records.contiguous().data_ptr(), n, float(scale),
                                           grad.data_ptr(), _stream_ptr(stream)))
         return grad
+
+    def reserve(self, wave_paths: int, train: bool = True, stream=None):
+        """xyzgpu_guide_reserve: allocate the guided-wave buffers (mixtures and,
+        with train, training records) for waves of up to wave_paths paths now,
+        so that no later render_guided call allocates."""
+        _check(_LIB.xyzgpu_guide_reserve(self.handle, int(wave_paths), int(bool(train)), _stream_ptr(stream)))
 
     def train_step(self, records, stream=None):
         _check(_LIB.xyzgpu_guide_train_step(self.handle, records.contiguous().data_ptr(), int(records.shape[0]),

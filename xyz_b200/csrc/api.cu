@@ -551,7 +551,8 @@ int check_render_args(const char *who, xyzgpu_scene scene, const xyzgpu_camera *
       (rp->spectral && (rp->hero_wavelengths < 1 || rp->hero_wavelengths > 4)) ||
       (rp->film_location != XYZGPU_FILM_DEVICE && rp->film_location != XYZGPU_FILM_HOST) ||
       !((rp->row_begin == 0 && rp->row_end == 0) ||
-        (rp->row_begin >= 0 && rp->row_begin < rp->row_end && rp->row_end <= rp->height)))
+        (rp->row_begin >= 0 && rp->row_begin < rp->row_end && rp->row_end <= rp->height)) ||
+      rp->row_step < 0)
     return set_error(XYZGPU_E_INVALID, "%s: parameters out of range", who);
   if (static_cast<int64_t>(rp->width) * rp->height >= (1ll << 31))
     return set_error(XYZGPU_E_LIMIT, "%s: image of %d x %d pixels exceeds 2^31", who, rp->width,

@@ -325,6 +325,49 @@ __device__ void loss_grad(const float *o, const float w[3], float scale, float *
   }
 }
 
+// ------------------------------------------------------------- training state
+// Device-resident training state, so that a whole training pass (records ->
+// steps_per_pass x (gradient, Adam) -> bookkeeping) runs without the host
+// reading anything back and can be replayed as one CUDA graph.
+struct TrainState {
+  long long step;               // Adam steps taken
+  long long offset;             // rolling start of the next batch in the training rows
+  unsigned long long trained;   // training rows produced so far
+  int count;                    // rows k_guide_records wrote (may exceed the buffer)
+  int pad;
+};
+
+// Rows of one gradient launch: explicit (rec, n, scale), or - with ts set -
+// batch `step_rel` of a training pass over min(ts->count, cap) rows at rec:
+// bs = min(batch, rows) rows from (ts->offset + step_rel * bs) mod rows,
+// moved back to rows - bs if they would run past the end, scale 1 / bs.
+struct GradArgs {
+  const float *rec;
+  int n;
+  float scale;
+  float *grad;
+  const TrainState *ts;
+  long long cap;
+  int step_rel;
+  int batch;
+};
+
+__device__ __forceinline__ bool grad_rows(const GradArgs &A, const float *&rec, int &n, float &scale) {
+  rec = A.rec;
+  n = A.n;
+  scale = A.scale;
+  if (!A.ts) return n > 0;
+  long long const rows = min(static_cast<long long>(A.ts->count), A.cap);
+  if (rows <= 0) return false;
+  long long const bs = min(static_cast<long long>(A.batch), rows);
+  long long off = (A.ts->offset + static_cast<long long>(A.step_rel) * bs) % rows;
+  if (off + bs > rows) off = rows - bs;
+  rec += 10 * off;
+  n = static_cast<int>(bs);
+  scale = 1.0f / static_cast<float>(bs);
+  return true;
+}
+
 // ------------------------------------------------------------- kernels
 // Copies the packed weight image (weights, ones tile, bias tiles) into shared
 // memory: 4,480 independent 16-byte loads, several in flight per thread.
@@ -418,7 +461,12 @@ __global__ void __launch_bounds__(kInferThreads, 1)
 // Gradient of sum over records of -w * log p(dir) * scale, added to grad
 // (flat parameter layout).  records: n x 10 = position, normal, direction, w.
 __global__ void __launch_bounds__(kGuideThreads, 1)
-    k_guide_gradient(const __grid_constant__ GuideDev G, const float *__restrict__ rec, int n, float scale, float *__restrict__ grad) {
+    k_guide_gradient(const __grid_constant__ GuideDev G, const __grid_constant__ GradArgs A) {
+  const float *rec;
+  int n;
+  float scale;
+  if (!grad_rows(A, rec, n, scale)) return;  // uniform over the grid: no rows
+  float *__restrict__ grad = A.grad;
   extern __shared__ __align__(128) uint8_t smem_raw[];
   GuideSmem &S = *reinterpret_cast<GuideSmem *>(smem_raw);
   load_weights(S.wt, G);
@@ -740,17 +788,68 @@ __global__ void k_guide_pack(const float *__restrict__ params, uint8_t *__restri
   }
 }
 
-__global__ void k_guide_adam(float *__restrict__ p, float *__restrict__ g, float *__restrict__ m,
-                             float *__restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2) {
+// One Adam step (bias-corrected, fp32 masters) fused with the re-pack of the
+// changed values into the weight image: a weight's bf16 copy in the blocked
+// W^T layout, a bias's hi / mid / lo parts in its bias tile (the ones tile and
+// the bias tiles' zero columns never change; k_guide_pack writes them).  The
+// step number comes from the training state: t = ts->step + step_rel + 1.
+// gate: skip the step when the training pass produced no rows.
+__global__ void k_guide_adam_pack(float *__restrict__ p, float *__restrict__ g, float *__restrict__ m,
+                                  float *__restrict__ v, uint8_t *__restrict__ wblk, float lr, float eps,
+                                  const TrainState *__restrict__ ts, int step_rel, long long cap, int gate) {
   int const i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= kParams) return;
+  if (gate && min(static_cast<long long>(ts->count), cap) <= 0) return;
+  long long const t = ts->step + step_rel + 1;
+  float const b1 = 0.9f, b2 = 0.99f;
+  float const c1 = static_cast<float>(1.0 - pow(0.9, static_cast<double>(t)));
+  float const c2 = static_cast<float>(1.0 - pow(0.99, static_cast<double>(t)));
   float const gi = g[i];
   float const mi = b1 * m[i] + (1.0f - b1) * gi;
   float const vi = b2 * v[i] + (1.0f - b2) * gi * gi;
   m[i] = mi;
   v[i] = vi;
-  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  float const pn = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  p[i] = pn;
   g[i] = 0.0f;
+  // position of parameter i in the image
+  int l = 0, rem = i;
+  while (l < kLayers && rem >= layer_in(l) * kW + kW) {
+    rem -= layer_in(l) * kW + kW;
+    ++l;
+  }
+  int const K = layer_in(l);
+  if (rem < K * kW) {
+    int const k = rem / kW, nn = rem % kW;  // W_l[k][nn]
+    *reinterpret_cast<__nv_bfloat16 *>(wblk + wblk_off(l) + tc::blocked_offset(nn, k, K)) = __float2bfloat16_rn(pn);
+  } else {
+    int const nn = rem - K * kW;  // b_l[nn]
+    __nv_bfloat16 const hi = __float2bfloat16_rn(pn);
+    float const r1 = pn - __bfloat162float(hi);
+    __nv_bfloat16 const mid = __float2bfloat16_rn(r1);
+    __nv_bfloat16 const lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
+    uint8_t *const base = wblk + kBiasOff + l * (kW * kBiasK * 2);
+    *reinterpret_cast<__nv_bfloat16 *>(base + tc::blocked_offset(nn, 0, kBiasK)) = hi;
+    *reinterpret_cast<__nv_bfloat16 *>(base + tc::blocked_offset(nn, 1, kBiasK)) = mid;
+    *reinterpret_cast<__nv_bfloat16 *>(base + tc::blocked_offset(nn, 2, kBiasK)) = lo;
+  }
+}
+
+// Bookkeeping after Adam steps.  pass: a training pass over min(count, cap)
+// rows took `steps` steps of min(batch, rows) rows (nothing happened if there
+// were no rows); else `steps` explicit steps.
+__global__ void k_guide_advance(TrainState *ts, int steps, int batch, long long cap, int pass) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (!pass) {
+    ts->step += steps;
+    return;
+  }
+  long long const rows = min(static_cast<long long>(ts->count), cap);
+  if (rows <= 0) return;
+  long long const bs = min(static_cast<long long>(batch), rows);
+  ts->offset += static_cast<long long>(steps) * bs;
+  ts->step += steps;
+  ts->trained += static_cast<unsigned long long>(rows);
 }
 
 }  // namespace
@@ -763,16 +862,23 @@ struct GuideImpl {
   float *d_params = nullptr, *d_grad = nullptr, *d_m = nullptr, *d_v = nullptr;
   uint8_t *d_wblk = nullptr;
   int *d_err = nullptr;
-  int64_t step = 0;
+  TrainState *d_ts = nullptr;  // Adam step, batch offset, row counts (device)
   float lo[3] = {0, 0, 0}, inv_ext[3] = {1, 1, 1};
   // guided-render buffers
   __half *d_mix = nullptr;
   int64_t mix_cap = 0;
   float *d_rec = nullptr, *d_train = nullptr;
   int64_t rec_cap = 0;  // paths
-  int *d_count = nullptr;
-  int64_t train_offset = 0;
-  uint64_t trained_records = 0;
+  // One CUDA graph per training-pass shape (records kernel, steps_per_pass x
+  // (gradient, Adam + pack), bookkeeping), captured on a private stream the
+  // first time a wave of that size trains and replayed on the caller's stream.
+  struct Pass {
+    int64_t npaths;
+    const float4 *radiance;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Pass> passes;
+  cudaStream_t cap_st = nullptr;
 };
 
 namespace {
@@ -841,10 +947,15 @@ int guide_gradient_launch(GuideImpl &g, const float *rec, int n, float scale, fl
     attr = true;
   }
   if (n <= 0) return XYZGPU_OK;
-  k_guide_gradient<<<grid_for(g.device, n), kGuideThreads, sizeof(GuideSmem), st>>>(guide_dev(g), rec, n, scale,
-                                                                                     grad);
+  GradArgs A{rec, n, scale, grad, nullptr, 0, 0, 0};
+  k_guide_gradient<<<grid_for(g.device, n), kGuideThreads, sizeof(GuideSmem), st>>>(guide_dev(g), A);
   XYZ_CUDA_TRY(cudaGetLastError());
   return XYZGPU_OK;
+}
+
+void drop_passes(GuideImpl &g) {
+  for (auto &p : g.passes) cudaGraphExecDestroy(p.exec);
+  g.passes.clear();
 }
 
 int guide_wave_prepare(GuideImpl &g, int64_t cap, bool train, cudaStream_t st, GuideWave *out) {
@@ -860,6 +971,7 @@ int guide_wave_prepare(GuideImpl &g, int64_t cap, bool train, cudaStream_t st, G
   int const tb = g.cfg.train_bounces;
   if (train && tb > 0 && g.rec_cap < cap) {
     XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+    drop_passes(g);
     cudaFree(g.d_rec);
     cudaFree(g.d_train);
     g.d_rec = g.d_train = nullptr;
@@ -870,7 +982,6 @@ int guide_wave_prepare(GuideImpl &g, int64_t cap, bool train, cudaStream_t st, G
       return set_error(XYZGPU_E_NOMEM, "render_guided: training record buffers of %zu records", n);
     g.rec_cap = cap;
   }
-  if (!g.d_count) XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&g.d_count), sizeof(int)));
   out->mix = g.d_mix;
   out->records = train && tb > 0 ? g.d_rec : nullptr;
   out->train_bounces = train ? tb : 0;
@@ -893,47 +1004,72 @@ int guide_infer_launch(GuideImpl &g, const float4 *qo, const float4 *qd, const f
   return XYZGPU_OK;
 }
 
-int guide_adam_launch(GuideImpl &g, cudaStream_t st);
+int adam_pack_launch(GuideImpl &g, const GuideDev &, int step_rel, long long cap, int gate, cudaStream_t st) {
+  k_guide_adam_pack<<<(kParams + 255) / 256, 256, 0, st>>>(g.d_params, g.d_grad, g.d_m, g.d_v, g.d_wblk,
+                                                          g.cfg.learning_rate, 1e-8f, g.d_ts, step_rel, cap, gate);
+  return cudaGetLastError() == cudaSuccess ? XYZGPU_OK : set_error(XYZGPU_E_CUDA, "guide: Adam launch failed");
+}
 
-// After a training wave: records -> training rows, then steps_per_pass Adam
-// steps on batches of batch_size rows (cycling through the rows).
-int guide_train_on_wave(GuideImpl &g, const float4 *radiance, int64_t npaths, cudaStream_t st) {
+// Enqueues a training pass's launches on `st` (which is being captured).
+int enqueue_pass(GuideImpl &g, const float4 *radiance, int64_t npaths, cudaStream_t st) {
   int const tb = g.cfg.train_bounces;
-  if (tb <= 0 || g.cfg.steps_per_pass <= 0 || !g.d_rec) return XYZGPU_OK;
-  int64_t const cap = npaths * tb;
-  XYZ_CUDA_TRY(cudaMemsetAsync(g.d_count, 0, sizeof(int), st));
+  long long const cap = npaths * tb;
+  GuideDev const G = guide_dev(g);
+  XYZ_CUDA_TRY(cudaMemsetAsync(&g.d_ts->count, 0, sizeof(int), st));
   int const blocks = std::max(1, std::min<int>(static_cast<int>((cap + 255) / 256), sm_count(g.device) * 8));
-  k_guide_records<<<blocks, 256, 0, st>>>(g.d_rec, tb, npaths, radiance, g.d_train, g.d_count, cap);
+  k_guide_records<<<blocks, 256, 0, st>>>(g.d_rec, tb, npaths, radiance, g.d_train, &g.d_ts->count, cap);
   XYZ_CUDA_TRY(cudaGetLastError());
-  int count = 0;
-  XYZ_CUDA_TRY(cudaMemcpyAsync(&count, g.d_count, sizeof(int), cudaMemcpyDeviceToHost, st));
-  XYZ_CUDA_TRY(cudaStreamSynchronize(st));
-  int64_t const rows = std::min<int64_t>(count, cap);
-  g.trained_records += static_cast<uint64_t>(rows);
-  if (rows <= 0) return XYZGPU_OK;
-  int64_t const bs = std::min<int64_t>(g.cfg.batch_size, rows);
+  // every CTA of the gradient grid takes tiles of the batch; the batch size
+  // is known only on the device, so the grid is one CTA per SM
+  int const grid = std::max(1, std::min(sm_count(g.device), (g.cfg.batch_size + kRows - 1) / kRows));
   for (int s = 0; s < g.cfg.steps_per_pass; ++s) {
-    int64_t off = (g.train_offset + s * bs) % rows;
-    if (off + bs > rows) off = rows - bs;
-    int rc = guide_gradient_launch(g, g.d_train + 10 * off, static_cast<int>(bs), 1.0f / static_cast<float>(bs),
-                                   g.d_grad, st);
-    if (rc) return rc;
-    rc = guide_adam_launch(g, st);
+    GradArgs A{g.d_train, 0, 0.0f, g.d_grad, g.d_ts, cap, s, g.cfg.batch_size};
+    k_guide_gradient<<<grid, kGuideThreads, sizeof(GuideSmem), st>>>(G, A);
+    XYZ_CUDA_TRY(cudaGetLastError());
+    int const rc = adam_pack_launch(g, G, s, cap, 1, st);
     if (rc) return rc;
   }
-  g.train_offset += g.cfg.steps_per_pass * bs;
+  k_guide_advance<<<1, 32, 0, st>>>(g.d_ts, g.cfg.steps_per_pass, g.cfg.batch_size, cap, 1);
+  XYZ_CUDA_TRY(cudaGetLastError());
   return XYZGPU_OK;
 }
 
-int guide_adam_launch(GuideImpl &g, cudaStream_t st) {
-  g.step += 1;
-  float const b1 = 0.9f, b2 = 0.99f;
-  float const c1 = static_cast<float>(1.0 - std::pow(0.9, static_cast<double>(g.step)));
-  float const c2 = static_cast<float>(1.0 - std::pow(0.99, static_cast<double>(g.step)));
-  k_guide_adam<<<(kParams + 255) / 256, 256, 0, st>>>(g.d_params, g.d_grad, g.d_m, g.d_v, g.cfg.learning_rate, b1,
-                                                      b2, 1e-8f, c1, c2);
-  XYZ_CUDA_TRY(cudaGetLastError());
-  return pack(g, st);
+// After a training wave: records -> training rows, then steps_per_pass Adam
+// steps on batches of batch_size rows (cycling through the rows), all on the
+// device: one graph launch, no host synchronisation.
+int guide_train_on_wave(GuideImpl &g, const float4 *radiance, int64_t npaths, cudaStream_t st) {
+  int const tb = g.cfg.train_bounces;
+  if (tb <= 0 || g.cfg.steps_per_pass <= 0 || !g.d_rec) return XYZGPU_OK;
+  cudaGraphExec_t exec = nullptr;
+  for (auto &p : g.passes)
+    if (p.npaths == npaths && p.radiance == radiance) exec = p.exec;
+  if (!exec) {
+    static bool attr = false;
+    if (!attr) {
+      XYZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_gradient, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(sizeof(GuideSmem))));
+      attr = true;
+    }
+    if (!g.cap_st) XYZ_CUDA_TRY(cudaStreamCreateWithFlags(&g.cap_st, cudaStreamNonBlocking));
+    if (g.passes.size() >= 4) drop_passes(g);
+    XYZ_CUDA_TRY(cudaStreamBeginCapture(g.cap_st, cudaStreamCaptureModeThreadLocal));
+    int const rc = enqueue_pass(g, radiance, npaths, g.cap_st);
+    cudaGraph_t graph = nullptr;
+    cudaError_t const e = cudaStreamEndCapture(g.cap_st, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return set_error(XYZGPU_E_CUDA, "render_guided: capturing the training pass: %s",
+                                           cudaGetErrorString(e));
+    cudaError_t const ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return set_error(XYZGPU_E_CUDA, "render_guided: instantiating the training pass: %s",
+                                            cudaGetErrorString(ei));
+    g.passes.push_back(GuideImpl::Pass{npaths, radiance, exec});
+  }
+  XYZ_CUDA_TRY(cudaGraphLaunch(exec, st));
+  return XYZGPU_OK;
 }
 
 }  // namespace xyzgpu
@@ -973,7 +1109,9 @@ void xyzgpu_guide_destroy(xyzgpu_guide h) {
   cudaFree(g.d_mix);
   cudaFree(g.d_rec);
   cudaFree(g.d_train);
-  cudaFree(g.d_count);
+  cudaFree(g.d_ts);
+  drop_passes(g);
+  if (g.cap_st) cudaStreamDestroy(g.cap_st);
   cudaSetDevice(prev);
   delete h;
 }
@@ -1014,7 +1152,8 @@ int xyzgpu_guide_create(xyzgpu_scene scene, const xyzgpu_guide_config *cfg, xyzg
       cudaMalloc(reinterpret_cast<void **>(&g.d_m), kParams * sizeof(float)) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void **>(&g.d_v), kParams * sizeof(float)) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void **>(&g.d_wblk), kWImageBytes) != cudaSuccess ||
-      cudaMalloc(reinterpret_cast<void **>(&g.d_err), sizeof(int)) != cudaSuccess)
+      cudaMalloc(reinterpret_cast<void **>(&g.d_err), sizeof(int)) != cudaSuccess ||
+      cudaMalloc(reinterpret_cast<void **>(&g.d_ts), sizeof(TrainState)) != cudaSuccess)
     return fail(set_error(XYZGPU_E_NOMEM, "guide_create: device allocation failed"));
   // He-uniform hidden layers, a small output layer (near-uniform mixture at
   // the start), zero biases
@@ -1028,7 +1167,8 @@ int xyzgpu_guide_create(xyzgpu_scene scene, const xyzgpu_guide_config *cfg, xyzg
       cudaMemset(g.d_grad, 0, kParams * sizeof(float)) != cudaSuccess ||
       cudaMemset(g.d_m, 0, kParams * sizeof(float)) != cudaSuccess ||
       cudaMemset(g.d_v, 0, kParams * sizeof(float)) != cudaSuccess ||
-      cudaMemset(g.d_err, 0, sizeof(int)) != cudaSuccess)
+      cudaMemset(g.d_err, 0, sizeof(int)) != cudaSuccess ||
+      cudaMemset(g.d_ts, 0, sizeof(TrainState)) != cudaSuccess)
     return fail(set_error(XYZGPU_E_CUDA, "guide_create: initialisation failed"));
   int rc = pack(g, nullptr);
   if (rc) return fail(rc);
@@ -1055,7 +1195,7 @@ int xyzgpu_guide_set_params(xyzgpu_guide h, const float *params) {
   XYZ_CUDA_TRY(cudaMemcpy(g.d_params, params, kParams * sizeof(float), cudaMemcpyHostToDevice));
   XYZ_CUDA_TRY(cudaMemset(g.d_m, 0, kParams * sizeof(float)));
   XYZ_CUDA_TRY(cudaMemset(g.d_v, 0, kParams * sizeof(float)));
-  g.step = 0;
+  XYZ_CUDA_TRY(cudaMemset(&g.d_ts->step, 0, sizeof(long long)));
   int const rc = pack(g, nullptr);
   if (rc) return rc;
   XYZ_CUDA_TRY(cudaStreamSynchronize(nullptr));
@@ -1097,7 +1237,8 @@ int xyzgpu_render_guided(xyzgpu_guide h, const xyzgpu_camera *cam, const xyzgpu_
       rp->max_depth > 1000 || rp->rr_start_depth < 1 || !(rp->rr_threshold >= 0.0f) || rp->wave_paths < 0 ||
       (rp->film_location != XYZGPU_FILM_DEVICE && rp->film_location != XYZGPU_FILM_HOST) ||
       !((rp->row_begin == 0 && rp->row_end == 0) ||
-        (rp->row_begin >= 0 && rp->row_begin < rp->row_end && rp->row_end <= rp->height)))
+        (rp->row_begin >= 0 && rp->row_begin < rp->row_end && rp->row_end <= rp->height)) ||
+      rp->row_step < 0)
     return set_error(XYZGPU_E_INVALID, "render_guided: parameters out of range");
   if (static_cast<int64_t>(rp->width) * rp->height >= (1ll << 31) ||
       static_cast<int64_t>(rp->spp_offset) + rp->spp >= (1ll << 32))
@@ -1120,8 +1261,12 @@ int xyzgpu_render_guided(xyzgpu_guide h, const xyzgpu_camera *cam, const xyzgpu_
 int xyzgpu_guide_stats_get(xyzgpu_guide h, xyzgpu_guide_stats *out) {
   clear_error();
   if (!h || !out) return set_error(XYZGPU_E_INVALID, "guide_stats_get: null argument");
-  out->adam_steps = static_cast<uint64_t>(h->g.step);
-  out->trained_records = h->g.trained_records;
+  XYZ_CUDA_TRY(cudaSetDevice(h->g.device));
+  XYZ_CUDA_TRY(cudaDeviceSynchronize());
+  TrainState ts;
+  XYZ_CUDA_TRY(cudaMemcpy(&ts, h->g.d_ts, sizeof(ts), cudaMemcpyDeviceToHost));
+  out->adam_steps = static_cast<uint64_t>(ts.step);
+  out->trained_records = ts.trained;
   return XYZGPU_OK;
 }
 
@@ -1134,9 +1279,26 @@ int xyzgpu_guide_train_step(xyzgpu_guide h, const float *records, int n, void *s
   XYZ_CUDA_TRY(cudaMemsetAsync(g.d_err, 0, sizeof(int), st));
   int rc = guide_gradient_launch(g, records, n, 1.0f / static_cast<float>(n), g.d_grad, st);
   if (rc) return rc;
-  rc = guide_adam_launch(g, st);
+  rc = adam_pack_launch(g, guide_dev(g), 0, 0, 0, st);
   if (rc) return rc;
+  k_guide_advance<<<1, 32, 0, st>>>(g.d_ts, 1, 0, 0, 0);
+  XYZ_CUDA_TRY(cudaGetLastError());
   return check_err(g, st, "guide_train_step");
+}
+
+int xyzgpu_guide_reserve(xyzgpu_guide h, int64_t wave_paths, int train, void *stream) {
+  clear_error();
+  if (!h || wave_paths <= 0) return set_error(XYZGPU_E_INVALID, "guide_reserve: bad argument");
+  if (wave_paths > (int64_t{1} << 23))
+    return set_error(XYZGPU_E_LIMIT, "guide_reserve: at most 2^23 paths per guided wave");
+  GuideImpl &g = h->g;
+  cudaStream_t const st = static_cast<cudaStream_t>(stream);
+  XYZ_CUDA_TRY(cudaSetDevice(g.device));
+  GuideWave gw;
+  int const rc = guide_wave_prepare(g, wave_paths, train != 0, st, &gw);
+  if (rc) return rc;
+  XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+  return XYZGPU_OK;
 }
 
 }  // extern "C"

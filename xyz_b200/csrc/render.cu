@@ -136,10 +136,11 @@ void render_workspace_free(RenderWorkspace &w) {
 int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp, float *film,
                   cudaStream_t st, const AdjointArgs *adj, const GuideHooks *guide) {
   XYZ_CUDA_TRY(cudaSetDevice(s.device));
-  // a band of rows renders the same pixels (and paths) as the full image
+  // a band of rows (every row_step-th row of it) renders the same pixels and
+  // paths as the full image
   int64_t const row0 = rp.row_end > 0 ? rp.row_begin : 0;
-  int64_t const rows = rp.row_end > 0 ? rp.row_end - rp.row_begin : rp.height;
-  int64_t const pix_first = row0 * rp.width;
+  int64_t const row_step = rp.row_end > 0 && rp.row_step > 1 ? rp.row_step : 1;
+  int64_t const rows = rp.row_end > 0 ? (rp.row_end - rp.row_begin + row_step - 1) / row_step : rp.height;
   int64_t const npix_total = static_cast<int64_t>(rp.width) * rows;
   int64_t const film_elems = 3 * static_cast<int64_t>(rp.width) * rp.height;
   int const iters = rp.max_depth;
@@ -266,7 +267,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   }
   GuideWave gw;
   if (guide) {
-    int const r = guide_wave_prepare(*guide->g, cap, guide->train, st, &gw);
+    // a wave never holds more paths than the call renders
+    int64_t const need = std::min<int64_t>(cap, std::max<int64_t>(1, npix_total * rp.spp));
+    int const r = guide_wave_prepare(*guide->g, need, guide->train, st, &gw);
     if (r) return r;
     A.mix = static_cast<const __half *>(gw.mix);
     A.guide_alpha = gw.alpha;
@@ -282,7 +285,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   for (int64_t s0 = 0; s0 < rp.spp; s0 += spp_per_wave) {
     int const ns = static_cast<int>(std::min<int64_t>(spp_per_wave, rp.spp - s0));
     for (int64_t p0 = 0; p0 < npix_total; p0 += pix_per_wave) {
-      A.p0 = pix_first + p0;
+      A.p0 = p0;
+      A.row0 = row0;
+      A.row_step = static_cast<int>(row_step);
       A.npix = std::min<int64_t>(pix_per_wave, npix_total - p0);
       A.s0 = static_cast<uint32_t>(rp.spp_offset + s0);
       A.nsamp = ns;

@@ -19,6 +19,8 @@
 // continues on the side its direction points to.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace xyzgpu {
@@ -81,7 +83,27 @@ struct __align__(8) StackEntry {
 //   Sink::store(i, hit)               result of ray i
 //   Sink::scene(i)                    (kBatch) the scene of ray i; rays of one
 //                                     queue may belong to different scenes
+//   Sink::target(i)                   (sinks with kTarget) the triangle whose
+//                                     being the closest hit is the only
+//                                     question the caller asks (next-event
+//                                     estimation's visibility test,
+//                                     xyz/bsdf/lambert.cpp:151-155)
+//
+// Target queries end early, with the same answer the full closest-hit search
+// gives: the target's own hit distance t_own is computed first, with the
+// same arithmetic the traversal would apply to it.  If the target is not hit
+// at all, it cannot be the closest hit and the ray needs no traversal.  Once
+// any triangle is accepted at t < t_own, the final closest hit has t < t_own
+// too, so it is not the target whatever the remaining nodes hold, and the ray
+// stops (the store then sees a non-target id).  Nothing else changes: the
+// target itself and hits at t >= t_own go through the unchanged closest-hit
+// rules, so ties and rounding across split planes resolve as before.
 constexpr int kRefillIdle = 12;
+
+template <class S, class = void>
+struct SinkHasTarget : std::false_type {};
+template <class S>
+struct SinkHasTarget<S, std::void_t<decltype(S::kTarget)>> : std::bool_constant<S::kTarget> {};
 // One iteration of the persistent loop descends at most this many nodes; a lane
 // still above its next leaf resumes there in the next iteration, so the warp's
 // leaf tests do not wait for its longest descent (counting renders descend
@@ -93,6 +115,7 @@ constexpr int kDescendSteps = XYZ_DESCEND_STEPS;
 
 template <bool kCount, bool kBatch = false, class Sink>
 XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, TraceCount &tc) {
+  constexpr bool kTarget = SinkHasTarget<Sink>::value;
   int const lane = threadIdx.x & 31;
   unsigned const lanes_below = (1u << lane) - 1u;
   int ray = -1;
@@ -101,6 +124,7 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
   float inv[3] = {0.0f, 0.0f, 0.0f};
   float tmin = 0.0f;
   RayHit h{};
+  float stop_t = 0.0f;  // target queries: the target's own hit distance
   uint32_t node = 0;
   float tn = 0.0f, tf = 0.0f;
   int sp = 0;
@@ -131,6 +155,13 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
           h.id = -1;
           h.f = h.g = 0.0f;
           h.back = 0;
+          bool skip = false;
+          if constexpr (kTarget) {
+            RayHit own = h;
+            skip = !hit_triangle(SL.tri, sink.target(i), o, d, tmin, own);
+            stop_t = own.t;
+            if (kCount) tc.tris++;
+          }
           inv[0] = __frcp_rn(d.x);
           inv[1] = __frcp_rn(d.y);
           inv[2] = __frcp_rn(d.z);
@@ -145,7 +176,10 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
             t0 = fmaxf(t0, fminf(ta, tb));
             t1 = fminf(t1, fmaxf(ta, tb));
           }
-          if (!(t0 <= t1)) {
+          if (skip) {
+            // the target is not hit: the answer is "not the target" (h.id = -1)
+            sink.store(i, h);
+          } else if (!(t0 <= t1)) {
             sink.store(i, h);  // misses the scene box
           } else {
             ray = i;
@@ -203,9 +237,10 @@ XYZ_DEV void trace_persistent(const DevScene &S, int n, int *fetch, Sink &sink, 
       int32_t const t = t_next;
       if (j + 1 < cnt) t_next = __ldg(&refs[nd.x + j + 1]);
       hit_triangle(tris, t, o, d, tmin, h);
+      if (kTarget && h.t < stop_t) break;
     }
     // next leaf (entered at this leaf's exit), or done
-    bool const done = (h.id >= 0 && h.t <= tf) || sp == 0;
+    bool const done = (h.id >= 0 && h.t <= tf) || sp == 0 || (kTarget && h.t < stop_t);
     if (!done) {
       --sp;
       StackEntry const e = stack[sp];

@@ -96,8 +96,10 @@ struct WaveArgs {
   int rr_start;
   float rr_threshold;
   uint64_t seed;
-  int64_t p0;       // first pixel of the wave
+  int64_t p0;       // first pixel of the wave, counted over the rendered rows
   int64_t npix;     // pixels in the wave
+  int64_t row0;     // first rendered image row
+  int row_step;     // rendered rows are row0, row0 + row_step, ... (0 or 1: consecutive)
   uint32_t s0;      // first sample index of the wave
   int nsamp;        // samples per pixel in the wave
   int64_t npaths;   // npix * nsamp
@@ -252,11 +254,18 @@ XYZ_DEV uint32_t pack_misc(uint32_t dim, uint32_t k, uint32_t specular) {
   return (dim & 0xffffu) | ((k & 0x7fffu) << 16) | (specular << 31);
 }
 
+// Image pixel (y * W + x) of pixel `lp` counted over the rendered rows.
+XYZ_DEV int64_t film_pixel(const WaveArgs &A, int64_t lp) {
+  if (A.row_step <= 1) return A.row0 * A.W + lp;
+  int64_t const r = lp / A.W;
+  return (A.row0 + r * A.row_step) * A.W + (lp - r * A.W);
+}
+
 XYZ_DEV void slot_to_pixel_sample(const WaveArgs &A, int64_t slot, uint32_t *pixel,
                                   uint32_t *sample) {
   int64_t const sl = slot / A.npix;
   int64_t const pl = slot - sl * A.npix;
-  *pixel = static_cast<uint32_t>(A.p0 + pl);
+  *pixel = static_cast<uint32_t>(film_pixel(A, A.p0 + pl));
   *sample = A.s0 + static_cast<uint32_t>(sl);
 }
 
@@ -447,8 +456,10 @@ struct ShadowSink {
   static constexpr bool kAdj = kMode == kModeAdjoint;
   static constexpr bool kBatch = kMode == kModeBatch;
   static constexpr bool kGuide = kMode == kModeGuided;
+  static constexpr bool kTarget = true;  // only "is the target the closest hit?" matters
   const WaveArgs *A;
   uint32_t visible;
+  XYZ_DEV int32_t target(int i) const { return __ldg(&A->s_target[i]); }
   XYZ_DEV void load(int i, f3 &o, f3 &d, float &tmin, float &tmax) const {
     float4 const a = __ldcs(&A->s_o[i]), b = __ldcs(&A->s_d[i]);
     o = xyz3(a);
@@ -1118,7 +1129,7 @@ __global__ void __launch_bounds__(kThreads) k_film_spectral(WaveArgs A, float *_
   int64_t const stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   float const scale = A.spectral == XYZGPU_SPECTRAL_BINNED ? static_cast<float>(kSpecBins) : 34.0f;
   for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < A.npix; p += stride) {
-    float *f = film + 3 * (A.p0 + p);
+    float *f = film + 3 * film_pixel(A, A.p0 + p);
     float fx = f[0], fy = f[1], fz = f[2];
     for (int s = 0; s < A.nsamp; ++s) {
       int64_t const slot = static_cast<int64_t>(s) * A.npix + p;
@@ -1154,7 +1165,7 @@ __global__ void __launch_bounds__(kThreads) k_film_spectral(WaveArgs A, float *_
 __global__ void __launch_bounds__(kThreads) k_film(WaveArgs A, float *__restrict__ film) {
   int64_t const stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < A.npix; p += stride) {
-    float *f = film + 3 * (A.p0 + p);
+    float *f = film + 3 * film_pixel(A, A.p0 + p);
     float fx = f[0], fy = f[1], fz = f[2];
     for (int s = 0; s < A.nsamp; ++s) {
       float4 const L = A.radiance[static_cast<int64_t>(s) * A.npix + p];
