@@ -458,12 +458,35 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
                     if gms > 0 else None}
                 return res, info
 
+        def importon_run(particles):
+            """The reference's non-learned guide: the light-importance map
+            (particles traced and sorted into the grid, CUDA-event time of the
+            build included in the total), then importance-driven passes."""
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            with api.Importons(s, particles=particles, seed=3) as m:
+                e1.record()
+                torch.cuda.synchronize()
+                build_s = e0.elapsed_time(e1) * 1e-3
+
+                def imp_pass(p, film):
+                    m.render(cam, W, H, pass_spp, seed=1, spp_offset=p * pass_spp, max_depth=depth, film=film,
+                             rows=rows)
+
+                res = run(imp_pass)
+                n_imp = m.count()
+            res["map_seconds"] = round(build_s, 4)
+            res["seconds"] = round(res["seconds"] + build_s, 3)
+            return res | {"particles": particles, "importons": n_imp}
+
         plains, guideds = [], []
         for _ in range(max(1, repeats)):
             plains.append(run(plain_pass))
             guideds.append(guided_run(cfg, plan_spp))
         plain = min(plains, key=lambda r: r["seconds"])
         guided, ginfo = min(guideds, key=lambda r: r[0]["seconds"])
+        importon = [importon_run(n) for n in (100000, 1000000)]
         more = []
         for v in variants:
             v = dict(v)
@@ -474,6 +497,7 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
            "plain": plain, "guided": guided,
            "speedup": round(plain["seconds"] / guided["seconds"], 2),
            "guide": ginfo,
+           "importance_driven": [r | {"speedup": round(plain["seconds"] / r["seconds"], 2)} for r in importon],
            "runs": {"plain_seconds": [r["seconds"] for r in plains],
                     "guided_seconds": [r[0]["seconds"] for r in guideds],
                     "guided_spp": [r[0]["spp"] for r in guideds]},

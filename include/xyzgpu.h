@@ -69,7 +69,22 @@ typedef struct {
    * power spectrum (the reference's basic_spectrum, libhi/hi/image/spectrum.hpp:14). */
   const float *albedo_spd;      /* 31 * n_materials, or NULL */
   float light_power_spd[31];
+  /* Kinds of the non-light materials (NULL: all Lambert): XYZGPU_MATERIAL_*.
+   * MIRROR is the reference's perfect mirror (xyz/bsdf/mirror.cpp: no
+   * next-event estimation, the throughput unchanged, a specular bounce);
+   * METAL its glossy Neumann-Neumann BRDF with a Phong-lobe half vector of
+   * exponent shininess[m], a Schlick-style Fresnel term with F0 = 0.9 and
+   * next-event estimation MIS-weighted against that lobe (xyz/bsdf/metal.cpp
+   * built with CONFIG_EXPLICIT_GLOSSY); its albedo multiplies the throughput as
+   * Lambert's does.  Scenes with MIRROR or METAL render in the XYZ film mode
+   * with xyzgpu_render, xyzgpu_render_noalloc and batches only. */
+  const int32_t *material_kind; /* n_materials, or NULL */
+  const float *shininess;       /* n_materials (METAL exponent), or NULL */
 } xyzgpu_scene_desc;
+
+#define XYZGPU_MATERIAL_LAMBERT 0
+#define XYZGPU_MATERIAL_MIRROR 2
+#define XYZGPU_MATERIAL_METAL 3
 
 /* kd-tree construction parameters (the reference: KDTree(max_bucket = 16,
  * max_depth = 16), SAH without traversal / intersection constants,
@@ -441,6 +456,58 @@ typedef struct {
 } xyzgpu_guide_stats;
 
 int xyzgpu_guide_stats_get(xyzgpu_guide guide, xyzgpu_guide_stats *out);
+
+/* ---- Importance-driven path tracing: the reference's non-learned path guide,
+ * Scene::EvaluteImportanceDrivenPathTracing (xyz/core/
+ * scene_importancedrivenpathtracing.cpp:11-180).  Light particles are traced
+ * first and leave "importons" (hit point, incoming direction) on Lambert
+ * surfaces (Scene::CreateLightImportanceMap, xyz/core/scene_photonmap.cpp:
+ * 272-330); at a path vertex the importons within `radius` give a 16-bin
+ * histogram over (cos^2 theta, phi) about the shading frame, every bin
+ * starting at 16 counts (ImportanceQuery, xyz/core/photonmap.cpp:321-439);
+ * the next direction is drawn from it (the throughput divided by the bin's
+ * density) and next-event estimation's MIS weight uses its density.  As the
+ * variants that act in Lambert-only scenes: importons at every Lambert hit
+ * from bounce min_depth on (the source keeps only those after a specular
+ * bounce), histogram sampling at every Lambert vertex of the first
+ * guide_bounces (the source's "[TEST]" condition; it uses it only after a
+ * specular bounce).  Particle p reads the Philox stream (pixel = p,
+ * sample = 0xffffffff): two draws for the light point, two for a cosine
+ * direction about the light's geometric normal, then per Lambert hit a
+ * roulette draw (survival albedo.y, Lambert::BoundsImportance) and two for the
+ * next cosine direction about the geometric normal.  At a guided vertex the
+ * path reads one draw for the bin and two inside it (after the optional
+ * roulette draw) instead of the two of cosine sampling. */
+typedef struct {
+  int particles;       /* light particles (100,000: CONFIG_EMITED_SIZE, xyz/core/config.hpp:57) */
+  int max_depth;       /* bounces per particle (16: the reference's kMax) */
+  int min_depth;       /* keep importons from this bounce on (1) */
+  float radius;        /* search radius (0.1: CONFIG_SEARCH_RADIUS, config.hpp:56) */
+  uint64_t seed;
+  int guide_bounces;   /* path vertices sampled from the histogram (the first ones); deeper
+                          vertices use cosine sampling (default: all) */
+} xyzgpu_importon_config;
+
+typedef struct xyzgpu_importons_s *xyzgpu_importons;
+
+void xyzgpu_importon_config_default(xyzgpu_importon_config *cfg);
+/* Builds the map of `scene`: traces cfg->particles light particles, or - with
+ * importons != NULL - takes the n_importons given ones (6 floats each:
+ * position, incoming direction; host memory).  Synchronises `stream`. */
+int xyzgpu_importons_create(xyzgpu_scene scene, const xyzgpu_importon_config *cfg, const float *importons,
+                            int64_t n_importons, void *stream, xyzgpu_importons *out);
+void xyzgpu_importons_destroy(xyzgpu_importons map);
+/* Number of importons, and with importons != NULL a host copy (6 floats each,
+ * in the map's cell order). */
+int xyzgpu_importons_get(xyzgpu_importons map, float *importons, int64_t *n);
+/* Histograms for n frames (device, 12 floats each: position, tangent,
+ * binormal, shading normal): hist (device) gets 16 cumulative bin counts per
+ * frame, bins u * 8 + v for u = floor(2 cos^2 theta), v = floor(8 phi / 2 pi). */
+int xyzgpu_importons_query(xyzgpu_importons map, const float *frames, int n, float *hist, void *stream);
+/* As xyzgpu_render (XYZ film mode; profile off or timing, class 5 = the
+ * histogram queries) with the importance-driven estimator. */
+int xyzgpu_render_importon(xyzgpu_importons map, const xyzgpu_camera *camera, const xyzgpu_render_params *rp,
+                           float *film, void *stream);
 
 /* ---- Film output.  Post-processing on the device of a film as xyzgpu_render
  * leaves it (W * H XYZ sums, row 0 at the bottom, device memory), and the

@@ -15,6 +15,7 @@
 // single global mt19937_64 (integrator.cpp:12-25), so that each (pixel, sample)
 // path reads a fixed stream that other implementations can reproduce.
 #include <atomic>
+#include <vector>
 #include <unordered_map>
 
 #define private public
@@ -25,6 +26,8 @@
 #include <bsdf/bsdf.hpp>
 #include <bsdf/lambert.hpp>
 #include <bsdf/light.hpp>
+#include <bsdf/metal.hpp>
+#include <bsdf/mirror.hpp>
 #include <geom/intersection.hpp>
 #include <geom/triangle.hpp>
 
@@ -117,6 +120,17 @@ void xyzref_set_path_params(int kmax, float rr_threshold) {
   xyzref_rr_threshold = rr_threshold;
 }
 
+// Kinds of the next scene's non-light materials: 0 Lambert (default),
+// 2 Mirror (xyz/bsdf/mirror.cpp), 3 Metal with its shininess
+// (xyz/bsdf/metal.cpp, Metal(shininess, albedo)).  Consumed by the next
+// xyzref_scene_create.
+static std::vector<int> g_kind;
+static std::vector<float> g_shininess;
+void xyzref_material_kinds(int nm, const int *kind, const float *shininess) {
+  g_kind.assign(kind, kind + nm);
+  g_shininess.assign(shininess, shininess + nm);
+}
+
 // Builds the scene.  Vertices `pos` (3*nv floats), optional per-vertex shading
 // normals `nrm` (3*nv or NULL), triangles `tri` (3*nt ints) with material ids
 // `tri_mat`; materials carry an XYZ albedo and a light flag.  Lights are
@@ -129,8 +143,14 @@ int xyzref_scene_create(int nv, const float *pos, const float *nrm, int nt,
   ClearScene();
   xyz::Scene &scene = xyz::Scene::GetInstance();
   for (int m = 0; m < nm; ++m) {
+    int const kind = m < static_cast<int>(g_kind.size()) ? g_kind[m] : 0;
+    xyz::float3_t const alb(mat_albedo_xyz[3 * m + 0], mat_albedo_xyz[3 * m + 1], mat_albedo_xyz[3 * m + 2]);
     if (mat_is_light[m]) {
       scene.bsdfs_.push_back(new xyz::Light());
+    } else if (kind == 2) {
+      scene.bsdfs_.push_back(new xyz::Mirror());
+    } else if (kind == 3) {
+      scene.bsdfs_.push_back(new xyz::Metal(g_shininess[m], alb));
     } else {
       scene.bsdfs_.push_back(new xyz::Lambert(xyz::float3_t(
           mat_albedo_xyz[3 * m + 0], mat_albedo_xyz[3 * m + 1],
@@ -167,6 +187,8 @@ int xyzref_scene_create(int nv, const float *pos, const float *nrm, int nt,
       ++nlights;
     }
   }
+  g_kind.clear();
+  g_shininess.clear();
   scene.kdtree_.SetMaxBucketSize(static_cast<std::size_t>(kd_max_bucket));
   scene.kdtree_.SetMaxHierarchyDepth(static_cast<std::size_t>(kd_max_depth));
   scene.Build();
@@ -266,6 +288,58 @@ void xyzref_render(int s0, int spp, std::uint64_t seed, int y0, int y1,
       }
     });
   }
+}
+
+// The named spectra of libhi/hi/image/spectrum.cpp:170-476 (lights, then the
+// Macbeth colour checker), in the order listed by xyzref_spectrum_names.
+const char *xyzref_spectrum_names(void) {
+  return "LightSourceA LightSourceB LightSourceC LightD65 LightD100 LightStandardWarmWhite LightWhite LightStandardWhite LightDaylight LightWarmWhiteDeLuxe LightSoftWhite LightCoolWhiteDeLuxe LightMercuryArcLamp MccDarkSkin MccLightSkin MccBlueSky MccFoliage MccBlueFlower MccBluishGreen MccOrange MccPurplishBlue MccModerateRed MccPurple MccYellowGreen MccOrangeYellow MccBlue MccGreen MccRed MccYellow MccMagenta MccCyan MccWhite MccNeutral80 MccNeutral65 MccNeutral50 MccNeutral35 MccBlack";
+}
+
+int xyzref_named_spectrum(int id, float out[31]) {
+  hi::basic_spectrum const *s = nullptr;
+  switch (id) {
+    case 0: s = &hi::basic_spectrum::LightSourceA(); break;
+    case 1: s = &hi::basic_spectrum::LightSourceB(); break;
+    case 2: s = &hi::basic_spectrum::LightSourceC(); break;
+    case 3: s = &hi::basic_spectrum::LightD65(); break;
+    case 4: s = &hi::basic_spectrum::LightD100(); break;
+    case 5: s = &hi::basic_spectrum::LightStandardWarmWhite(); break;
+    case 6: s = &hi::basic_spectrum::LightWhite(); break;
+    case 7: s = &hi::basic_spectrum::LightStandardWhite(); break;
+    case 8: s = &hi::basic_spectrum::LightDaylight(); break;
+    case 9: s = &hi::basic_spectrum::LightWarmWhiteDeLuxe(); break;
+    case 10: s = &hi::basic_spectrum::LightSoftWhite(); break;
+    case 11: s = &hi::basic_spectrum::LightCoolWhiteDeLuxe(); break;
+    case 12: s = &hi::basic_spectrum::LightMercuryArcLamp(); break;
+    case 13: s = &hi::basic_spectrum::MccDarkSkin(); break;
+    case 14: s = &hi::basic_spectrum::MccLightSkin(); break;
+    case 15: s = &hi::basic_spectrum::MccBlueSky(); break;
+    case 16: s = &hi::basic_spectrum::MccFoliage(); break;
+    case 17: s = &hi::basic_spectrum::MccBlueFlower(); break;
+    case 18: s = &hi::basic_spectrum::MccBluishGreen(); break;
+    case 19: s = &hi::basic_spectrum::MccOrange(); break;
+    case 20: s = &hi::basic_spectrum::MccPurplishBlue(); break;
+    case 21: s = &hi::basic_spectrum::MccModerateRed(); break;
+    case 22: s = &hi::basic_spectrum::MccPurple(); break;
+    case 23: s = &hi::basic_spectrum::MccYellowGreen(); break;
+    case 24: s = &hi::basic_spectrum::MccOrangeYellow(); break;
+    case 25: s = &hi::basic_spectrum::MccBlue(); break;
+    case 26: s = &hi::basic_spectrum::MccGreen(); break;
+    case 27: s = &hi::basic_spectrum::MccRed(); break;
+    case 28: s = &hi::basic_spectrum::MccYellow(); break;
+    case 29: s = &hi::basic_spectrum::MccMagenta(); break;
+    case 30: s = &hi::basic_spectrum::MccCyan(); break;
+    case 31: s = &hi::basic_spectrum::MccWhite(); break;
+    case 32: s = &hi::basic_spectrum::MccNeutral80(); break;
+    case 33: s = &hi::basic_spectrum::MccNeutral65(); break;
+    case 34: s = &hi::basic_spectrum::MccNeutral50(); break;
+    case 35: s = &hi::basic_spectrum::MccNeutral35(); break;
+    case 36: s = &hi::basic_spectrum::MccBlack(); break;
+    default: return -1;
+  }
+  for (int i = 0; i < 31; ++i) out[i] = (*s)[i];
+  return 0;
 }
 
 int xyzref_max_threads(void) {

@@ -8,6 +8,8 @@
 #define GL_BLEND 0
 #define GL_FRONT_AND_BACK 0
 #define GL_AMBIENT_AND_DIFFUSE 0
+#define GL_SPECULAR 0
+#define GL_SHININESS 0
 #define GL_PROJECTION 0
 #define GL_MODELVIEW 0
 #define GL_COMPILE 0

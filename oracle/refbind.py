@@ -163,6 +163,14 @@ class RefLib(_Common):
         pos, tris, mat = _f(sd.positions), _i(sd.tris), _i(sd.tri_mat)
         alb, lit = _f(sd.albedo_xyz), _i(sd.is_light)
         nrm = _f(sd.normals) if sd.normals is not None else None
+        if getattr(sd, "material_kind", None) is not None:
+            # Mirror (2) / Metal (3) materials of the next scene
+            kind = _i(sd.material_kind)
+            shin = _f(sd.shininess if sd.shininess is not None else np.ones(kind.shape[0]))
+            self.lib.xyzref_material_kinds.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+            self.lib.xyzref_material_kinds(kind.shape[0], kind.ctypes.data_as(C.c_void_p),
+                                           shin.ctypes.data_as(C.c_void_p))
+            self._kinds = (kind, shin)
         r = self.lib.xyzref_scene_create(pos.shape[0], pos.ctypes.data_as(C.c_void_p),
                                          None if nrm is None else nrm.ctypes.data_as(C.c_void_p),
                                          tris.shape[0], tris.ctypes.data_as(C.c_void_p),
@@ -178,6 +186,20 @@ class RefLib(_Common):
 
     def max_threads(self):
         return self.lib.xyzref_max_threads()
+
+    def named_spectra(self):
+        """The reference library's named spectra {CamelCaseName: 31 float32}
+        (libhi/hi/image/spectrum.cpp:170-476)."""
+        self.lib.xyzref_spectrum_names.restype = C.c_char_p
+        self.lib.xyzref_named_spectrum.argtypes = [C.c_int, C.c_void_p]
+        names = self.lib.xyzref_spectrum_names().decode().split()
+        out = {}
+        for i, n in enumerate(names):
+            v = np.zeros(31, np.float32)
+            if self.lib.xyzref_named_spectrum(i, v.ctypes.data_as(C.c_void_p)) != 0:
+                raise ValueError(n)
+            out[n] = v
+        return out
 
 
 class PortLib(_Common):
@@ -208,6 +230,10 @@ class PortLib(_Common):
         L.xyzo_scene_set_spectra.argtypes = [C.c_void_p, C.c_void_p]
         L.xyzo_set_spectral.argtypes = [C.c_int, C.c_int]
         L.xyzo_set_materials.argtypes = [C.c_void_p, C.c_void_p]
+        L.xyzo_importons_emit.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_void_p, C.c_int]
+        L.xyzo_importons_emit.restype = C.c_int
+        L.xyzo_importons_set.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_int, C.c_int]
+        L.xyzo_importons_query.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.xyzo_encode_rgbe.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p]
         L.xyzo_tonemap.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float,
                                    C.c_float, C.c_float, C.c_int, C.c_void_p]
@@ -218,6 +244,31 @@ class PortLib(_Common):
 
     def _set_path(self, kmax, rr_threshold, rr_start):
         self.lib.xyzo_set_path_params(kmax, rr_threshold, rr_start)
+
+    def importons_emit(self, particles: int, max_depth: int = 16, min_depth: int = 1, seed: int = 0):
+        """Light-importance map of the importance-driven tracer: (n, 6)
+        float32 importons (position, incoming direction) in particle order."""
+        n = self.lib.xyzo_importons_emit(particles, max_depth, min_depth, C.c_uint64(seed), None, 0)
+        out = np.zeros((max(n, 1), 6), np.float32)
+        self.lib.xyzo_importons_emit(particles, max_depth, min_depth, C.c_uint64(seed),
+                                     out.ctypes.data_as(C.c_void_p), n)
+        return out[:n]
+
+    def importons_set(self, importons, radius: float = 0.1, enable: bool = True, guide_bounces: int = 1 << 30):
+        """Loads a map; with enable the estimator samples Lambert vertices of
+        the first guide_bounces from its histograms."""
+        imp = _f(importons).reshape(-1, 6)
+        self._imp = imp
+        self.lib.xyzo_importons_set(imp.ctypes.data_as(C.c_void_p), imp.shape[0], C.c_float(radius), int(enable),
+                                    int(guide_bounces))
+
+    def importons_query(self, frames):
+        """Cumulative histograms (n, 16) for frames (n, 12): position, tangent,
+        binormal, shading normal."""
+        fr = _f(frames).reshape(-1, 12)
+        out = np.zeros((fr.shape[0], 16), np.float32)
+        self.lib.xyzo_importons_query(fr.ctypes.data_as(C.c_void_p), fr.shape[0], out.ctypes.data_as(C.c_void_p))
+        return out
 
     def encode_rgbe(self, film, scale: float, xyze: bool = False):
         """Pixels of the reference's .hdr writer, (H, W, 4) uint8 in file order."""

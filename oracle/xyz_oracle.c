@@ -460,6 +460,12 @@ static void grad_contrib(const double phi_w[3], int light_m) {
   g->g_em[light_m] += cu;
 }
 
+/* importance-driven mode (defined with the importon map below) */
+#define XYZO_IMP_N 16
+static int IMP_ON, IMP_BOUNCES;
+static void imp_hist(f3 pos, f3 sn, f3 tan, f3 bin, float c[XYZO_IMP_N + 1]);
+static float imp_density(const float c[XYZO_IMP_N + 1], f3 dir, f3 sn, f3 tan, f3 bin);
+
 static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
   xyzo_stream st;
   xyzo_stream_init(&st, seed, (uint32_t)(py * CAM.W + px), (uint32_t)s, 0u);
@@ -566,6 +572,12 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
     }
     if (++k >= KMAX) break;
 
+    /* importance-driven mode: the histogram of this Lambert vertex
+     * (kNN_query, scene_importancedrivenpathtracing.cpp:121-123) */
+    int const imp = IMP_ON && !S.is_light[m] && (int)k - 2 < IMP_BOUNCES;
+    float ic[XYZO_IMP_N + 1];
+    if (imp) imp_hist(pos, fr.sn, fr.tan, fr.bin, ic);
+
     /* NEE (Lambert::CalculateWeightedDirectLighting); a light's NEE is zero
      * and leaves the throughput alone (xyz/bsdf/light.cpp:18-25). */
     if (!S.is_light[m]) {
@@ -583,7 +595,10 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
           rec_seg(lpos, vin, sh, sh >= 0 ? q.tmax : 0.0f, 1);
           if (sh == tri) {
             float const G = nk2 * nk3 / (q.tmax * q.tmax);
-            float const dimp = (float)(XYZO_M_1_PI * (double)G);
+            /* importance-driven: M_1_PI * G * GetDensity (lambert.cpp:210-212) */
+            float const dimp = imp ? (float)(XYZO_M_1_PI * (double)G *
+                                             (double)imp_density(ic, vin, fr.sn, fr.tan, fr.bin))
+                                   : (float)(XYZO_M_1_PI * (double)G);
             float const dexp = 1.0f / A;
             float const dens = dimp / dexp;
             double const w =
@@ -615,6 +630,34 @@ static int eval_path(int px, int py, int s, uint64_t seed, f3 *color) {
 
     /* Light::NextScatteringDirection ends the path (xyz/bsdf/light.cpp:27-31). */
     if (S.is_light[m]) break;
+
+    if (imp) {
+      /* Lambert::NextScatteringDirection with importons (lambert.cpp:243-257)
+       * -> ImportanceQuery::SetDiffusedVector (photonmap.cpp:403-439): a bin
+       * by the cumulative counts, (cos^2 theta, phi) uniform in it; the
+       * throughput is divided by the bin's density. */
+      float const value = ic[XYZO_IMP_N] * xyzo_stream_next(&st);
+      int lo = 0, hi = XYZO_IMP_N + 1; /* upper_bound over c[0..16] */
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (!(value < ic[mid])) lo = mid + 1; else hi = mid;
+      }
+      int const n = lo - 1;
+      int const u = n / 8, v = n % 8;
+      float const mu_u = ((float)u + xyzo_stream_next(&st)) / 2;
+      float const mu_v = ((float)v + xyzo_stream_next(&st)) / 8;
+      float const cos_t = sqrtf(mu_u);
+      float const sin_t = sqrtf(1 - mu_u);
+      float const phi = (float)(2 * XYZO_M_PI) * mu_v;
+      dir = add3(add3(scale3(fr.tan, sin_t * cosf(phi)), scale3(fr.bin, sin_t * sinf(phi))),
+                 scale3(fr.sn, cos_t));
+      float const dens = XYZO_IMP_N * (ic[n + 1] - ic[n]) / ic[XYZO_IMP_N];
+      fSamplingNext = (float)((double)(dens * cos_t) * XYZO_M_1_PI);
+      beta = scale3(beta, 1.0f / dens);
+      specular = 0;
+      if (!(dot3(dir, fr.gn) > 0)) break;
+      continue;
+    }
 
     /* Lambert::NextScatteringDirection: fMuPhi = first draw, fMuTheta = second */
     float const mu_phi = xyzo_stream_next(&st);
@@ -1269,5 +1312,246 @@ void xyzo_tonemap(const float *film, int W, int H, float scale, int op, float ex
     o[2] = tone_one(c[0], op, exposure, white, gamma);
     o[1] = tone_one(c[1], op, exposure, white, gamma);
     o[0] = tone_one(c[2], op, exposure, white, gamma);
+  }
+}
+
+/* ------------------------------------------------ importance-driven tracing
+ * The reference's importance-driven path tracer (Scene::
+ * EvaluteImportanceDrivenPathTracing, xyz/core/scene_importancedrivenpathtracing
+ * .cpp:11-180) with its light-importance map (Scene::CreateLightImportanceMap,
+ * xyz/core/scene_photonmap.cpp:272-330) and histogram guide (ImportanceQuery,
+ * xyz/core/photonmap.cpp:321-494), as the variants that act in scenes of
+ * Lambert surfaces only: importons are kept at every Lambert hit from bounce
+ * `min_depth` on (the source's commented `depth > 0` test; its active test
+ * also wants a specular bounce first) and the histogram guides every Lambert
+ * vertex of the first `guide_bounces` (the source's "[TEST]" condition).
+ *
+ * Particle p reads the Philox stream (pixel = p, sample = 0xffffffff): two
+ * draws for the light point (as SampleLightPosition), two for a cosine
+ * direction about the light's geometric normal, then per Lambert hit one
+ * roulette draw (survival albedo.y, Lambert::BoundsImportance,
+ * xyz/bsdf/lambert.cpp:16-42) and two for the next cosine direction about the
+ * hit's geometric normal. */
+#define XYZO_IMP_U 2  /* CONFIG_U_SIZE (photonmap.hpp:9) */
+#define XYZO_IMP_V 8  /* CONFIG_V_SIZE (photonmap.hpp:10); XYZO_IMP_N = U * V */
+
+static float *IMP_P = NULL, *IMP_D = NULL; /* 3 floats each per importon */
+static int IMP_N = 0;
+static float IMP_R2 = 0.01f;               /* CONFIG_SEARCH_RADIUS^2 in float */
+/* uniform grid over the importons (any structure finds the same set) */
+static f3 IMP_LO;
+static float IMP_CS = 1.0f;
+static int IMP_G[3] = {1, 1, 1};
+static int *IMP_START = NULL, *IMP_IDX = NULL;
+
+/* Light point from two draws (SampleLightPosition + Triangle::Sample). */
+static void light_point(float lt, float ls, f3 *pos, f3 *sn, f3 *gn, int *mat) {
+  float const u = ls * S.cdf[S.nl];
+  int lo = 0, hi = S.nl + 1;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (!(u < S.cdf[mid])) lo = mid + 1; else hi = mid;
+  }
+  int const n = lo - 1;
+  float const v = (u - S.cdf[n]) / (S.cdf[n + 1] - S.cdf[n]);
+  int const li = S.lights[n];
+  float const ss = sqrtf(v);
+  float const uu = ss * (1 - lt), vv = ss * lt;
+  *pos = add3(add3(S.v0[li], scale3(S.e1[li], uu)), scale3(S.e2[li], vv));
+  *sn = normalize3(add3(add3(S.n0[li], scale3(S.s1[li], uu)), scale3(S.s2[li], vv)));
+  *gn = S.ng[li];
+  *mat = S.mat[li];
+}
+
+/* Tangent frame about a normal as Triangle::GeometricBasis builds it
+ * (xyz/geom/triangle.cpp:181-191). */
+static void frame_about(f3 n, f3 *t, f3 *b) {
+  f3 tt = mk(-n.z, 0, n.x);
+  float const l2 = dot3(tt, tt);
+  if (l2 > 0) {
+    tt = scale3(tt, 1.0f / sqrtf(l2));
+    *b = cross3(tt, n);
+  } else {
+    *b = mk(0, 0, (n.y > 0) ? 1.0f : -1.0f);
+    tt = cross3(n, *b);
+  }
+  *t = tt;
+}
+
+static f3 cosine_dir(f3 t, f3 b, f3 n, float mu_phi, float mu_theta) {
+  float const phi = (float)(2 * XYZO_M_PI) * mu_phi;
+  float const cos_t = sqrtf(mu_theta), sin_t = sqrtf(1 - mu_theta);
+  return add3(add3(scale3(t, sin_t * cosf(phi)), scale3(b, sin_t * sinf(phi))), scale3(n, cos_t));
+}
+
+/* Emits `particles` light particles; writes up to `cap` importons (position,
+ * incoming direction: 6 floats each) in particle order, returns how many
+ * there are in all. */
+int xyzo_importons_emit(int particles, int max_depth, int min_depth, uint64_t seed, float *out, int cap) {
+  int count = 0;
+  if (S.nl <= 0) return 0;
+  for (int pi = 0; pi < particles; ++pi) {
+    xyzo_stream st;
+    xyzo_stream_init(&st, seed, (uint32_t)pi, 0xffffffffu, 0u);
+    float const lt = xyzo_stream_next(&st);
+    float const ls = xyzo_stream_next(&st);
+    f3 pos, lsn, lgn, t, b;
+    int lmat;
+    light_point(lt, ls, &pos, &lsn, &lgn, &lmat);
+    frame_about(lgn, &t, &b);
+    float const mp = xyzo_stream_next(&st);
+    float const mt = xyzo_stream_next(&st);
+    f3 dir = cosine_dir(t, b, lgn, mp, mt);
+    for (int depth = 0; depth < max_depth; ++depth) {
+      isect_t p;
+      int const tri = find_intersection(pos, dir, &p);
+      if (tri < 0) break;
+      int const m = S.mat[tri];
+      if (S.is_light[m]) break; /* Light::BoundsImportance */
+      f3 sn = normalize3(add3(add3(S.n0[tri], scale3(S.s1[tri], p.f)), scale3(S.s2[tri], p.g)));
+      f3 gn = S.ng[tri];
+      if (p.back) {
+        gn = neg3(gn);
+        sn = neg3(sn);
+      }
+      pos = add3(pos, scale3(dir, p.tmax));
+      if (depth >= min_depth) {
+        if (count < cap) {
+          float *o = out + 6 * (size_t)count;
+          o[0] = pos.x, o[1] = pos.y, o[2] = pos.z, o[3] = dir.x, o[4] = dir.y, o[5] = dir.z;
+        }
+        ++count;
+      }
+      if (-dot3(dir, sn) <= 0) break;
+      if (xyzo_stream_next(&st) >= S.albedo[m].y) break;
+      frame_about(gn, &t, &b);
+      float const a = xyzo_stream_next(&st);
+      float const c = xyzo_stream_next(&st);
+      dir = cosine_dir(t, b, gn, a, c);
+    }
+  }
+  return count;
+}
+
+static int imp_cell(float v, int k) {
+  int c = (int)floorf((v - at3(IMP_LO, k)) / IMP_CS);
+  return c < 0 ? 0 : (c >= IMP_G[k] ? IMP_G[k] - 1 : c);
+}
+
+/* Loads an importon map (6 floats per importon) with search radius r. */
+void xyzo_importons_set(const float *pd, int n, float radius, int enable, int guide_bounces) {
+  free(IMP_P);
+  free(IMP_D);
+  free(IMP_START);
+  free(IMP_IDX);
+  IMP_P = (float *)malloc(sizeof(float) * 3 * (size_t)(n > 0 ? n : 1));
+  IMP_D = (float *)malloc(sizeof(float) * 3 * (size_t)(n > 0 ? n : 1));
+  IMP_N = n;
+  IMP_R2 = radius * radius;
+  IMP_ON = enable;
+  IMP_BOUNCES = guide_bounces;
+  f3 lo = mk(INFINITY, INFINITY, INFINITY), hi = mk(-INFINITY, -INFINITY, -INFINITY);
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) {
+      IMP_P[3 * i + k] = pd[6 * i + k];
+      IMP_D[3 * i + k] = pd[6 * i + 3 + k];
+    }
+    lo = mk(fminf(lo.x, pd[6 * i]), fminf(lo.y, pd[6 * i + 1]), fminf(lo.z, pd[6 * i + 2]));
+    hi = mk(fmaxf(hi.x, pd[6 * i]), fmaxf(hi.y, pd[6 * i + 1]), fmaxf(hi.z, pd[6 * i + 2]));
+  }
+  if (n == 0) lo = hi = mk(0, 0, 0);
+  IMP_LO = lo;
+  IMP_CS = radius > 0 ? radius : 1.0f;
+  size_t cells = 1;
+  for (int k = 0; k < 3; ++k) {
+    IMP_G[k] = (int)((at3(hi, k) - at3(lo, k)) / IMP_CS) + 1;
+    if (IMP_G[k] > 1024) IMP_G[k] = 1024;
+    cells *= (size_t)IMP_G[k];
+  }
+  if (cells > ((size_t)1 << 24)) { /* coarser cells for very spread maps */
+    IMP_CS *= cbrtf((float)cells / (float)(1 << 24)) + 1.0f;
+    cells = 1;
+    for (int k = 0; k < 3; ++k) {
+      IMP_G[k] = (int)((at3(hi, k) - at3(lo, k)) / IMP_CS) + 1;
+      cells *= (size_t)IMP_G[k];
+    }
+  }
+  IMP_START = (int *)calloc(cells + 1, sizeof(int));
+  IMP_IDX = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  int *key = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  for (int i = 0; i < n; ++i) {
+    key[i] = (imp_cell(IMP_P[3 * i + 2], 2) * IMP_G[1] + imp_cell(IMP_P[3 * i + 1], 1)) * IMP_G[0] +
+             imp_cell(IMP_P[3 * i], 0);
+    IMP_START[key[i] + 1]++;
+  }
+  for (size_t c = 0; c < cells; ++c) IMP_START[c + 1] += IMP_START[c];
+  int *fill = (int *)malloc(sizeof(int) * (cells + 1));
+  memcpy(fill, IMP_START, sizeof(int) * (cells + 1));
+  for (int i = 0; i < n; ++i) IMP_IDX[fill[key[i]]++] = i;
+  free(fill);
+  free(key);
+}
+
+/* ImportanceQuery over a fixed-radius neighbourhood (begin_query, push_back,
+ * end_query: photonmap.cpp:321-373): 16 (cos^2 theta, phi) bins that start at
+ * 16 counts each, one count per importon within the radius whose direction
+ * arrives from above the shading normal and whose point, moved along that
+ * direction onto the tangent plane, is within the radius; c[0] = 0 and c[i]
+ * the cumulative counts. */
+static void imp_hist(f3 pos, f3 sn, f3 tan, f3 bin, float c[XYZO_IMP_N + 1]) {
+  c[0] = 0;
+  for (int i = 1; i <= XYZO_IMP_N; ++i) c[i] = (float)XYZO_IMP_N;
+  int lo[3], hi[3];
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = imp_cell(at3(pos, k) - IMP_CS, k);
+    hi[k] = imp_cell(at3(pos, k) + IMP_CS, k);
+  }
+  for (int z = lo[2]; z <= hi[2]; ++z)
+    for (int y = lo[1]; y <= hi[1]; ++y)
+      for (int x = lo[0]; x <= hi[0]; ++x) {
+        int const cell = (z * IMP_G[1] + y) * IMP_G[0] + x;
+        for (int q = IMP_START[cell]; q < IMP_START[cell + 1]; ++q) {
+          int const j = IMP_IDX[q];
+          f3 const d = mk(IMP_P[3 * j] - pos.x, IMP_P[3 * j + 1] - pos.y, IMP_P[3 * j + 2] - pos.z);
+          if (!(dot3(d, d) < IMP_R2)) continue;
+          f3 const dir = mk(IMP_D[3 * j], IMP_D[3 * j + 1], IMP_D[3 * j + 2]);
+          float const cs = -dot3(dir, sn);
+          if (cs <= 0) continue;
+          f3 const vp = add3(d, scale3(dir, dot3(d, sn)));
+          if (dot3(vp, vp) >= IMP_R2) continue;
+          int u = (int)(cs * cs * XYZO_IMP_U);
+          if (u >= XYZO_IMP_U) u = XYZO_IMP_U - 1;
+          float phi = 0.5f * atan2f(-dot3(dir, bin), -dot3(dir, tan));
+          if (phi < 0) phi = (float)((double)phi + XYZO_M_PI);
+          int v = (int)((double)phi * (XYZO_IMP_V * XYZO_M_1_PI));
+          if (v >= XYZO_IMP_V) v = XYZO_IMP_V - 1;
+          c[1 + u * XYZO_IMP_V + v] += 1;
+        }
+      }
+  for (int i = 2; i <= XYZO_IMP_N; ++i) c[i] += c[i - 1];
+}
+
+/* ImportanceQuery::GetDensity (photonmap.cpp:375-401). */
+static float imp_density(const float c[XYZO_IMP_N + 1], f3 dir, f3 sn, f3 tan, f3 bin) {
+  float const cs = -dot3(dir, sn);
+  if (cs <= 0) return 0.0f;
+  int u = (int)(cs * cs * XYZO_IMP_U);
+  if (u >= XYZO_IMP_U) u = XYZO_IMP_U - 1;
+  float phi = 0.5f * atan2f(-dot3(dir, bin), -dot3(dir, tan));
+  if (phi < 0) phi = (float)((double)phi + XYZO_M_PI);
+  int v = (int)((double)phi * (XYZO_IMP_V * XYZO_M_1_PI));
+  if (v >= XYZO_IMP_V) v = XYZO_IMP_V - 1;
+  int const n = u * XYZO_IMP_V + v;
+  return XYZO_IMP_N * (c[n + 1] - c[n]) / c[XYZO_IMP_N];
+}
+
+/* Histograms (16 cumulative counts c[1..16]) for n frames given as 12 floats:
+ * position, tangent, binormal, shading normal. */
+void xyzo_importons_query(const float *fr, int n, float *out) {
+  for (int i = 0; i < n; ++i) {
+    const float *q = fr + 12 * (size_t)i;
+    float c[XYZO_IMP_N + 1];
+    imp_hist(mk(q[0], q[1], q[2]), mk(q[9], q[10], q[11]), mk(q[3], q[4], q[5]), mk(q[6], q[7], q[8]), c);
+    memcpy(out + XYZO_IMP_N * (size_t)i, c + 1, sizeof(float) * XYZO_IMP_N);
   }
 }

@@ -1,0 +1,113 @@
+"""Importance-driven path tracing on the GPU (xyzgpu_importons_*,
+xyzgpu_render_importon) against the oracle's restatement of the reference's
+Scene::EvaluteImportanceDrivenPathTracing, its light-importance map
+(Scene::CreateLightImportanceMap) and ImportanceQuery histograms."""
+
+import numpy as np
+import pytest
+
+from tests.helpers import ensure_port
+
+pytestmark = pytest.mark.gpu
+
+
+def _sorted_rows(a):
+    return a[np.lexsort(a.T[::-1])]
+
+
+def _cornell_port(sd, W=48, H=36, depth=8):
+    P = ensure_port()
+    P.set_spectral(0, 1)
+    P.scene_create(sd)
+    P.set_camera(sd.camera, W, H)
+    P.set_path_params(max_depth=depth)
+    return P
+
+
+def test_light_particles_leave_the_oracles_importons():
+    """Same Philox streams per particle: the same importons (the map holds
+    them in cell order, so the sets are compared)."""
+    from xyz_b200 import api, scenes
+    for sd in (scenes.cornell_box(), scenes.spheres_scene(level=3, n_spheres=2, seed=1)):
+        P = _cornell_port(sd)
+        want = P.importons_emit(20000, 16, 1, seed=7)
+        with api.Scene(sd) as s, api.Importons(s, particles=20000, seed=7) as m:
+            got = m.importons()
+        assert got.shape[0] > 1000
+        # a particle whose ray grazes an edge may take another path in either
+        # implementation; nearly all importons are identical
+        a, b = _sorted_rows(got), _sorted_rows(want)
+        common = np.intersect1d(a.view([("", np.float32)] * 6).ravel(), b.view([("", np.float32)] * 6).ravel())
+        assert common.shape[0] >= 0.99 * max(a.shape[0], b.shape[0])
+
+
+def test_histograms_equal_the_oracles():
+    import torch
+    from xyz_b200 import api, scenes
+    sd = scenes.cornell_box()
+    P = _cornell_port(sd)
+    imp = P.importons_emit(30000, 16, 1, seed=3)
+    P.importons_set(imp, 0.1, enable=False)
+    rng = np.random.default_rng(4)
+    n = 4000
+    pos = imp[rng.integers(0, imp.shape[0], n), :3] + rng.normal(scale=0.03, size=(n, 3)).astype(np.float32)
+    nrm = rng.normal(size=(n, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    t = np.stack([-nrm[:, 2], np.zeros(n), nrm[:, 0]], axis=1)
+    t /= np.linalg.norm(t, axis=1, keepdims=True)
+    fr = np.concatenate([pos, t, np.cross(t, nrm), nrm], axis=1).astype(np.float32)
+    want = P.importons_query(fr)
+    with api.Scene(sd) as s, api.Importons(s, importons=imp) as m:
+        assert m.count() == imp.shape[0]
+        got = m.query(torch.from_numpy(fr).cuda()).cpu().numpy()
+    assert (got[:, -1] == want[:, -1]).all()
+    # the bin of an importon on a bin edge depends on the last bit of atan2f
+    assert (got == want).all(axis=1).mean() >= 0.99
+    assert (want[:, -1] > 256).mean() > 0.5
+
+
+def test_render_matches_the_oracle_on_the_same_streams_and_map():
+    from xyz_b200 import api, scenes
+    sd = scenes.cornell_box()
+    W, H, spp, seed = 48, 36, 4, 12
+    P = _cornell_port(sd, W, H)
+    imp = P.importons_emit(50000, 16, 1, seed=9)
+    try:
+        P.importons_set(imp, 0.1, enable=True)
+        ref = P.render(spp, seed=seed, nthreads=0)
+    finally:
+        P.importons_set(imp, 0.1, enable=False)
+    with api.Scene(sd) as s, api.Importons(s, importons=imp) as m:
+        film = m.render(sd.camera, W, H, spp, seed=seed, max_depth=8).cpu().numpy()
+    close = (np.abs(film - ref) <= 1e-6 + 1e-4 * np.abs(ref)).all(axis=-1).mean()
+    assert close >= 0.98, close
+    assert abs(film.sum() - ref.sum()) / ref.sum() < 2e-2
+
+
+def test_render_is_unbiased_against_the_plain_tracer():
+    import torch
+    from xyz_b200 import api, scenes
+    sd = scenes.cornell_box()
+    W, H, spp = 64, 48, 512
+    with api.Scene(sd) as s, api.Importons(s, particles=100000, seed=1) as m:
+        a = s.render(sd.camera, W, H, spp, seed=21, max_depth=8).double() / spp
+        b = m.render(sd.camera, W, H, spp, seed=22, max_depth=8).double() / spp
+        c = m.render(sd.camera, W, H, spp, seed=22, max_depth=8, wave_paths=50000).double() / spp
+        torch.cuda.synchronize()
+    assert torch.equal(b, c)               # per-path results do not depend on the wave
+    assert abs(float(b.mean() / a.mean()) - 1.0) < 0.01
+    ba = a.reshape(6, 8, 8, 8, 3).mean(dim=(1, 3))
+    bb = b.reshape(6, 8, 8, 8, 3).mean(dim=(1, 3))
+    assert float((bb / ba - 1.0).abs().max()) < 0.05
+
+
+def test_importon_arguments():
+    from xyz_b200 import api, scenes
+    sd = scenes.cornell_box()
+    with api.Scene(sd) as s:
+        with pytest.raises(api.XyzGpuError):
+            api.Importons(s, radius=0.0)
+        with api.Importons(s, particles=0) as m:
+            assert m.count() == 0
+            f = m.render(sd.camera, 16, 12, 2, seed=1, max_depth=6)   # empty map: prior-only histograms
+            assert float(f.sum()) > 0

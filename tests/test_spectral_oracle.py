@@ -70,3 +70,19 @@ def test_spectral_port_binned_one_hero_is_unbiased_against_xyz_for_grey_scenes()
     white = spectrum.ccir601_rgb_to_xyz((1, 1, 1)).astype(np.float64)
     ratio = spec / xyz
     assert np.all(np.abs(ratio - 1.0) < 0.25), ratio
+
+
+def test_named_spectra_are_the_reference_tables():
+    """xyz_b200.spectrum.NAMED_SPECTRA (illuminants and the Macbeth
+    ColorChecker) against the reference's own tables, read from its build."""
+    import re
+    from tests.helpers import ref_lib
+    from xyz_b200 import spectrum
+    R = ref_lib(True)
+    if R is None:
+        pytest.skip("reference oracle not built (make -C oracle)")
+    ref = R.named_spectra()
+    assert len(ref) == len(spectrum.NAMED_SPECTRA) == 37
+    for name, v in ref.items():
+        mine = spectrum.named_spectrum(re.sub(r"(?<!^)(?=[A-Z])", "_", name).lower())
+        assert np.array_equal(mine, v), name

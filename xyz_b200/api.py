@@ -41,7 +41,9 @@ EXPORTED = [
     "xyzgpu_guide_gradient", "xyzgpu_guide_train_step", "xyzgpu_render_guided", "xyzgpu_guide_stats_get",
     "xyzgpu_guide_reserve", "xyzgpu_film_encode_rgbe", "xyzgpu_hdr_write", "xyzgpu_tonemap_params_default",
     "xyzgpu_film_tonemap", "xyzgpu_bmp_write", "xyzgpu_checkpoint_save", "xyzgpu_checkpoint_load",
-    "xyzgpu_film_save_hdr", "xyzgpu_film_save_bmp",
+    "xyzgpu_film_save_hdr", "xyzgpu_film_save_bmp", "xyzgpu_importon_config_default",
+    "xyzgpu_importons_create", "xyzgpu_importons_destroy", "xyzgpu_importons_get", "xyzgpu_importons_query",
+    "xyzgpu_render_importon",
 ]
 
 
@@ -56,7 +58,10 @@ class SceneDesc(C.Structure):
                 ("triangles", C.c_void_p), ("tri_material", C.c_void_p), ("n_triangles", C.c_int),
                 ("albedo_xyz", C.c_void_p), ("is_light", C.c_void_p), ("n_materials", C.c_int),
                 ("light_power_xyz", C.c_float * 3), ("albedo_spd", C.c_void_p),
-                ("light_power_spd", C.c_float * 31)]
+                ("light_power_spd", C.c_float * 31), ("material_kind", C.c_void_p), ("shininess", C.c_void_p)]
+
+
+MATERIAL_LAMBERT, MATERIAL_MIRROR, MATERIAL_METAL = 0, 2, 3
 
 
 class BuildParams(C.Structure):
@@ -105,6 +110,11 @@ class GuideConfig(C.Structure):
 
 class GuideStats(C.Structure):
     _fields_ = [("adam_steps", C.c_uint64), ("trained_records", C.c_uint64)]
+
+
+class ImportonConfig(C.Structure):
+    _fields_ = [("particles", C.c_int), ("max_depth", C.c_int), ("min_depth", C.c_int), ("radius", C.c_float),
+                ("seed", C.c_uint64), ("guide_bounces", C.c_int)]
 
 
 class TonemapParams(C.Structure):
@@ -203,6 +213,14 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                        C.c_void_p, C.c_void_p]
     L.xyzgpu_guide_stats_get.argtypes = [C.c_void_p, C.POINTER(GuideStats)]
     L.xyzgpu_guide_reserve.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+    L.xyzgpu_importon_config_default.argtypes = [C.POINTER(ImportonConfig)]
+    L.xyzgpu_importons_create.argtypes = [C.c_void_p, C.POINTER(ImportonConfig), C.c_void_p, C.c_int64, C.c_void_p,
+                                          C.POINTER(C.c_void_p)]
+    L.xyzgpu_importons_destroy.argtypes = [C.c_void_p]
+    L.xyzgpu_importons_get.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]
+    L.xyzgpu_importons_query.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.xyzgpu_render_importon.argtypes = [C.c_void_p, C.POINTER(CameraDesc), C.POINTER(RenderParams), C.c_void_p,
+                                         C.c_void_p]
     L.xyzgpu_film_encode_rgbe.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
     L.xyzgpu_hdr_write.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
     L.xyzgpu_tonemap_params_default.argtypes = [C.POINTER(TonemapParams)]
@@ -304,6 +322,10 @@ class Scene:
             d.albedo_spd = keep(sd.albedo_spd, np.float32)
             for k in range(31):
                 d.light_power_spd[k] = float(sd.light_power_spd[k])
+        if getattr(sd, "material_kind", None) is not None:
+            d.material_kind = keep(sd.material_kind, np.int32)
+            d.shininess = keep(sd.shininess if sd.shininess is not None
+                               else np.ones(d.n_materials, np.float32), np.float32)
         bp = default_build_params(**build_kw)
         h = C.c_void_p()
         _check(L.xyzgpu_scene_create(C.byref(d), C.byref(bp), C.byref(h)))
@@ -496,6 +518,82 @@ class Scene:
         _check(_LIB.xyzgpu_adjoint(self.handle, C.byref(cam), C.byref(rp), d_film.data_ptr(),
                                    d_albedo.data_ptr(), d_emission.data_ptr(), _stream_ptr(stream)))
         return d_albedo, d_emission
+
+
+# ------------------------------------------------------------------ importance-driven tracing
+class Importons:
+    """xyzgpu_importons: the light-importance map of the reference's
+    importance-driven path tracer, built by tracing light particles (or from
+    given importons, an (n, 6) array of position and incoming direction)."""
+
+    def __init__(self, scene: "Scene", importons=None, stream=None, **config):
+        L = load_library()
+        cfg = ImportonConfig()
+        L.xyzgpu_importon_config_default(C.byref(cfg))
+        for k, v in config.items():
+            setattr(cfg, k, v)
+        h = C.c_void_p()
+        ptr, n = None, 0
+        if importons is not None:
+            arr = np.ascontiguousarray(importons, np.float32).reshape(-1, 6)
+            ptr, n = arr.ctypes.data, arr.shape[0]
+        _check(L.xyzgpu_importons_create(scene.handle, C.byref(cfg), ptr, n, _stream_ptr(stream), C.byref(h)))
+        self.handle = h
+        self.scene = scene
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _LIB.xyzgpu_importons_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def count(self) -> int:
+        n = C.c_int64()
+        _check(_LIB.xyzgpu_importons_get(self.handle, None, C.byref(n)))
+        return n.value
+
+    def importons(self) -> np.ndarray:
+        n = self.count()
+        out = np.zeros((max(n, 1), 6), np.float32)
+        k = C.c_int64()
+        _check(_LIB.xyzgpu_importons_get(self.handle, out.ctypes.data, C.byref(k)))
+        return out[:n]
+
+    def query(self, frames, stream=None):
+        """frames: CUDA float32 (n, 12) -> cumulative histograms (n, 16)."""
+        import torch
+        n = int(frames.shape[0])
+        out = torch.empty((n, 16), dtype=torch.float32, device=frames.device)
+        _check(_LIB.xyzgpu_importons_query(self.handle, frames.contiguous().data_ptr(), n, out.data_ptr(),
+                                           _stream_ptr(stream)))
+        return out
+
+    def render(self, camera, width: int, height: int, spp: int, *, seed: int = 0, spp_offset: int = 0,
+               max_depth: int = 15, rr_start_depth: int = 1, rr_threshold: float = 0.2, film=None,
+               accumulate: bool = False, wave_paths: int = 0, rows=None, profile: int = 0, stream=None):
+        """xyzgpu_render_importon into a CUDA film (H, W, 3) of sums."""
+        import torch
+        if film is None:
+            film = torch.zeros((height, width, 3), dtype=torch.float32, device="cuda")
+        cam = camera_desc(camera)
+        rp = render_params(width, height, spp, seed=seed, spp_offset=spp_offset, max_depth=max_depth,
+                           rr_start_depth=rr_start_depth, rr_threshold=rr_threshold, accumulate=accumulate,
+                           wave_paths=wave_paths, profile=profile, rows=rows)
+        rp.film_location = XYZGPU_FILM_DEVICE
+        _check(_LIB.xyzgpu_render_importon(self.handle, C.byref(cam), C.byref(rp), film.data_ptr(),
+                                           _stream_ptr(stream)))
+        return film
 
 
 # ------------------------------------------------------------------ film output

@@ -83,7 +83,7 @@ void free_scene(SceneImpl *s) {
   // work queued on any stream that still reads the scene finishes first
   cudaDeviceSynchronize();
   render_workspace_free(s->ws);
-  void *bufs[] = {s->d_tri, s->d_ng, s->d_sn, s->d_mat, s->d_emission, s->d_lights, s->d_cdf, s->d_spd,
+  void *bufs[] = {s->d_tri, s->d_ng, s->d_sn, s->d_mat, s->d_shininess, s->d_emission, s->d_lights, s->d_cdf, s->d_spd,
                   s->d_nodes, s->d_refs, s->d_fetch, s->d_trace_counts};
   for (void *b : bufs)
     if (b) cudaFreeAsync(b, nullptr);
@@ -286,9 +286,25 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   std::vector<int32_t> lights;
   std::vector<float> cdf(1, 0.0f);
   bool const smooth = d->normals != nullptr;
+  std::vector<float> shin(mat.size(), 1.0f);
+  int n_specular = 0;
   for (int m = 0; m < nm; ++m) {
-    mat[m] = make_float4(d->albedo_xyz[3 * m], d->albedo_xyz[3 * m + 1], d->albedo_xyz[3 * m + 2],
-                         d->is_light[m] ? 1.0f : 0.0f);
+    int const kind = d->material_kind ? d->material_kind[m] : XYZGPU_MATERIAL_LAMBERT;
+    if (kind != XYZGPU_MATERIAL_LAMBERT && kind != XYZGPU_MATERIAL_MIRROR && kind != XYZGPU_MATERIAL_METAL)
+      return set_error(XYZGPU_E_INVALID, "scene_create: material %d has unknown kind %d", m, kind);
+    float kw = 0.0f;
+    if (d->is_light[m]) {
+      kw = 1.0f;
+    } else if (kind != XYZGPU_MATERIAL_LAMBERT) {
+      kw = static_cast<float>(kind);
+      ++n_specular;
+    }
+    if (kind == XYZGPU_MATERIAL_METAL && !d->is_light[m]) {
+      if (!d->shininess || !(d->shininess[m] > 0.0f) || !std::isfinite(d->shininess[m]))
+        return set_error(XYZGPU_E_INVALID, "scene_create: metal material %d needs a shininess > 0", m);
+      shin[m] = d->shininess[m];
+    }
+    mat[m] = make_float4(d->albedo_xyz[3 * m], d->albedo_xyz[3 * m + 1], d->albedo_xyz[3 * m + 2], kw);
   }
   for (int i = 0; i < nt; ++i) {
     int32_t const a = d->triangles[3 * i], b = d->triangles[3 * i + 1], c = d->triangles[3 * i + 2];
@@ -316,6 +332,7 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   s->n_tris = nt;
   s->n_lights = static_cast<int>(lights.size());
   s->n_materials = nm;
+  s->n_specular = n_specular;
   s->smooth = smooth;
   configure_pool(dev);
   cudaStream_t const st = nullptr;
@@ -344,6 +361,7 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   XYZ_TRY(dev_alloc(&s->d_ng, static_cast<size_t>(nt), &bytes, st));
   if (smooth) XYZ_TRY(dev_alloc(&s->d_sn, 3 * static_cast<size_t>(nt), &bytes, st));
   XYZ_TRY(dev_upload(&s->d_mat, mat.data(), mat.size(), &bytes, st));
+  XYZ_TRY(dev_upload(&s->d_shininess, shin.data(), shin.size(), &bytes, st));
   {
     std::vector<float> ones(mat.size(), 1.0f);
     XYZ_TRY(dev_upload(&s->d_emission, ones.data(), ones.size(), &bytes, st));
@@ -464,6 +482,11 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   v.tri_ng = s->d_ng;
   v.tri_sn = s->d_sn;
   v.mat = s->d_mat;
+  v.shininess = s->d_shininess;
+  v.has_metal = 0;
+  if (d->material_kind)
+    for (int m = 0; m < nm; ++m)
+      if (!d->is_light[m] && d->material_kind[m] == XYZGPU_MATERIAL_METAL) v.has_metal = 1;
   v.emission = s->d_emission;
   v.lights = s->d_lights;
   v.cdf = s->d_cdf;
@@ -540,8 +563,10 @@ int xyzgpu_trace_closest_counted(xyzgpu_scene scene, const float *rays, int n, f
                           static_cast<cudaStream_t>(stream), counters);
 }
 
-namespace {
-// Checks shared by xyzgpu_render and xyzgpu_adjoint.
+}  // extern "C"
+
+namespace xyzgpu {
+// Checks shared by xyzgpu_render, xyzgpu_adjoint and xyzgpu_render_importon.
 int check_render_args(const char *who, xyzgpu_scene scene, const xyzgpu_camera *cam,
                       const xyzgpu_render_params *rp) {
   if (rp->width <= 0 || rp->height <= 0 || rp->spp < 0 || rp->spp_offset < 0 ||
@@ -564,11 +589,15 @@ int check_render_args(const char *who, xyzgpu_scene scene, const xyzgpu_camera *
       return set_error(XYZGPU_E_INVALID, "%s: camera position is not finite", who);
   if (!(cam->film_size > 0) || !(cam->focal_length > 0) || !(cam->f_number > 0))
     return set_error(XYZGPU_E_INVALID, "%s: camera film size, focal length and F-number must be > 0", who);
+  if (rp->spectral && reinterpret_cast<SceneImpl *>(scene)->n_specular)
+    return set_error(XYZGPU_E_INVALID, "%s: mirror and metal materials render in the XYZ film mode only", who);
   if (rp->spectral && !reinterpret_cast<SceneImpl *>(scene)->d_spd)
     return set_error(XYZGPU_E_INVALID, "%s: the spectral film modes need albedo spectra in the scene", who);
   return XYZGPU_OK;
 }
-}  // namespace
+}  // namespace xyzgpu
+
+extern "C" {
 
 int xyzgpu_render(xyzgpu_scene scene, const xyzgpu_camera *cam, const xyzgpu_render_params *rp,
                   float *film, void *stream) {
@@ -589,6 +618,8 @@ int xyzgpu_adjoint(xyzgpu_scene scene, const xyzgpu_camera *cam, const xyzgpu_re
   if (rc) return rc;
   if (rp->spectral != XYZGPU_SPECTRAL_OFF)
     return set_error(XYZGPU_E_INVALID, "adjoint: only the XYZ film mode is differentiated");
+  if (reinterpret_cast<SceneImpl *>(scene)->n_specular)
+    return set_error(XYZGPU_E_INVALID, "adjoint: scenes with mirror or metal materials are not differentiated");
   if (rp->profile != XYZGPU_PROFILE_OFF)
     return set_error(XYZGPU_E_INVALID, "adjoint: profiling is not supported");
   if ((reinterpret_cast<uintptr_t>(d_film) | reinterpret_cast<uintptr_t>(d_albedo) |

@@ -182,6 +182,7 @@ int issue(Batch &b, cudaStream_t st, const std::vector<float *> &films, bool cle
   A.s_o = wv.s_o;
   A.s_d = wv.s_d;
   A.s_pb = wv.s_pb;
+  A.s_m = wv.s_m;
   A.s_target = wv.s_target;
   A.counts = wv.counts;
   A.fsn = wv.fsn;

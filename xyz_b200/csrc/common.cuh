@@ -109,7 +109,9 @@ struct DevScene {
   const float4 *tri;      // 3 per triangle: (v0, n.x) (e1, n.y) (e2, n.z), n = cross(e2, e1)
   const float4 *tri_ng;   // (normalize(n), material id bits)
   const float4 *tri_sn;   // 3 per triangle: shading n0, s1 = n1 - n0, s2 = n2 - n0 (or null)
-  const float4 *mat;      // (albedo xyz, 1 = light)
+  const float4 *mat;      // (albedo xyz, kind: 0 Lambert, 1 light, 2 mirror, 3 metal)
+  const float *shininess; // per material (metal lobe exponent)
+  int has_metal;          // a metal material exists (shadow rays check their vertex's kind)
   const float *emission;  // per-material scale of the light's emitted power (1 by default)
   const int32_t *lights;  // light triangle ids, triangle order
   const float *cdf;       // n_lights + 1 prefix sums of light areas, cdf[0] = 0

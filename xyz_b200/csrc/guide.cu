@@ -1249,6 +1249,8 @@ int xyzgpu_render_guided(xyzgpu_guide h, const xyzgpu_camera *cam, const xyzgpu_
   if (!(cam->film_size > 0) || !(cam->focal_length > 0) || !(cam->f_number > 0))
     return set_error(XYZGPU_E_INVALID, "render_guided: camera film size, focal length and F-number must be > 0");
   GuideImpl &g = h->g;
+  if (g.scene->n_specular)
+    return set_error(XYZGPU_E_INVALID, "render_guided: scenes with mirror or metal materials are not guided");
   cudaStream_t const st = static_cast<cudaStream_t>(stream);
   XYZ_CUDA_TRY(cudaSetDevice(g.device));
   XYZ_CUDA_TRY(cudaMemsetAsync(g.d_err, 0, sizeof(int), st));

@@ -18,8 +18,8 @@ constexpr int64_t kMaxGuidedWave = int64_t{1} << 23;
 // published under a mutex only when complete, so threads rendering on several
 // devices never see a partly filled entry or another device's grids.
 struct Grids {
-  int raygen, trace_e, trace_s, trace_s_adj, trace_s_guide;
-  int shade, shade_adj, shade_guide, shade_sp, film;
+  int raygen, trace_e, trace_s, trace_s_adj, trace_s_guide, trace_s_imp;
+  int shade, shade_adj, shade_guide, shade_sp, shade_imp, film;
 };
 
 Grids wave_grids(int device) {
@@ -39,6 +39,8 @@ Grids wave_grids(int device) {
     g.shade_adj = occupancy_grid(k_shade<kModeAdjoint>, device);
     g.shade_guide = occupancy_grid(k_shade<kModeGuided>, device);
     g.shade_sp = occupancy_grid(k_shade_spectral, device);
+    g.trace_s_imp = occupancy_grid(k_trace_queue<true, false, kModeImporton>, device);
+    g.shade_imp = occupancy_grid(k_shade<kModeImporton>, device);
     g.film = occupancy_grid(k_film, device);
     table[d] = g;
     ready[d] = true;
@@ -49,7 +51,7 @@ Grids wave_grids(int device) {
 
 extern const int64_t kBytesPerPath = 3 * sizeof(float4) + sizeof(uint32_t) +  // beta, radiance, hits, misc
                                   2 * (2 * sizeof(float4) + sizeof(int32_t)) +  // extension queues
-                                  3 * sizeof(float4) + sizeof(int32_t) +         // shadow queue
+                                  4 * sizeof(float4) + sizeof(int32_t) +         // shadow queue
                                   sizeof(float) + sizeof(int32_t);               // spectral fsn, slot
 
 SharedWaves &shared_waves(int device) {
@@ -70,13 +72,14 @@ void free_wave_buffers(RenderWorkspace &w) {
   cudaFree(w.s_o);
   cudaFree(w.s_d);
   cudaFree(w.s_pb);
+  cudaFree(w.s_m);
   cudaFree(w.s_target);
   cudaFree(w.fsn);
   cudaFree(w.s_slot);
   cudaFree(w.counts);
   w.fsn = nullptr;
   w.s_slot = nullptr;
-  w.beta = w.radiance = w.hits = w.s_o = w.s_d = w.s_pb = nullptr;
+  w.beta = w.radiance = w.hits = w.s_o = w.s_d = w.s_pb = w.s_m = nullptr;
   w.misc = nullptr;
   w.q_o[0] = w.q_o[1] = w.q_d[0] = w.q_d[1] = nullptr;
   w.q_slot[0] = w.q_slot[1] = w.s_target = w.counts = nullptr;
@@ -112,6 +115,7 @@ int ensure_wave_buffers(RenderWorkspace &w, int64_t capacity, int iters) {
   XYZ_ALLOC(w.s_o, c * sizeof(float4));
   XYZ_ALLOC(w.s_d, c * sizeof(float4));
   XYZ_ALLOC(w.s_pb, c * sizeof(float4));
+  XYZ_ALLOC(w.s_m, c * sizeof(float4));
   XYZ_ALLOC(w.s_target, c * sizeof(int32_t));
   XYZ_ALLOC(w.fsn, c * sizeof(float));
   XYZ_ALLOC(w.s_slot, c * sizeof(int32_t));
@@ -134,7 +138,7 @@ void render_workspace_free(RenderWorkspace &w) {
 }
 
 int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp, float *film,
-                  cudaStream_t st, const AdjointArgs *adj, const GuideHooks *guide) {
+                  cudaStream_t st, const AdjointArgs *adj, const GuideHooks *guide, const ImportonHooks *imp) {
   XYZ_CUDA_TRY(cudaSetDevice(s.device));
   // a band of rows (every row_step-th row of it) renders the same pixels and
   // paths as the full image
@@ -163,8 +167,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       cap = std::min(cap, std::max<int64_t>(afford, int64_t{1} << 20));
     }
     cap = std::max(cap, sw.ws.capacity);
-    // guided waves also hold a mixture (80 B) and training records per path
-    if (guide) cap = std::min<int64_t>(cap, kMaxGuidedWave);
+    // guided waves also hold a mixture (80 B) and training records per path,
+    // importance-driven waves a histogram (64 B) per path
+    if (guide || imp) cap = std::min<int64_t>(cap, kMaxGuidedWave);
   }
   if (sw.done && sw.last != st) XYZ_CUDA_TRY(cudaStreamWaitEvent(st, sw.done, 0));
   int rc = ensure_wave_buffers(sw.ws, cap, iters);
@@ -252,6 +257,7 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   A.s_o = wv.s_o;
   A.s_d = wv.s_d;
   A.s_pb = wv.s_pb;
+  A.s_m = wv.s_m;
   A.s_target = wv.s_target;
   A.counts = wv.counts;
   A.spectral = rp.spectral;
@@ -275,6 +281,15 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
     A.guide_alpha = gw.alpha;
     A.records = gw.records;
     A.train_bounces = gw.train_bounces;
+  }
+
+  float *imp_cdf = nullptr;
+  int imp_bounces = 0;
+  if (imp) {
+    int64_t const need = std::min<int64_t>(cap, std::max<int64_t>(1, npix_total * rp.spp));
+    int const r = importon_wave_prepare(*imp->m, need, &imp_cdf);
+    if (r) return r;
+    imp_bounces = importon_guide_bounces(*imp->m);
   }
 
   xyzgpu_render_counters rc_out{};
@@ -328,9 +343,23 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
             XYZ_MARK(5, false);
             ++launches;
           }
+          // importance-driven: the histograms of this bounce's hit points
+          bool const imp_here = imp && b < iters - 1 && b < imp_bounces;
+          A.imp_cdf = imp_here ? imp_cdf : nullptr;
+          if (imp_here) {
+            int const qi = b & 1;
+            XYZ_MARK(5, true);
+            int const r = importon_query_launch(*imp->m, A.q_o[qi], A.q_d[qi], A.hits,
+                                                A.counts + b * kCountStride + kCExt, A.S, imp_cdf, st);
+            if (r) return r;
+            XYZ_MARK(5, false);
+            ++launches;
+          }
           XYZ_MARK(2, true);
           if (spectral)
             k_shade_spectral<<<G.shade_sp, kThreads, 0, st>>>(A, b);
+          else if (imp)
+            k_shade<kModeImporton><<<G.shade_imp, kThreads, 0, st>>>(A, b);
           else if (guide)
             k_shade<kModeGuided><<<G.shade_guide, kThreads, 0, st>>>(A, b);
           else if (replay)
@@ -345,6 +374,8 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
             k_trace_queue<true, false, kModeAdjoint><<<G.trace_s_adj, kThreads, 0, st>>>(A, b, pc);
           else if (guide)
             k_trace_queue<true, false, kModeGuided><<<G.trace_s_guide, kThreads, 0, st>>>(A, b, pc);
+          else if (imp)
+            k_trace_queue<true, false, kModeImporton><<<G.trace_s_imp, kThreads, 0, st>>>(A, b, pc);
           else
             k_trace_queue<true, false><<<G.trace_s, kThreads, 0, st>>>(A, b, pc);
           XYZ_MARK(3, false);
@@ -531,6 +562,8 @@ int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_r
     return set_error(XYZGPU_E_INVALID, "render_noalloc: profiling is not available");
   if (rp.spectral != XYZGPU_SPECTRAL_OFF)
     return set_error(XYZGPU_E_INVALID, "render_noalloc: only the XYZ film mode is available");
+  if (s.dev.has_metal)
+    return set_error(XYZGPU_E_INVALID, "render_noalloc: scenes with metal materials are not available");
   if (rp.wave_paths > kNoAllocPaths)
     return set_error(XYZGPU_E_LIMIT, "render_noalloc: wave_paths %d exceeds the maximum of %lld",
                      rp.wave_paths, static_cast<long long>(kNoAllocPaths));

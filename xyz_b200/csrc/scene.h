@@ -39,6 +39,7 @@ struct RenderWorkspace {
   int32_t *q_slot[2] = {nullptr, nullptr};
   float4 *hits = nullptr;
   float4 *s_o = nullptr, *s_d = nullptr, *s_pb = nullptr;
+  float4 *s_m = nullptr;        // metal vertices' next-event terms (nk2, nk3, lobe pdf, factor)
   int32_t *s_target = nullptr;
   float *fsn = nullptr;         // spectral modes: fSamplingNext per path
   int32_t *s_slot = nullptr;    // spectral modes: path slot of each shadow ray
@@ -64,6 +65,8 @@ struct SceneImpl {
   int32_t *d_lights = nullptr;
   float *d_cdf = nullptr;
   float *d_spd = nullptr;  // 31-bin albedo spectra (spectral modes)
+  float *d_shininess = nullptr;  // per material
+  int n_specular = 0;            // materials of kind mirror or metal
   uint2 *d_nodes = nullptr;
   int32_t *d_refs = nullptr;
   int64_t n_nodes = 0, n_refs = 0, n_leaves = 0, n_empty = 0;
@@ -124,9 +127,23 @@ int guide_infer_launch(GuideImpl &g, const float4 *qo, const float4 *qd, const f
                        const int32_t *count, const DevScene &S, void *mix, cudaStream_t st);
 int guide_train_on_wave(GuideImpl &g, const float4 *radiance, int64_t npaths, cudaStream_t st);
 
+// Importance-driven render (xyzgpu_render_importon): the light-importance map
+// and its per-wave histogram buffer (importon.cu).
+struct ImportonImpl;
+struct ImportonHooks {
+  ImportonImpl *m;
+};
+int importon_wave_prepare(ImportonImpl &m, int64_t capacity, float **cdf);
+int importon_query_launch(ImportonImpl &m, const float4 *qo, const float4 *qd, const float4 *hits,
+                          const int32_t *count, const DevScene &S, float *cdf, cudaStream_t st);
+int importon_guide_bounces(const ImportonImpl &m);
+
 int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp,
                   float *film, cudaStream_t st, const AdjointArgs *adj = nullptr,
-                  const GuideHooks *guide = nullptr);
+                  const GuideHooks *guide = nullptr, const ImportonHooks *imp = nullptr);
+// Argument checks of xyzgpu_render (api.cu).
+int check_render_args(const char *who, xyzgpu_scene scene, const xyzgpu_camera *cam,
+                      const xyzgpu_render_params *rp);
 void render_workspace_free(RenderWorkspace &ws);
 int render_collect(SceneImpl &s);
 int render_noalloc_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_params &rp,

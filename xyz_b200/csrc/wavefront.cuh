@@ -86,7 +86,7 @@ struct WaveBlock {
 
 // Variants of the shading and shadow kernels: the plain render, the replay
 // pass of the adjoint, batched renders and guided renders.
-enum WaveMode : int { kModePlain = 0, kModeAdjoint = 1, kModeBatch = 2, kModeGuided = 3 };
+enum WaveMode : int { kModePlain = 0, kModeAdjoint = 1, kModeBatch = 2, kModeGuided = 3, kModeImporton = 4 };
 
 struct WaveArgs {
   DevScene S;
@@ -98,6 +98,8 @@ struct WaveArgs {
   uint64_t seed;
   int64_t p0;       // first pixel of the wave, counted over the rendered rows
   int64_t npix;     // pixels in the wave
+  const float *imp_cdf;  // importance-driven: 16 cumulative histogram counts per extension-queue
+                         // entry of this bounce, or null (Lambert sampling)
   int64_t row0;     // first rendered image row
   int row_step;     // rendered rows are row0, row0 + row_step, ... (0 or 1: consecutive)
   uint32_t s0;      // first sample index of the wave
@@ -111,6 +113,7 @@ struct WaveArgs {
   int32_t *q_slot[2];
   float4 *hits;
   float4 *s_o, *s_d, *s_pb;
+  float4 *s_m;      // metal vertices: nk2, nk3, lobe pdf, pdf / max(nk1, nk2) * Fresnel
   int32_t *s_target;
   int32_t *counts;
   // spectral modes (XYZGPU_SPECTRAL_*): beta and radiance hold one channel per
@@ -456,6 +459,7 @@ struct ShadowSink {
   static constexpr bool kAdj = kMode == kModeAdjoint;
   static constexpr bool kBatch = kMode == kModeBatch;
   static constexpr bool kGuide = kMode == kModeGuided;
+  static constexpr bool kImp = kMode == kModeImporton;
   static constexpr bool kTarget = true;  // only "is the target the closest hit?" matters
   const WaveArgs *A;
   uint32_t visible;
@@ -472,16 +476,35 @@ struct ShadowSink {
   }
   XYZ_DEV void store(int i, const RayHit &h) {
     if (h.id < 0 || h.id != A->s_target[i]) return;
-    // Lambert::CalculateWeightedDirectLighting, lambert.cpp:157-172
-    float const G = A->s_d[i].w / (h.t * h.t);  // nk2 * nk3 / t^2
-    float dimp = static_cast<float>(kInvPi * static_cast<double>(G));
-    // guided: the sampling density is the guide / Lambert mixture, rho times Lambert's
-    if (kGuide) dimp *= __int_as_float(A->s_slot[i]);
     float const light_area = kBatch ? scene(i)->light_area : A->S.light_area;
-    float const dexp = 1.0f / light_area;
-    float const dens = dimp / dexp;
-    double const wgt = (static_cast<double>(G) * (kInvPi * kInvPi)) *
-                       static_cast<double>(1.0f / (1.0f + dens * dens));
+    const DevScene &SV = kBatch ? *scene(i) : A->S;
+    double wgt;
+    if (!kSpec && SV.has_metal && __ldg(&SV.mat[__float_as_int(__ldg(&SV.tri_ng[h.id]).w)]).w == 3.0f) {
+      // Metal::CalculateWeightedDirectLighting (xyz/bsdf/metal.cpp:68-119):
+      // w = nk3 / t^2, G = nk2 w, the MIS density of the lobe's pdf against
+      // the light's area density; the lobe pdf / max(nk1, nk2) * Fresnel
+      // factor comes with the record
+      float4 const sm = A->s_m[i];
+      float const w = sm.y / (h.t * h.t);
+      float const Gm = sm.x * w;
+      float const fd = sm.z * w * light_area;
+      wgt = (static_cast<double>(Gm) * kInvPi) * static_cast<double>(sm.w) *
+            static_cast<double>(1.0f / (1.0f + fd * fd));
+    } else {
+      // Lambert::CalculateWeightedDirectLighting, lambert.cpp:157-172
+      float const G = A->s_d[i].w / (h.t * h.t);  // nk2 * nk3 / t^2
+      // importance-driven: M_1_PI * G * the histogram's density of the light
+      // direction, in double as Lambert::CalculateWeightedDirectLighting with
+      // importons computes it (xyz/bsdf/lambert.cpp:210-212)
+      float dimp = kImp ? static_cast<float>(kInvPi * static_cast<double>(G) *
+                                             static_cast<double>(__int_as_float(A->s_slot[i])))
+                        : static_cast<float>(kInvPi * static_cast<double>(G));
+      // guided: the sampling density is the guide / Lambert mixture, rho times Lambert's
+      if (kGuide) dimp *= __int_as_float(A->s_slot[i]);
+      float const dexp = 1.0f / light_area;
+      float const dens = dimp / dexp;
+      wgt = (static_cast<double>(G) * (kInvPi * kInvPi)) * static_cast<double>(1.0f / (1.0f + dens * dens));
+    }
     float4 pb = A->s_pb[i];
     int32_t const slot = kSpec ? A->s_slot[i] : __float_as_int(pb.w);
     if (kAdj) {
@@ -627,14 +650,88 @@ XYZ_DEV LightSample sample_light(const DevScene &S, uint64_t seed, uint32_t pixe
   return L;
 }
 
+// ImportanceQuery::GetDensity (xyz/core/photonmap.cpp:375-401): the density,
+// relative to cosine sampling, of direction `dir` (towards the surface) under
+// the histogram c (cumulative counts, c[0] = 0): bins of cos^2 theta (2) and
+// phi / 2 (8) about the shading frame.
+XYZ_DEV int importon_bin(f3 dir, f3 sn, f3 tan, f3 bin, bool *above) {
+  float const cs = -dot3(dir, sn);
+  *above = cs > 0.0f;
+  int u = static_cast<int>(cs * cs * 2.0f);
+  if (u >= 2) u = 1;
+  float phi = 0.5f * atan2f(-dot3(dir, bin), -dot3(dir, tan));
+  if (phi < 0.0f) phi = static_cast<float>(static_cast<double>(phi) + kPi);
+  int v = static_cast<int>(static_cast<double>(phi) * (8.0 * kInvPi));
+  if (v >= 8) v = 7;
+  return u * 8 + v;
+}
+
+XYZ_DEV float importon_density(const float *c, f3 dir, f3 sn, f3 tan, f3 bin) {
+  bool above;
+  int const n = importon_bin(dir, sn, tan, bin, &above);
+  if (!above) return 0.0f;
+  return 16.0f * (c[n + 1] - c[n]) / c[16];
+}
+
+// FakeFresnelTerm (xyz/stdafx.hpp:44-47): F0 + (1 - F0) (1 - hk)^5, F0 = 0.9,
+// the fifth power as hi::fifth_power_of forms it (x * ((x x) (x x))).
+XYZ_DEV float fake_fresnel(float hk) {
+  float const f0 = 0.9f;
+  float const x = 1.0f - hk;
+  float const x2 = x * x;
+  return f0 + (1.0f - f0) * (x * (x2 * x2));
+}
+
+// Triangle::ShadingBasis (triangle.cpp:194-219) at barycentrics (f, g):
+// geometric and interpolated shading normals (flipped on the back side) and
+// the tangent frame about the shading normal; returns the material id.
+XYZ_DEV int32_t shading_frame(const DevScene &S, int32_t tri, int back, float f, float g, f3 *gn_out, f3 *sn_out,
+                              f3 *tan_out, f3 *bin_out) {
+  float4 const g4 = __ldg(&S.tri_ng[tri]);
+  f3 gn = xyz3(g4);
+  f3 sn;
+  if (S.tri_sn) {
+    f3 const n0 = xyz3(__ldg(&S.tri_sn[3 * tri])), s1 = xyz3(__ldg(&S.tri_sn[3 * tri + 1])),
+             s2 = xyz3(__ldg(&S.tri_sn[3 * tri + 2]));
+    sn = normalize3(add3(add3(n0, scl3(s1, f)), scl3(s2, g)));
+  } else {
+    f3 const z = mk3(0.0f, 0.0f, 0.0f);
+    sn = normalize3(add3(add3(gn, scl3(z, f)), scl3(z, g)));
+  }
+  if (back) {
+    gn = neg3(gn);
+    sn = neg3(sn);
+  }
+  f3 tan = mk3(-sn.z, 0.0f, sn.x), bin;
+  float const l2 = dot3(tan, tan);
+  if (l2 > 0.0f) {
+    tan = scl3(tan, 1.0f / sqrtf(l2));
+    bin = cross3(tan, sn);
+  } else {
+    bin = mk3(0.0f, 0.0f, (sn.y > 0.0f) ? 1.0f : -1.0f);
+    tan = cross3(sn, bin);
+  }
+  *gn_out = gn;
+  *sn_out = sn;
+  *tan_out = tan;
+  *bin_out = bin;
+  return __float_as_int(g4.w);
+}
+
 // kModeAdjoint: the replay pass of xyzgpu_adjoint (same path, plus gradients).
 // kModeBatch: paths of many scenes (xyzgpu_batch_*).
 // kModeGuided: directions from the learned guide mixed with Lambert sampling.
+// kModeImporton: directions from the light-importance histogram of the vertex
+// (the reference's importance-driven tracer).
 template <int kMode>
 __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shade(WaveArgs A, int b) {
   constexpr bool kAdj = kMode == kModeAdjoint;
   constexpr bool kBatch = kMode == kModeBatch;
   constexpr bool kGuide = kMode == kModeGuided;
+  constexpr bool kImp = kMode == kModeImporton;
+  // mirror and metal materials exist in plain and batched renders only (the
+  // other modes refuse such scenes), so the other variants carry no code for them
+  constexpr bool kSpecMat = kMode == kModePlain || kMode == kModeBatch;
   int32_t *const cnt = A.counts + b * kCountStride;
   int32_t *const cnt_next = A.counts + (b + 1) * kCountStride;
   int const n = cnt[kCExt];
@@ -652,6 +749,8 @@ __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shad
     uint32_t misc = 0;
     int32_t light_mat = 0;
     float rho = 1.0f;
+    float4 sm4{};           // metal vertex: next-event terms for the shadow ray
+    bool sh_metal = false;
     int block = 0;
     // guide_alpha is 0 at bounces without inference: Lambert sampling
     // alone, and the mixture buffer is not read
@@ -678,36 +777,13 @@ __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shad
           rec[14] = L.y;
           rec[15] = L.z;
         }
-        // Triangle::ShadingBasis (triangle.cpp:194-219)
-        float4 const g4 = __ldg(&S.tri_ng[tri]);
-        f3 gn = xyz3(g4);
-        int32_t const m = __float_as_int(g4.w);
-        f3 sn;
-        if (S.tri_sn) {
-          f3 const n0 = xyz3(__ldg(&S.tri_sn[3 * tri])), s1 = xyz3(__ldg(&S.tri_sn[3 * tri + 1])),
-                   s2 = xyz3(__ldg(&S.tri_sn[3 * tri + 2]));
-          sn = normalize3(add3(add3(n0, scl3(s1, h.y)), scl3(s2, h.z)));
-        } else {
-          f3 const z = mk3(0.0f, 0.0f, 0.0f);
-          sn = normalize3(add3(add3(gn, scl3(z, h.y)), scl3(z, h.z)));
-        }
-        if (back) {
-          gn = neg3(gn);
-          sn = neg3(sn);
-        }
-        f3 tan = mk3(-sn.z, 0.0f, sn.x), bin;
-        float const l2 = dot3(tan, tan);
-        if (l2 > 0.0f) {
-          tan = scl3(tan, 1.0f / sqrtf(l2));
-          bin = cross3(tan, sn);
-        } else {
-          bin = mk3(0.0f, 0.0f, (sn.y > 0.0f) ? 1.0f : -1.0f);
-          tan = cross3(sn, bin);
-        }
+        f3 gn, sn, tan, bin;
+        int32_t const m = shading_frame(S, tri, back, h.y, h.z, &gn, &sn, &tan, &bin);
         if (!(-dot3(d, sn) <= 0.0f)) {
           pos = add3(xyz3(o4), scl3(d, h.x));
           float4 const m4 = __ldg(&S.mat[m]);
-          bool const is_light = m4.w != 0.0f;
+          int const kind = static_cast<int>(m4.w);  // 0 Lambert, 1 light, 2 mirror, 3 metal
+          bool const is_light = kind == 1;
           beta4 = A.beta[slot];
           f3 beta = xyz3(beta4);
           misc = A.misc[slot];
@@ -761,11 +837,31 @@ __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shad
           }
           uint32_t pixel = 0, sample = 0;
           if (use_guide && alive && !is_light) finish_mix(M);
+          // importance-driven: this vertex's histogram (cumulative counts
+          // c[1..16], c[0] = 0), filled by k_importon_query; none beyond the
+          // guided bounces
+          bool const use_imp = kImp && A.imp_cdf != nullptr && alive && !is_light;
+          float ic[17];
+          if (use_imp) {
+            ic[0] = 0.0f;
+            const float4 *c4 = reinterpret_cast<const float4 *>(A.imp_cdf + 16 * static_cast<int64_t>(i));
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              float4 const v4 = c4[q];
+              ic[1 + 4 * q] = v4.x;
+              ic[2 + 4 * q] = v4.y;
+              ic[3 + 4 * q] = v4.z;
+              ic[4 + 4 * q] = v4.w;
+            }
+          }
           float nee_pl = 0.0f;  // guided: Lambert density of the light direction (0: no shadow ray)
           if (alive) {
             path_pixel_sample<kBatch>(A, block, slot, &pixel, &sample);
-            if (!is_light) {
-              // next-event estimation (lambert.cpp:125-156)
+            // a mirror has no next-event estimation and leaves the throughput
+            // alone (Mirror::CalculateWeightedDirectLighting, xyz/bsdf/mirror.cpp:47-51)
+            if (!is_light && !(kSpecMat && kind == 2)) {
+              // next-event estimation (lambert.cpp:125-156; a metal's albedo
+              // enters the throughput the same way, metal.cpp:68-71)
               beta = mul3(beta, xyz3(m4));
               if (kAdj) {
                 // Every contribution from here on carries this vertex's albedo
@@ -793,6 +889,26 @@ __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shad
                     light_mat = ls.mat;
                     if (!kAdj) pbv = scl3(pbv, __ldg(&S.emission[ls.mat]));
                     if (use_guide) nee_pl = nk2 * static_cast<float>(kInvPi);
+                    if (kImp) rho = use_imp ? importon_density(ic, v, sn, tan, bin) : 1.0f;
+                    if (kSpecMat && kind == 3) {
+                      // Metal::CalculateWeightedDirectLighting (metal.cpp:92-113):
+                      // the Phong-lobe pdf of the light direction about the
+                      // half vector, its Fresnel term and the max(nk1, nk2)
+                      // normalisation travel with the shadow ray
+                      float const shin = __ldg(&S.shininess[m]);
+                      f3 const hv = neg3(normalize3(add3(v, d)));
+                      float const hk = -dot3(hv, v);
+                      float const nh = dot3(sn, hv);
+                      float const nk1 = -dot3(sn, d);
+                      float const fsn_m = static_cast<float>(static_cast<double>(shin + 1.0f) * (kInvPi / 8.0) *
+                                                             static_cast<double>(powf(nh, shin)) /
+                                                             static_cast<double>(hk));
+                      float const kf = static_cast<float>(static_cast<double>(fsn_m) /
+                                                          static_cast<double>(fmaxf(nk1, nk2)) *
+                                                          static_cast<double>(fake_fresnel(hk)));
+                      sm4 = make_float4(nk2, nk3, fsn_m, kf);
+                      sh_metal = true;
+                    }
                   }
                 }
               }
@@ -870,6 +986,72 @@ __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shad
                   rec[13] = rec[14] = rec[15] = __int_as_float(0x7fc00000);
                 }
               }
+            } else if (kImp && use_imp && alive) {
+              // Lambert::NextScatteringDirection with importons
+              // (lambert.cpp:243-257) -> ImportanceQuery::SetDiffusedVector
+              // (photonmap.cpp:403-439): a bin by the cumulative counts, then
+              // (cos^2 theta, phi) uniform in it; the throughput is divided by
+              // the bin's density and the sampling density is density cos / pi
+              float const value = ic[16] * rng.next();
+              int lo = 0, hi = 17;  // upper_bound over c[0..16]
+              while (lo < hi) {
+                int const mid = (lo + hi) >> 1;
+                if (!(value < ic[mid]))
+                  lo = mid + 1;
+                else
+                  hi = mid;
+              }
+              int const nb = lo - 1;
+              int const bu = nb / 8, bv = nb % 8;
+              float const mu_u = (static_cast<float>(bu) + rng.next()) / 2.0f;
+              float const mu_v = (static_cast<float>(bv) + rng.next()) / 8.0f;
+              float const cos_t = sqrtf(mu_u);
+              float const sin_t = sqrtf(1.0f - mu_u);
+              float const phi = static_cast<float>(2.0 * kPi) * mu_v;
+              dir = add3(add3(scl3(tan, sin_t * cosf(phi)), scl3(bin, sin_t * sinf(phi))), scl3(sn, cos_t));
+              float const dens = 16.0f * (ic[nb + 1] - ic[nb]) / ic[16];
+              float const fsn = static_cast<float>(static_cast<double>(dens * cos_t) * kInvPi);
+              beta = scl3(beta, 1.0f / dens);
+              if (dot3(dir, gn) > 0.0f) {
+                push_ext = true;
+                beta4 = make_float4(beta.x, beta.y, beta.z, fsn);
+                misc = pack_misc(rng.dim, k, 0u);
+              }
+            } else if (kSpecMat && alive && kind == 2) {
+              // Mirror::NextScatteringDirection (mirror.cpp:53-71): the
+              // reflection about the shading normal, a specular bounce
+              float const ct = -dot3(d, sn);
+              dir = add3(d, scl3(sn, 2.0f * ct));
+              if (dot3(dir, gn) > 0.0f) {
+                push_ext = true;
+                beta4 = make_float4(beta.x, beta.y, beta.z, 1.0f);
+                misc = pack_misc(rng.dim, k, 1u);
+              }
+            } else if (kSpecMat && alive && kind == 3) {
+              // Metal::NextScatteringDirection (metal.cpp:122-159) with
+              // ComputeGlossyHalfwayVector (xyz/stdafx.hpp:154-168): a half
+              // vector from the Phong lobe (g++ passes the first draw to rMuPhi),
+              // the mirror direction about it; throughput times
+              // Fresnel / max(nk1, nk2) * nk2; not specular (CONFIG_EXPLICIT_GLOSSY)
+              float const mu_phi = rng.next();
+              float const mu_theta = rng.next();
+              float const shin = __ldg(&S.shininess[m]);
+              float const rphi = static_cast<float>(2.0 * kPi) * mu_phi;
+              float const cos_t = powf(mu_theta, 1.0f / shin);
+              float const sin_t = sqrtf(1.0f - cos_t * cos_t);
+              f3 const hv = add3(add3(scl3(tan, sin_t * cosf(rphi)), scl3(bin, sin_t * sinf(rphi))), scl3(sn, cos_t));
+              float const nk1 = -dot3(sn, d);
+              float const hk = -dot3(hv, d);
+              dir = add3(d, scl3(hv, 2.0f * hk));
+              float const nk2 = dot3(sn, dir);
+              if (!((nk2 <= 0.0f) || (dot3(gn, dir) <= 0.0f))) {
+                beta = scl3(beta, fake_fresnel(hk) / fmaxf(nk1, nk2) * nk2);
+                float const fsn = static_cast<float>(static_cast<double>(shin + 1.0f) * (kInvPi / 8.0) *
+                                                     static_cast<double>(powf(cos_t, shin)) / static_cast<double>(hk));
+                push_ext = true;
+                beta4 = make_float4(beta.x, beta.y, beta.z, fsn);
+                misc = pack_misc(rng.dim, k, 0u);
+              }
             } else if (alive) {
               // Lambert::NextScatteringDirection / ComputeDiffusedVector
               // (lambert.cpp:176-187, stdafx.hpp:50-63); g++ passes the first
@@ -899,7 +1081,8 @@ __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shad
       A.s_pb[js] = make_float4(pbv.x, pbv.y, pbv.z, __int_as_float(slot));
       A.s_target[js] = tri;
       if (kAdj) A.s_slot[js] = light_mat;
-      if (kGuide) A.s_slot[js] = __float_as_int(rho);
+      if (kGuide || kImp) A.s_slot[js] = __float_as_int(rho);
+      if (sh_metal) A.s_m[js] = sm4;
     }
     int32_t const je = warp_append(&cnt_next[kCExt], push_ext);
     if (push_ext) {
@@ -1008,7 +1191,7 @@ __global__ void __launch_bounds__(kThreads) k_shade_spectral(WaveArgs A, int b) 
         }
         if (!(-dot3(d, sn) <= 0.0f)) {
           pos = add3(xyz3(o4), scl3(d, h.x));
-          bool const is_light = __ldg(&S.mat[m]).w != 0.0f;
+          bool const is_light = __ldg(&S.mat[m]).w == 1.0f;
           beta = A.beta[slot];
           float const fsn_in = A.fsn[slot];
           misc = A.misc[slot];

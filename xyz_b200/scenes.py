@@ -21,7 +21,7 @@ from typing import Optional
 
 import numpy as np
 
-from .spectrum import N_BINS, ccir601_rgb_to_xyz, flat_spd_xyz, rgb_to_spd
+from .spectrum import N_BINS, ccir601_rgb_to_xyz, flat_spd_xyz, named_spectrum, rgb_to_spd, spd_to_xyz
 
 
 @dataclass
@@ -63,6 +63,8 @@ class SceneData:
     name: str = ""
     albedo_spd: Optional[np.ndarray] = None       # (nm, 31) float32 spectra (spectral modes)
     light_power_spd: Optional[np.ndarray] = None  # (31,) float32, Phi per bin
+    material_kind: Optional[np.ndarray] = None    # (nm,) int32: 0 Lambert, 2 mirror, 3 metal
+    shininess: Optional[np.ndarray] = None        # (nm,) float32 metal lobe exponents
 
     @property
     def n_tris(self) -> int:
@@ -178,6 +180,75 @@ def cornell_box(res_fov: float = 40.0, pinhole: bool = True,
     sd.albedo_spd = np.stack([rgb_to_spd((0.8, 0.8, 0.8)), rgb_to_spd((0.63, 0.06, 0.05)),
                               rgb_to_spd((0.14, 0.45, 0.09)), np.zeros(N_BINS, np.float32)])
     sd.light_power_spd = flat_emitter_power_spd(radiance, sd.light_area())
+    return sd
+
+
+def cornell_specular(shininess: float = 40.0, pinhole: bool = True, radiance: float = 15.0) -> SceneData:
+    """The Cornell room with the tall box a perfect mirror (the reference's
+    Mirror, xyz/bsdf/mirror.cpp) and the short box a glossy metal (its Metal,
+    xyz/bsdf/metal.cpp: Phong lobe of exponent `shininess`, albedo of a
+    gold-like RGB (1.0, 0.78, 0.34) in XYZ)."""
+    sd = cornell_box(pinhole=pinhole, radiance=radiance)
+    # materials 0..3 are white, red, green, light; 4 mirror, 5 metal
+    tall = slice(10, 22)     # triangles of the tall box (after 10 wall triangles)
+    short = slice(22, 34)
+    tri_mat = sd.tri_mat.copy()
+    tri_mat[tall] = 4
+    tri_mat[short] = 5
+    albedo = np.concatenate([sd.albedo_xyz, np.ones((1, 3), np.float32),
+                             ccir601_rgb_to_xyz((1.0, 0.78, 0.34))[None]]).astype(np.float32)
+    sd.tri_mat = tri_mat
+    sd.albedo_xyz = albedo
+    sd.is_light = np.array([0, 0, 0, 1, 0, 0], np.int32)
+    sd.material_kind = np.array([0, 0, 0, 0, 2, 3], np.int32)
+    sd.shininess = np.array([1, 1, 1, 1, 1, shininess], np.float32)
+    sd.albedo_spd = None
+    sd.name = "cornell-specular"
+    return sd
+
+
+def color_checker_room(illuminant: str = "light_d65", radiance: float = 15.0, pinhole: bool = True) -> SceneData:
+    """The Cornell room with spectral materials from the reference's tables
+    (libhi/hi/image/spectrum.cpp:170-476): walls of Macbeth ColorChecker
+    patches (floor and ceiling neutral 8, back wall white, left red, right
+    green, boxes blue sky and foliage), the 24 patches as a 6 x 4 chart of
+    0.2 m squares 1 mm in front of the back wall, and the ceiling light
+    emitting the named illuminant's spectrum scaled to a mean radiance of
+    `radiance` W/m^2/sr per bin.  XYZ albedos are the spectra's XYZ (clamped to
+    [0, 1]) for the XYZ film mode."""
+    from .spectrum import COLOR_CHECKER
+    WALL = ["mcc_neutral80", "mcc_white", "mcc_red", "mcc_green", "mcc_blue_sky", "mcc_foliage"]
+    b = _Builder()
+    N80, WHITE, RED, GREEN, SKY, FOL, LIGHT = range(7)
+    b.add_quad((-1, 0, -1), (1, 0, -1), (1, 0, 1), (-1, 0, 1), N80, (0, 1, 0))
+    b.add_quad((-1, 2, -1), (1, 2, -1), (1, 2, 1), (-1, 2, 1), N80, (0, -1, 0))
+    b.add_quad((-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1), WHITE, (0, 0, 1))
+    b.add_quad((-1, 0, -1), (-1, 2, -1), (-1, 2, 1), (-1, 0, 1), RED, (1, 0, 0))
+    b.add_quad((1, 0, -1), (1, 2, -1), (1, 2, 1), (1, 0, 1), GREEN, (-1, 0, 0))
+    b.add_box((-0.70, 0.0, -0.70), (-0.10, 1.2, -0.10), SKY)
+    b.add_box((0.10, 0.0, -0.20), (0.70, 0.6, 0.40), FOL)
+    y = 2.0 - 0.001
+    b.add_quad((-0.25, y, -0.25), (0.25, y, -0.25), (0.25, y, 0.25), (-0.25, y, 0.25), LIGHT, (0, -1, 0))
+    z = -1.0 + 0.001
+    for k, _ in enumerate(COLOR_CHECKER):
+        r, c = divmod(k, 6)
+        x0, y0 = -0.6 + 0.2 * c, 1.95 - 0.2 * (r + 1)
+        b.add_quad((x0, y0, z), (x0 + 0.19, y0, z), (x0 + 0.19, y0 + 0.19, z), (x0, y0 + 0.19, z), 7 + k, (0, 0, 1))
+    pos, tris, mat = b.arrays()
+    names = WALL + [None] + list(COLOR_CHECKER)
+    spd = np.stack([named_spectrum(n) if n else np.zeros(N_BINS, np.float32) for n in names]).astype(np.float32)
+    albedo = np.stack([np.clip(spd_to_xyz(v), 0.0, 1.0) for v in spd]).astype(np.float32)
+    is_light = np.zeros(len(names), np.int32)
+    is_light[LIGHT] = 1
+    sd = SceneData(pos, tris, mat, albedo, is_light, np.zeros(3, np.float32),
+                   camera=Camera.with_fov((0.0, 1.0, 3.75), (0.0, 1.0, 0.0), 40.0, pinhole=pinhole),
+                   name="color-checker-room")
+    illum = named_spectrum(illuminant).astype(np.float64)
+    L = (illum / illum.mean() * radiance).astype(np.float32)
+    area = sd.light_area()
+    sd.light_power_spd = (np.float32(math.pi * area) * L).astype(np.float32)
+    sd.light_power_xyz = spd_to_xyz(sd.light_power_spd)
+    sd.albedo_spd = spd
     return sd
 
 
