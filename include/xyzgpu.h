@@ -582,6 +582,20 @@ int xyzgpu_film_save_bmp(const char *path, const float *film, int width, int hei
 int xyzgpu_checkpoint_save(const char *path, const xyzgpu_render_params *rp, int spp_done, const float *film);
 int xyzgpu_checkpoint_load(const char *path, xyzgpu_render_params *rp, int *spp_done, float *film);
 
+/* ---- Spectral tables on the host (for scene loaders and tools).  The named
+ * spectra of the reference's library (libhi/hi/image/spectrum.cpp:170-476),
+ * 31 bins at 400, 410, ..., 700 nm: illuminants "light_source_a",
+ * "light_source_b", "light_source_c", "light_d65", "light_d100",
+ * "light_standard_warm_white", "light_white", "light_standard_white",
+ * "light_daylight", "light_warm_white_de_luxe", "light_soft_white",
+ * "light_cool_white_de_luxe", "light_mercury_arc_lamp" and the 24 Macbeth
+ * ColorChecker patches "mcc_dark_skin" ... "mcc_black" (reflectances).
+ * Returns XYZGPU_E_INVALID for an unknown name. */
+int xyzgpu_named_spectrum(const char *name, float out[31]);
+/* hi::spd2xyz (spectrum.cpp:554-559): the spectrum's XYZ through the CIE 1931
+ * colour-matching functions (float dot products in bin order). */
+void xyzgpu_spectrum_to_xyz(const float spd[31], float xyz[3]);
+
 /* Host evaluation of the random stream defined above (for tests). */
 float xyzgpu_philox_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim);
 

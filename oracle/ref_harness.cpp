@@ -15,6 +15,7 @@
 // single global mt19937_64 (integrator.cpp:12-25), so that each (pixel, sample)
 // path reads a fixed stream that other implementations can reproduce.
 #include <atomic>
+#include <fstream>
 #include <vector>
 #include <unordered_map>
 
@@ -287,6 +288,95 @@ void xyzref_render(int s0, int spp, std::uint64_t seed, int y0, int y1,
         f[2] += color[2];
       }
     });
+  }
+}
+
+}  // extern "C"
+
+// Triangle's stored vectors are private: an explicit instantiation may name
+// private members and hands their pointers out.
+namespace {
+template <int K>
+struct TriMember {
+  typedef xyz::Triangle::float3_t const xyz::Triangle::*type;
+  friend type tri_member(TriMember);
+};
+template <typename Tag, typename Tag::type M>
+struct ExposeTri {
+  friend typename Tag::type tri_member(Tag) { return M; }
+};
+template struct ExposeTri<TriMember<0>, &xyz::Triangle::v0_>;
+template struct ExposeTri<TriMember<1>, &xyz::Triangle::e1_>;
+template struct ExposeTri<TriMember<2>, &xyz::Triangle::e2_>;
+template struct ExposeTri<TriMember<3>, &xyz::Triangle::ng_>;
+template struct ExposeTri<TriMember<4>, &xyz::Triangle::n0_>;
+template struct ExposeTri<TriMember<5>, &xyz::Triangle::s1_>;
+template struct ExposeTri<TriMember<6>, &xyz::Triangle::s2_>;
+}  // namespace
+
+extern "C" {
+
+// ---- The reference's MQO loader (Scene::Load, xyz/core/scene_mqo.cpp:547-696)
+// on a file: the triangles in the order it leaves them (Morton-sorted), their
+// stored geometry (v0, e1, e2, geometric normal, shading n0, s1, s2), materials
+// and the camera the file's Scene chunk sets.  Returns the triangle count.
+int xyzref_load_mqo(const char *path) {
+  ClearScene();
+  std::ifstream in(path);
+  if (!in) return -1;
+  xyz::Scene &scene = xyz::Scene::GetInstance();
+  scene.Load(in);
+  return static_cast<int>(scene.triangles_.size());
+}
+
+void xyzref_mqo_counts(int *n_tris, int *n_mats, int *n_lights) {
+  xyz::Scene &scene = xyz::Scene::GetInstance();
+  *n_tris = static_cast<int>(scene.triangles_.size());
+  *n_mats = static_cast<int>(scene.bsdfs_.size());
+  *n_lights = static_cast<int>(scene.lights_.size());
+}
+
+// geo: 21 floats per triangle (v0, e1, e2, ng, n0, s1, s2); mat: material id
+void xyzref_mqo_triangles(float *geo, int *mat) {
+  xyz::Scene &scene = xyz::Scene::GetInstance();
+  for (std::size_t i = 0; i < scene.triangles_.size(); ++i) {
+    xyz::Triangle const *t = scene.triangles_[i];
+    xyz::float3_t const v[7] = {t->*tri_member(TriMember<0>()), t->*tri_member(TriMember<1>()),
+                                t->*tri_member(TriMember<2>()), t->*tri_member(TriMember<3>()),
+                                t->*tri_member(TriMember<4>()), t->*tri_member(TriMember<5>()),
+                                t->*tri_member(TriMember<6>())};
+    for (int k = 0; k < 7; ++k)
+      for (int c = 0; c < 3; ++c) geo[21 * i + 3 * k + c] = v[k][c];
+    mat[i] = static_cast<int>(t->bsdf());
+  }
+}
+
+// kind: Bsdf::What() (0 Lambert, 1 mirror, 2 glass, 3 metal, 4 light);
+// albedo: Lambert / metal XYZ; shininess: metal exponent
+void xyzref_mqo_materials(int *kind, float *albedo, float *shininess) {
+  xyz::Scene &scene = xyz::Scene::GetInstance();
+  for (std::size_t m = 0; m < scene.bsdfs_.size(); ++m) {
+    xyz::Bsdf const *b = scene.bsdfs_[m];
+    kind[m] = static_cast<int>(b->What());
+    albedo[3 * m] = albedo[3 * m + 1] = albedo[3 * m + 2] = 0.0f;
+    shininess[m] = 0.0f;
+    if (b->What() == xyz::Bsdf::LAMBERT) {
+      xyz::float3_t const a = static_cast<xyz::Lambert const *>(b)->albedo();
+      for (int c = 0; c < 3; ++c) albedo[3 * m + c] = a[c];
+    } else if (b->What() == xyz::Bsdf::METAL) {
+      xyz::Metal const *mt = static_cast<xyz::Metal const *>(b);
+      for (int c = 0; c < 3; ++c) albedo[3 * m + c] = mt->albedo()[c];
+      shininess[m] = mt->sininess();
+    }
+  }
+}
+
+void xyzref_mqo_camera(float eye[3], float at[3]) {
+  xyz::Scene &scene = xyz::Scene::GetInstance();
+  xyz::float3_t const e = scene.ThinLensCamera().Eye(), a = scene.ThinLensCamera().At();
+  for (int c = 0; c < 3; ++c) {
+    eye[c] = e[c];
+    at[c] = a[c];
   }
 }
 

@@ -9,6 +9,8 @@
 #define GL_FRONT_AND_BACK 0
 #define GL_AMBIENT_AND_DIFFUSE 0
 #define GL_SPECULAR 0
+#define GL_SRC_ALPHA 0
+#define GL_ONE_MINUS_SRC_ALPHA 0
 #define GL_SHININESS 0
 #define GL_PROJECTION 0
 #define GL_MODELVIEW 0
@@ -31,6 +33,7 @@ XYZREF_NOGL(glPopMatrix)
 XYZREF_NOGL(glutSolidSphere)
 XYZREF_NOGL(glNewList)
 XYZREF_NOGL(glEndList)
+XYZREF_NOGL(glBlendFunc)
 inline unsigned int glGenLists(int) { return 0u; }
 namespace hi {
 XYZREF_NOGL(glNormal)

@@ -187,6 +187,26 @@ class RefLib(_Common):
     def max_threads(self):
         return self.lib.xyzref_max_threads()
 
+    def load_mqo(self, path: str):
+        """The reference's Scene::Load on an .mqo file (run by the program
+        oracle/_ref/xyzref_mqo in a process of its own): per triangle (in its
+        order) the stored geometry (n, 21: v0, e1, e2, ng, n0, s1, s2) and
+        material; per material (kind = Bsdf::What, albedo XYZ, shininess);
+        the camera (eye, at)."""
+        import subprocess
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            pre = os.path.join(d, "ref")
+            subprocess.run([os.path.join(REF_DIR, "xyzref_mqo"), path, pre], check=True,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            cam = np.fromfile(pre + ".cam", np.float32)
+            return {"geo": np.fromfile(pre + ".geo", np.float32).reshape(-1, 21),
+                    "mat": np.fromfile(pre + ".mat", np.int32),
+                    "kind": np.fromfile(pre + ".kind", np.int32),
+                    "albedo": np.fromfile(pre + ".alb", np.float32).reshape(-1, 3),
+                    "shininess": np.fromfile(pre + ".shin", np.float32),
+                    "eye": cam[:3], "at": cam[3:]}
+
     def named_spectra(self):
         """The reference library's named spectra {CamelCaseName: 31 float32}
         (libhi/hi/image/spectrum.cpp:170-476)."""

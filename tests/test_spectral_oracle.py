@@ -86,3 +86,19 @@ def test_named_spectra_are_the_reference_tables():
     for name, v in ref.items():
         mine = spectrum.named_spectrum(re.sub(r"(?<!^)(?=[A-Z])", "_", name).lower())
         assert np.array_equal(mine, v), name
+
+
+def test_library_spectra_tables_equal_the_package_tables():
+    """xyzgpu_named_spectrum / xyzgpu_spectrum_to_xyz (the C ABI for scene
+    loaders) hold the same tables as xyz_b200.spectrum, pinned above."""
+    import ctypes as C
+    from xyz_b200 import api, spectrum
+    L = api.load_library()
+    out = np.zeros(31, np.float32)
+    xyz = np.zeros(3, np.float32)
+    for name, v in spectrum.NAMED_SPECTRA.items():
+        assert L.xyzgpu_named_spectrum(name.encode(), out.ctypes.data) == 0, name
+        assert np.array_equal(out, np.asarray(v, np.float32)), name
+        L.xyzgpu_spectrum_to_xyz(out.ctypes.data, xyz.ctypes.data)
+        assert np.array_equal(xyz, spectrum.spd_to_xyz(v)), name
+    assert L.xyzgpu_named_spectrum(b"mcc_nothing", out.ctypes.data) == -1

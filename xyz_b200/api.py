@@ -43,7 +43,7 @@ EXPORTED = [
     "xyzgpu_film_tonemap", "xyzgpu_bmp_write", "xyzgpu_checkpoint_save", "xyzgpu_checkpoint_load",
     "xyzgpu_film_save_hdr", "xyzgpu_film_save_bmp", "xyzgpu_importon_config_default",
     "xyzgpu_importons_create", "xyzgpu_importons_destroy", "xyzgpu_importons_get", "xyzgpu_importons_query",
-    "xyzgpu_render_importon",
+    "xyzgpu_render_importon", "xyzgpu_named_spectrum", "xyzgpu_spectrum_to_xyz",
 ]
 
 
@@ -221,6 +221,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.xyzgpu_importons_query.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.xyzgpu_render_importon.argtypes = [C.c_void_p, C.POINTER(CameraDesc), C.POINTER(RenderParams), C.c_void_p,
                                          C.c_void_p]
+    L.xyzgpu_named_spectrum.argtypes = [C.c_char_p, C.c_void_p]
+    L.xyzgpu_spectrum_to_xyz.argtypes = [C.c_void_p, C.c_void_p]
     L.xyzgpu_film_encode_rgbe.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
     L.xyzgpu_hdr_write.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
     L.xyzgpu_tonemap_params_default.argtypes = [C.POINTER(TonemapParams)]
