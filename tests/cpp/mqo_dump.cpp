@@ -12,6 +12,11 @@
 //                         albedo XYZ, shininess
 //       out_prefix.cam    6 float32: eye, at
 //   mqo_dump --ply2mqo <mesh.ply> <out.mqo>    PlyToMqo's document
+//   mqo_dump --desc <scene.mqo | mesh.ply> <out_prefix>
+//       the arrays of the C ABI's scene description: .pos (3 float32 per
+//       vertex), .nrm (3 float32 per vertex, or empty), .tri (3 int32 per
+//       triangle), .mat, .alb (3 float32 per material), .light, .kind
+//       (XYZGPU_MATERIAL_*), .shin, .power (the reference's light power XYZ)
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -37,8 +42,9 @@ int main(int argc, char **argv) {
     std::ofstream(argv[3], std::ios::binary) << text;
     return 0;
   }
-  if (argc != 3) return 2;
-  std::string const path = argv[1], pre = argv[2];
+  bool const desc = argc == 4 && std::string(argv[1]) == "--desc";
+  if (argc != 3 && !desc) return 2;
+  std::string const path = argv[desc ? 2 : 1], pre = argv[desc ? 3 : 2];
   std::ifstream in(path, std::ios::binary);
   xyzgpu::MqoScene sc;
   std::string err;
@@ -46,6 +52,22 @@ int main(int argc, char **argv) {
   if (!(ply ? xyzgpu::LoadPly(in, &sc, &err) : xyzgpu::LoadMqo(in, &sc, &err))) {
     std::fprintf(stderr, "%s\n", err.c_str());
     return 1;
+  }
+  if (desc) {
+    float power[3];
+    xyzgpu::ReferenceLightPowerXYZ(power);
+    xyzgpu_scene_desc const d = sc.Desc(power);
+    int const nm = d.n_materials;
+    put(pre + ".pos", sc.positions);
+    put(pre + ".nrm", sc.normals);
+    put(pre + ".tri", sc.triangles);
+    put(pre + ".mat", sc.tri_material);
+    put(pre + ".alb", std::vector<float>(d.albedo_xyz, d.albedo_xyz + 3 * nm));
+    put(pre + ".light", std::vector<int32_t>(d.is_light, d.is_light + nm));
+    put(pre + ".kind", std::vector<int32_t>(d.material_kind, d.material_kind + nm));
+    put(pre + ".shin", std::vector<float>(d.shininess, d.shininess + nm));
+    put(pre + ".power", std::vector<float>(power, power + 3));
+    return 0;
   }
   std::vector<float> geo;
   auto P = [&](int v, int c) { return sc.positions[3 * v + c]; };
