@@ -332,6 +332,50 @@ def relmse_estimator(half_a, half_b):
     return relmse, ref_noise, scale
 
 
+GUIDE_FP64_FIXTURE = os.path.join(ROOT, "tests", "golden", "guide_reference_fp64.npz")
+
+
+def fp64_cpu_reference(rows, gpu_ref_y, gpu_ref_spp):
+    """The converged image of the FP64 CPU oracle (65,536 samples per pixel
+    of the oracle's restatement of the reference estimator, sums in double,
+    on the 32 x 32 pixel grid x, y = 16, 48, ..., 1008 of the same scene and
+    camera; tests/golden/make_guide_reference.py): how the GPU reference
+    (`gpu_ref_y`: Y of the measured rows, a torch tensor) agrees with it per
+    pixel, and relmse(img) of an image of the measured rows against it on
+    those pixels (exposed and with the reference's own noise removed as in
+    relmse_estimator).  None when the fixture is absent."""
+    if not os.path.exists(GUIDE_FP64_FIXTURE):
+        return None
+    fx = np.load(GUIDE_FP64_FIXTURE)
+    row_of = {y: i for i, y in enumerate(range(*rows))}
+    if not all(int(y) in row_of for y in fx["py"]):
+        return None
+    ri = np.array([row_of[int(y)] for y in fx["py"]])
+    px = np.asarray(fx["px"])
+    n = int(fx["spp"])
+    mean_c = fx["acc"][:, 1] / n
+    var_mean_c = np.maximum(fx["acc"][:, 3] / n - mean_c ** 2, 0.0) / n
+    scale = 1.0 / mean_c.mean()
+    ry = mean_c * scale
+    den = ry ** 2 + 1e-2
+    noise = float((var_mean_c * scale ** 2 / den).mean())
+    g = gpu_ref_y.cpu().numpy()[ri, px]
+    z = (g - mean_c) / np.sqrt(np.maximum(fx["acc"][:, 3] / n - mean_c ** 2, 0.0) * (1.0 / gpu_ref_spp + 1.0 / n)
+                               + 1e-30)
+
+    def relmse(img):
+        iy = img[..., 1].cpu().numpy()[ri, px] * scale
+        return float(((iy - ry) ** 2 / den).mean()) - noise
+
+    return {"relmse": relmse,
+            "summary": {"pixels": int(px.size), "spp": n, "sums": "float64",
+                        "tracer": "CPU oracle (C restatement of the reference's estimator), seed 77",
+                        "own_relmse": round(noise, 5),
+                        "gpu_reference_vs_oracle": {
+                            "mean_y_ratio": round(float(g.mean() / mean_c.mean()), 5),
+                            "fraction_beyond_3_sigma": round(float((np.abs(z) > 3).mean()), 4)}}}
+
+
 GUIDE_SETTINGS = dict(train_bounces=5, guide_bounces=9, alpha=0.5, steps_per_pass=512, batch_size=16384)
 # forward flops of one guide query, 2 (192 * 64 + 3 * 64 * 64 + 64 * 40)
 GUIDE_QUERY_FLOPS = 2 * (192 * 64 + 3 * 64 * 64 + 64 * 40)
@@ -391,6 +435,8 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
         def relmse(img):
             return relmse_y(img[..., 1])
 
+        cpu_ref = fp64_cpu_reference(rows, (a + b) / 2, ref_spp)
+
         def run(render_pass, train_passes=0):
             acc = torch.zeros((band, W, 3), dtype=torch.float64, device="cuda")
             film = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
@@ -417,6 +463,8 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
                        "training_seconds": round(sum(tr), 4),
                        "median_pass_ms": round(statistics.median(rd if rd else tr) * 1e3, 3),
                        "passes_times_median_seconds": round(robust, 3)}
+                if cpu_ref is not None and (e <= 0.01 or total > max_seconds):
+                    out["relmse_vs_fp64_cpu_oracle"] = round(cpu_ref["relmse"](acc / ((p - train_passes) * pass_spp)), 5)
                 if e <= 0.01:
                     return {"seconds": round(total, 3), "reached": True} | out
                 if total > max_seconds:
@@ -502,7 +550,8 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
                     "guided_seconds": [r[0]["seconds"] for r in guideds],
                     "guided_spp": [r[0]["spp"] for r in guideds]},
            "reference": {"spp": ref_spp, "seconds": round(ref_s, 2), "own_relmse": round(ref_noise, 5),
-                         "tracer": "plain GPU path tracer, float64 sums"},
+                         "tracer": "plain GPU path tracer, float64 sums",
+                         "fp64_cpu_oracle": cpu_ref["summary"] if cpu_ref else None},
            "time": "sum of the CUDA-event times of every pass (training passes included)",
            "config": f"occluded room, 196,146 triangles, 1024x1024 camera, {band} rows spread over the frame "
                      f"(rows {rows[0]}, {rows[0] + rows[2]}, ..., {row_list[-1]}), max depth 10, "

@@ -242,6 +242,8 @@ class PortLib(_Common):
         L.xyzo_eval_path.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_void_p]
         L.xyzo_eval_path.restype = C.c_int
         L.xyzo_render.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_void_p, C.c_int]
+        L.xyzo_render_pixels.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_uint64,
+                                         C.c_void_p, C.c_int]
         L.xyzo_light_area.restype = C.c_float
         L.xyzo_max_threads.restype = C.c_int
         L.xyzo_philox_u01.restype = C.c_float
@@ -262,6 +264,18 @@ class PortLib(_Common):
         self.kind = "port"
         self.light_scale = np.ones(3)
 
+
+    def render_pixels(self, px, py, spp: int, seed: int, s0: int = 0, acc=None, nthreads: int = 0):
+        """Per-pixel double sums over samples [s0, s0 + spp) of the listed
+        pixels: (n, 4) float64 rows (sum X, sum Y, sum Z, sum Y^2), added to
+        `acc` when given."""
+        px = np.ascontiguousarray(px, np.int32)
+        py = np.ascontiguousarray(py, np.int32)
+        if acc is None:
+            acc = np.zeros((px.shape[0], 4), np.float64)
+        self.lib.xyzo_render_pixels(px.shape[0], px.ctypes.data, py.ctypes.data, s0, spp, C.c_uint64(seed),
+                                    acc.ctypes.data, nthreads)
+        return acc
     def _set_path(self, kmax, rr_threshold, rr_start):
         self.lib.xyzo_set_path_params(kmax, rr_threshold, rr_start)
 

@@ -1039,6 +1039,9 @@ typedef struct {
   int spp;
   const float *dfilm;
   double *g_alb, *g_em;
+  /* pixels: samples [s, s + spp) of pixels [lo, hi) of the list px, py */
+  const int *px, *py;
+  double *acc;
 } job_t;
 
 static int job_take(job_t *j, int *b, int *e) {
@@ -1078,9 +1081,32 @@ static void *adjoint_worker(job_t *j) {
   return NULL;
 }
 
+static void *pixels_worker(job_t *j) {
+  int b, e;
+  while (job_take(j, &b, &e))
+    for (int i = b; i < e; ++i) {
+      double sx = 0, sy = 0, sz = 0, syy = 0;
+      for (int s = j->s; s < j->s + j->spp; ++s) {
+        f3 c;
+        eval_path(j->px[i], j->py[i], s, j->seed, &c);
+        sx += c.x;
+        sy += c.y;
+        sz += c.z;
+        syy += (double)c.y * c.y;
+      }
+      double *a = j->acc + 4 * (size_t)i;
+      a[0] += sx;
+      a[1] += sy;
+      a[2] += sz;
+      a[3] += syy;
+    }
+  return NULL;
+}
+
 static void *job_worker(void *arg) {
   job_t *j = (job_t *)arg;
   if (j->mode == 2) return adjoint_worker(j);
+  if (j->mode == 3) return pixels_worker(j);
   int b, e;
   while (job_take(j, &b, &e)) {
     for (int i = b; i < e; ++i) {
@@ -1192,6 +1218,27 @@ void xyzo_render(int s0, int spp, uint64_t seed, int y0, int y1, float *film, in
     j.film = film;
     run_job(&j, nthreads);
   }
+}
+
+/* Per-pixel statistics in double for reference images (test and benchmark
+ * infrastructure): for each listed pixel (px[i], py[i]), the samples
+ * [s0, s0 + spp) of PathTracer::run's estimator are evaluated and
+ * acc[4 i .. 4 i + 3] += (sum X, sum Y, sum Z, sum Y^2), summed in double. */
+void xyzo_render_pixels(int n, const int *px, const int *py, int s0, int spp, uint64_t seed, double *acc,
+                        int nthreads) {
+  job_t j;
+  memset(&j, 0, sizeof(j));
+  j.mode = 3;
+  j.lo = 0;
+  j.hi = n;
+  j.chunk = 1;
+  j.s = s0;
+  j.spp = spp;
+  j.seed = seed;
+  j.px = px;
+  j.py = py;
+  j.acc = acc;
+  run_job(&j, nthreads);
 }
 
 int xyzo_max_threads(void) { return default_threads(0); }
