@@ -212,6 +212,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_bf16_sustained():
+    """Dense bf16 TFLOP/s of a seconds-long cuBLAS loop (MEASURED_PEAKS.json),
+    the denominator for a kernel timed inside a long step; else the fallback."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if "bf16_tflops_sustained" in d:
+            return float(d["bf16_tflops_sustained"]), "measured"
+    return 1400.0, "fallback"
+
+
 def adjoint_bench(steps: int, warmup: int):
     """Differentiable-rendering iteration on the 19,392-triangle room: render
     512 x 512 x 32 spp, L2 loss gradient to a target, 32 spp path-replay adjoint
@@ -499,11 +511,14 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
                 nb = min(depth - 1, gcfg.get("guide_bounces", depth))
                 queries = sum(pr["ext_rays_by_iter"][:nb])
                 gms = pr["ms"]["guide"]
+                tf = queries * GUIDE_QUERY_FLOPS / (gms * 1e-3) / 1e12 if gms > 0 else None
+                bf16, bf16_kind = measured_bf16_sustained()
                 info["profiled_pass"] = {
                     "ms": {k: round(v, 3) for k, v in pr["ms"].items()},
                     "guide_queries": queries,
-                    "guide_inference_tflops": round(queries * GUIDE_QUERY_FLOPS / (gms * 1e-3) / 1e12, 1)
-                    if gms > 0 else None}
+                    "guide_inference_tflops": round(tf, 1) if tf else None,
+                    "guide_inference_frac_of_bf16_sustained": round(tf / bf16, 4) if tf else None,
+                    "bf16_sustained_tflops": bf16, "bf16_peak_source": bf16_kind}
                 return res, info
 
         def importon_run(particles):

@@ -77,7 +77,9 @@ typedef struct {
    * next-event estimation MIS-weighted against that lobe (xyz/bsdf/metal.cpp
    * built with CONFIG_EXPLICIT_GLOSSY); its albedo multiplies the throughput as
    * Lambert's does.  Scenes with MIRROR or METAL render in the XYZ film mode
-   * with xyzgpu_render, xyzgpu_render_noalloc and batches only. */
+   * with xyzgpu_render and batches only (xyzgpu_render_noalloc takes MIRROR
+   * but refuses METAL, whose shadow records need a per-path array it does
+   * not hold; the guided and importance-driven tracers refuse both). */
   const int32_t *material_kind; /* n_materials, or NULL */
   const float *shininess;       /* n_materials (METAL exponent), or NULL */
 } xyzgpu_scene_desc;

@@ -53,6 +53,23 @@ def test_noalloc_render_splits_pixels_and_samples_over_waves():
             assert torch.equal(film, ref), c
 
 
+def test_noalloc_render_takes_mirror_scenes():
+    """Mirror materials (no per-path shadow-record extras) render as
+    xyzgpu_render does; metal scenes are refused (test_materials_gpu)."""
+    import torch
+    from xyz_b200 import api, scenes
+    sd = scenes.cornell_specular()
+    kinds = sd.material_kind.copy()
+    kinds[kinds == api.MATERIAL_METAL] = api.MATERIAL_LAMBERT
+    sd.material_kind = kinds
+    assert (kinds == api.MATERIAL_MIRROR).any()
+    with api.Scene(sd) as s:
+        for c in (dict(cam=sd.camera, W=64, H=48, spp=4, seed=2, depth=9),
+                  dict(cam=sd.camera, W=32, H=24, spp=3, seed=4, depth=5, wave_paths=700)):
+            film, ref = _render_pair(s, c)
+            assert torch.equal(film, ref), c
+
+
 def test_noalloc_render_rejects_sizes_beyond_its_limits():
     import numpy as np
     import torch
