@@ -612,19 +612,41 @@ def gpu_lead(ms: float = 100.0):
     torch.cuda._sleep(int(ms * 1e-3 * 1.9e9))
 
 
-def profiled_traffic():
-    """DRAM bytes per traced ray of the trace kernel from the committed ncu
-    summary (profiles/trace_queue_spheres1m.txt), if present."""
+def profiled_traffic(key: str = "dram_bytes_per_ray"):
+    """Bytes per traced ray of the trace kernel (`key`: dram_bytes_per_ray or
+    l2_bytes_per_ray) from the committed ncu summary
+    (profiles/trace_queue_spheres1m.txt), if present."""
     p = os.path.join(ROOT, "profiles", "trace_queue_spheres1m.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_ray:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
                 return None
     return None
+
+
+def measure_l2_copy_gbs(mib: int = 8, reps: int = 200):
+    """L2 bandwidth of a device copy whose buffers (2 x `mib` MiB) stay in
+    L2: read + write bytes over CUDA-event time, best of three runs."""
+    import torch
+    n = mib * (1 << 20) // 4
+    a = torch.ones(n, device="cuda")
+    b = torch.empty_like(a)
+    best = 0.0
+    for _ in range(3):
+        for _ in range(10):
+            b.copy_(a)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * a.nbytes * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    return best
 
 
 def run_gpu_arm(args, rank, world):
@@ -733,6 +755,16 @@ def run_gpu_arm(args, rank, world):
         "kernel_share": {c: round(ms_cls[c] / max(1e-9, sum(ms_cls.values())), 4) for c in api.KERNEL_CLASSES},
         "grays_per_s": round(rays / (trace_ms / 1000.0) / 1e9, 3) if trace_ms > 0 else None,
     }
+    # the traversal's working set (tree and triangles, about 100 MB) lives in
+    # L2, so its roof is also stated against a copy that stays in L2
+    l2_per_ray = profiled_traffic("l2_bytes_per_ray")
+    if l2_per_ray is not None and trace_ms > 0:
+        l2_peak = measure_l2_copy_gbs()
+        l2_ach = l2_per_ray * rays / (trace_ms * 1e-3) / 1e9
+        roofline["l2"] = {"achieved": round(l2_ach, 1), "peak": round(l2_peak, 1), "unit": "GB/s",
+                          "frac": round(l2_ach / l2_peak, 4), "bytes_per_ray": l2_per_ray,
+                          "peak_source": "measured in this run: device copy of 2 x 8 MiB buffers (in L2)",
+                          "bytes_source": "lts__t_bytes per ray, profiles/trace_queue_spheres1m.txt"}
 
     # end to end through the C ABI with host buffers: upload + build + render + read back
     e2e = None
@@ -746,14 +778,21 @@ def run_gpu_arm(args, rank, world):
         # upload, the build's per-level reads, the film read-back); the value
         # uses the median step so that a host stall on a shared machine does
         # not stand for the path's cost; the total is reported beside it
-        step_s = []
+        step_s, parts = [], []
         for k in range(args.steps):
             t0 = time.perf_counter()
-            with api.Scene(sd) as s2:
+            s2 = api.Scene(sd)
+            t1 = time.perf_counter()
+            try:
                 s2.render(cam, W_PIX, H_PIX, SPP, seed=SEED, spp_offset=offset, max_depth=MAX_DEPTH,
                           film=host_film)
+                t2 = time.perf_counter()
+            finally:
+                s2.close()
             torch.cuda.synchronize()
-            step_s.append(time.perf_counter() - t0)
+            t3 = time.perf_counter()
+            step_s.append(t3 - t0)
+            parts.append((t1 - t0, t2 - t1, t3 - t2))
         e2e_s, total_s = statistics.median(step_s), sum(step_s)
         if dist is not None:
             t = torch.tensor([e2e_s, total_s], device="cuda", dtype=torch.float64)
@@ -762,6 +801,8 @@ def run_gpu_arm(args, rank, world):
         e2e = {"value": round(samples_per_step * world / e2e_s / 1e6, 3), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(host_film.nbytes),
                "median_step_ms": round(e2e_s * 1e3, 2),
+               "median_ms": {name: round(statistics.median(p[i] for p in parts) * 1e3, 2)
+                             for i, name in enumerate(("scene_create", "render_with_film_copies", "scene_destroy"))},
                "value_from_total_time": round(samples_per_step * world * args.steps / total_s / 1e6, 3),
                "includes": "scene upload + kd-tree build + render + film read-back, every step"}
 

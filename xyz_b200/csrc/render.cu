@@ -176,21 +176,27 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   if (rc) return rc;
   if (!sw.done) XYZ_CUDA_TRY(cudaEventCreateWithFlags(&sw.done, cudaEventDisableTiming));
   RenderWorkspace const &wv = sw.ws;
+  // Host films go through one device film and one pinned buffer per device
+  // (kept across scenes, so a program that creates a scene per frame does not
+  // pin and unpin host memory every time); the device lock held for the whole
+  // call serialises their use, and the call returns only after the read-back.
+  RenderWorkspace &fs = sw.ws;
   if (!adj && rp.film_location == XYZGPU_FILM_HOST) {
-    if (w.film_elems < film_elems) {
-      cudaFree(w.film_dev);
-      cudaFreeHost(w.film_pinned);
-      w.film_dev = nullptr;
-      w.film_pinned = nullptr;
-      w.film_elems = 0;
-      XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&w.film_dev), film_elems * sizeof(float)));
-      XYZ_CUDA_TRY(cudaMallocHost(reinterpret_cast<void **>(&w.film_pinned), film_elems * sizeof(float)));
-      w.film_elems = film_elems;
+    if (fs.film_elems < film_elems) {
+      XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+      cudaFree(fs.film_dev);
+      cudaFreeHost(fs.film_pinned);
+      fs.film_dev = nullptr;
+      fs.film_pinned = nullptr;
+      fs.film_elems = 0;
+      XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&fs.film_dev), film_elems * sizeof(float)));
+      XYZ_CUDA_TRY(cudaMallocHost(reinterpret_cast<void **>(&fs.film_pinned), film_elems * sizeof(float)));
+      fs.film_elems = film_elems;
     }
-    film_dev = w.film_dev;
+    film_dev = fs.film_dev;
     if (rp.accumulate) {
-      std::memcpy(w.film_pinned, film, film_elems * sizeof(float));
-      XYZ_CUDA_TRY(cudaMemcpyAsync(film_dev, w.film_pinned, film_elems * sizeof(float),
+      std::memcpy(fs.film_pinned, film, film_elems * sizeof(float));
+      XYZ_CUDA_TRY(cudaMemcpyAsync(film_dev, fs.film_pinned, film_elems * sizeof(float),
                                    cudaMemcpyHostToDevice, st));
     }
   }
@@ -419,9 +425,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   XYZ_CUDA_TRY(cudaEventRecord(sw.done, st));
   sw.last = st;
   if (!adj && rp.film_location == XYZGPU_FILM_HOST) {
-    XYZ_CUDA_TRY(cudaMemcpyAsync(w.film_pinned, film_dev, film_elems * sizeof(float), cudaMemcpyDeviceToHost, st));
+    XYZ_CUDA_TRY(cudaMemcpyAsync(fs.film_pinned, film_dev, film_elems * sizeof(float), cudaMemcpyDeviceToHost, st));
     XYZ_CUDA_TRY(cudaStreamSynchronize(st));
-    std::memcpy(film, w.film_pinned, film_elems * sizeof(float));
+    std::memcpy(film, fs.film_pinned, film_elems * sizeof(float));
   }
   rc_out.kernel_launches = launches;
   s.counters = rc_out;
