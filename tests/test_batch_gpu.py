@@ -130,3 +130,34 @@ def test_batch_argument_checks():
     finally:
         for s in scenes_:
             s.close()
+
+
+def test_batch_films_match_the_oracle_on_the_same_streams():
+    """Each job of a batch against the CPU oracle (the restatement pinned to
+    the reference's renderer) directly, not only through single renders."""
+    import torch
+    from tests.helpers import ensure_port
+    from xyz_b200 import api, scenes
+    entries = [(scenes.cornell_box(pinhole=True), 48, 36, 4, 3), (scenes.batch_scene(1, target_tris=4000), 40, 32, 3, 8),
+               (scenes.spheres_scene(level=2, n_spheres=2, seed=4), 32, 24, 5, 21)]
+    scenes_ = [api.Scene(sd) for sd, *_ in entries]
+    try:
+        jobs = [api.BatchJob(s, sd.camera, w, h, spp, seed=seed, max_depth=8)
+                for s, (sd, w, h, spp, seed) in zip(scenes_, entries)]
+        with api.Batch(jobs) as b:
+            b.launch()
+            torch.cuda.synchronize()
+            films = [j.film.cpu().numpy() for j in jobs]
+    finally:
+        for s in scenes_:
+            s.close()
+    P = ensure_port()
+    P.set_spectral(0, 1)
+    for (sd, w, h, spp, seed), film in zip(entries, films):
+        P.scene_create(sd)
+        P.set_camera(sd.camera, w, h)
+        P.set_path_params(max_depth=8)
+        ref = P.render(spp, seed=seed, nthreads=0)
+        close = (np.abs(film - ref) <= 1e-6 + 1e-4 * np.abs(ref)).all(axis=-1).mean()
+        assert close >= 0.98, close
+        assert abs(film.sum() - ref.sum()) / ref.sum() < 1e-2

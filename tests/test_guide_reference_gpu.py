@@ -53,3 +53,64 @@ def test_gpu_render_agrees_with_the_fp64_cpu_oracle_per_pixel():
     # X and Z follow Y's light: the channels' ratios agree as well
     assert abs(g[:, 0].sum() / (cpu[:, 0].sum() / n_cpu) - 1.0) < 0.015
     assert abs(g[:, 2].sum() / (cpu[:, 2].sum() / n_cpu) - 1.0) < 0.015
+
+
+def _passes_vs_oracle(render_pass, K, spp):
+    """Per-pixel z of the mean of K independent passes (spp samples each, on
+    the fixture's rows) against the FP64 CPU oracle, with each estimate's
+    variance of the mean: the passes' sample variance / K, the oracle's
+    per-sample variance / its sample count."""
+    import torch
+    fx = np.load(FIXTURE)
+    px, py = fx["px"], fx["py"]
+    ri = (py - 16) // 32
+    n_cpu = int(fx["spp"])
+    ys = []
+    for k in range(K):
+        f = render_pass(k)
+        ys.append(f[16::32][ri, px, 1].double().cpu().numpy() / spp)
+        torch.cuda.synchronize()
+    ys = np.stack(ys)
+    mg, vg = ys.mean(axis=0), ys.var(axis=0, ddof=1) / K
+    mc = fx["acc"][:, 1] / n_cpu
+    vc = np.maximum(fx["acc"][:, 3] / n_cpu - mc ** 2, 0.0) / n_cpu
+    z = (mg - mc) / np.sqrt(vg + vc + 1e-30)
+    return z, mg, mc
+
+
+def _guide_scene():
+    from xyz_b200 import scenes
+    fx = np.load(FIXTURE)
+    c = fx["camera"]
+    cam = scenes.Camera.with_fov(tuple(c[:3]), tuple(c[3:6]), float(c[6]), pinhole=True)
+    return scenes.occluded_room(), cam, int(fx["width"]), int(fx["height"]), int(fx["max_depth"])
+
+
+def test_trained_guide_agrees_with_the_fp64_cpu_oracle_per_pixel():
+    """The learned guide (trained online on these rows, as in the benchmark)
+    leaves the estimate unbiased: per pixel within 3 sigma of the oracle."""
+    from xyz_b200 import api
+    sd, cam, W, H, depth = _guide_scene()
+    rows = (16, H, 32)
+    K, spp = 32, 128
+    with api.Scene(sd) as s, api.Guide(s, train_bounces=5, guide_bounces=9, alpha=0.5, steps_per_pass=512,
+                                       batch_size=16384) as g:
+        for p in range(8):
+            g.render(cam, W, H, 64, seed=41, spp_offset=64 * p, max_depth=depth, rows=rows, train=True)
+        assert g.stats()["adam_steps"] > 0
+        z, mg, mc = _passes_vs_oracle(
+            lambda k: g.render(cam, W, H, spp, seed=43, spp_offset=spp * k, max_depth=depth, rows=rows), K, spp)
+    assert (np.abs(z) > 3).mean() < 0.025, np.sort(np.abs(z))[-8:]
+    assert abs(mg.mean() / mc.mean() - 1.0) < 0.02
+
+
+def test_importance_driven_tracer_agrees_with_the_fp64_cpu_oracle_per_pixel():
+    from xyz_b200 import api
+    sd, cam, W, H, depth = _guide_scene()
+    rows = (16, H, 32)
+    K, spp = 32, 128
+    with api.Scene(sd) as s, api.Importons(s, particles=100000, seed=5) as m:
+        z, mg, mc = _passes_vs_oracle(
+            lambda k: m.render(cam, W, H, spp, seed=47, spp_offset=spp * k, max_depth=depth, rows=rows), K, spp)
+    assert (np.abs(z) > 3).mean() < 0.025, np.sort(np.abs(z))[-8:]
+    assert abs(mg.mean() / mc.mean() - 1.0) < 0.02

@@ -56,11 +56,22 @@ def test_mirror_and_metal_agree_per_pixel_on_independent_streams():
         s2 += f * f
     mo = s1 / spp
     se = np.sqrt(np.maximum(s2 / spp - mo * mo, 0.0) / spp)
+    g1 = np.zeros((H, W, 3))
+    g2 = np.zeros((H, W, 3))
     with api.Scene(sd) as s:
-        mg = s.render(sd.camera, W, H, spp, seed=12, max_depth=depth).cpu().numpy().astype(np.float64) / spp
-    z = np.abs(mg - mo)[..., 1] / np.maximum(np.sqrt(2.0) * se[..., 1], 1e-12)
-    valid = se[..., 1] > 0
-    assert (z[valid] > 3.0).mean() < 0.02
+        for k in range(spp):
+            f = s.render(sd.camera, W, H, 1, seed=12, spp_offset=k, max_depth=depth).cpu().numpy().astype(np.float64)
+            g1 += f
+            g2 += f * f
+    mg = g1 / spp
+    sg = np.sqrt(np.maximum(g2 / spp - mg * mg, 0.0) / spp)
+    # each side's own standard error: a pixel whose few samples on one side
+    # missed a rare specular path has a near-zero variance estimate there
+    # (two runs of the reference itself fail a test that doubles one side's)
+    comb = np.sqrt(se[..., 1] ** 2 + sg[..., 1] ** 2)
+    valid = comb > 0
+    z = np.abs(mg - mo)[..., 1][valid] / comb[valid]
+    assert (z > 3.0).mean() < 0.02
     assert abs(mg.mean() / mo.mean() - 1.0) < 0.02
 
 

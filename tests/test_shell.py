@@ -80,11 +80,16 @@ def _lambert_document(path):
     mats = ['\t"white" shader(3) col(1.000 1.000 1.000 1.000) dif(0.800) amb(0.600) emi(0.000) spc(0.700) power(5.00)',
             '\t"lamp" shader(3) col(1.000 1.000 1.000 1.000) dif(0.800) amb(0.600) emi(1.000) spc(0.000) power(5.00)',
             '\t"cloth mcc-red" shader(3) col(0.2 0.3 0.4 1.000) dif(0.800) amb(0.600) emi(0.000) spc(0.500) power(5.00)']
+    # the camera inside the room (its boxes' faces point inwards), the lamp a
+    # ceiling quad facing down
     lines = ["Metasequoia Document", "Format Text Ver 1.0", "",
-             "Scene {", "\tpos 0.0000 0.0000 900.0000", "\tlookat 0.0000 100.0000 0.0000", "\thead 0.0000",
+             "Scene {", "\tpos 0.0000 0.0000 95.0000", "\tlookat 0.0000 100.0000 0.0000", "\thead 0.0000",
              "\tpich 0.0000", "}", f"Material {len(mats)} {{"] + mats + ["}"]
     lines += _box_obj("room", (-100, 0, -100), (100, 200, 100), 0)
-    lines += _box_obj("lamp", (-20, 199, -20), (20, 199.9, 20), 1)
+    lines += ['Object "lamp" {', "\tvisible 15", "\tshading 0", "\tvertex 4 {",
+              "\t\t-25.0000 199.0000 -25.0000", "\t\t25.0000 199.0000 -25.0000", "\t\t25.0000 199.0000 25.0000",
+              "\t\t-25.0000 199.0000 25.0000", "\t}", "\tface 2 {", "\t\t3 V(0 2 1) M(1)", "\t\t3 V(0 3 2) M(1)",
+              "\t}", "}"]
     lines += _icosphere_obj("ball", (-30, 40, 0), 35, 1, 2)
     lines += ["Eof"]
     open(path, "w").write("\n".join(lines) + "\n")

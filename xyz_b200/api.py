@@ -326,8 +326,8 @@ class Scene:
                 d.light_power_spd[k] = float(sd.light_power_spd[k])
         if getattr(sd, "material_kind", None) is not None:
             d.material_kind = keep(sd.material_kind, np.int32)
-            d.shininess = keep(sd.shininess if sd.shininess is not None
-                               else np.ones(d.n_materials, np.float32), np.float32)
+            # no exponents: NULL, which the library accepts unless a material is metal
+            d.shininess = keep(sd.shininess, np.float32) if sd.shininess is not None else None
         bp = default_build_params(**build_kw)
         h = C.c_void_p()
         _check(L.xyzgpu_scene_create(C.byref(d), C.byref(bp), C.byref(h)))

@@ -140,6 +140,9 @@ __global__ void k_film_tonemap(const float *__restrict__ film, int W, int H, Ton
     o[2] = tone_one(c[0], T, white);
     o[1] = tone_one(c[1], T, white);
     o[0] = tone_one(c[2], T, white);
+    // the row's padding bytes are zero (the caller's buffer may hold anything)
+    if (x == W - 1)
+      for (int64_t b = 3 * static_cast<int64_t>(W); b < stride_b; ++b) out[y * stride_b + b] = 0;
   }
 }
 
