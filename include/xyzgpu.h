@@ -92,12 +92,12 @@ typedef struct {
  * max_depth = 16), SAH without traversal / intersection constants,
  * xyz/geom/kdtree.hpp:19-20, kdtree.cpp:261-272). */
 typedef struct {
-  int leaf_max_tris;      /* make a leaf at or below this many triangles (4) */
+  int leaf_max_tris;      /* make a leaf at or below this many triangles (8) */
   int max_depth;          /* depth limit; 0 = 8 + 1.3 * log2(n_triangles) */
   float cost_traversal;   /* SAH traversal cost (1.0) */
   float cost_intersect;   /* SAH intersection cost (1.5) */
-  float empty_bonus;      /* SAH discount for a split with an empty side (0.2) */
-  int bins;               /* SAH bins per axis per node (32, max 64) */
+  float empty_bonus;      /* SAH discount for a split with an empty side (0) */
+  int bins;               /* SAH bins per axis per node (64, the maximum) */
   int builder;            /* XYZGPU_BUILD_DEVICE (default) or XYZGPU_BUILD_HOST */
   int max_refs_factor;    /* reference budget = factor * n_triangles (6) */
 } xyzgpu_build_params;

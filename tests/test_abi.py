@@ -52,7 +52,7 @@ def test_philox_known_answer():
 def test_defaults():
     from xyz_b200 import api
     bp = api.default_build_params()
-    assert (bp.leaf_max_tris, bp.bins) == (4, 32)
+    assert (bp.leaf_max_tris, bp.bins, bp.empty_bonus) == (8, 64, 0.0)
     assert abs(bp.cost_traversal - 1.0) < 1e-7 and abs(bp.cost_intersect - 1.5) < 1e-7
     rp = api.RenderParams()
     api.load_library().xyzgpu_render_params_default(C.byref(rp))

@@ -34,7 +34,7 @@ def test_light_particles_leave_the_oracles_importons():
         want = P.importons_emit(20000, 16, 1, seed=7)
         with api.Scene(sd) as s, api.Importons(s, particles=20000, seed=7) as m:
             got = m.importons()
-        assert got.shape[0] > 1000
+        assert got.shape[0] > 150   # the open sphere scene keeps few: most particles leave it
         # cosf / sinf of the device and of the host C library may differ in
         # the last bit, so an importon may differ from the oracle's in the last
         # bits of its position and direction (about half are bit-identical),

@@ -255,10 +255,14 @@ __global__ void k_imp_scatter(const float4 *pos, const float4 *dir, int64_t n, c
 // importon counts if it arrives from above the shading normal and its point,
 // moved along its direction onto the tangent plane, lies within the radius.
 // Writes the cumulative counts c[1..16].
-XYZ_DEV void importon_histogram(const ImpGrid &M, f3 pos, f3 sn, f3 tan, f3 bin, float *out16) {
-  float c[16];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) c[k] = 16.0f;
+// One query's histogram, computed by a whole warp: the lanes stride over the
+// importons of the cells around `pos` (consecutive lanes read consecutive
+// importons), each puts its importon in a bin, and 16 ballots per round count
+// the bins (lane k keeps bin k).  Every bin starts at 16 counts; lanes 0..15
+// return the cumulative counts (integers, exact in float below 2^24).  All
+// lanes of the warp call this with the same query.
+XYZ_DEV float importon_histogram_warp(const ImpGrid &M, f3 pos, f3 sn, f3 tan, f3 bin, int lane) {
+  unsigned mine = 0;
   int const x0 = cell_of(pos.x - M.cs, M.lo.x, M.cs, M.g0), x1 = cell_of(pos.x + M.cs, M.lo.x, M.cs, M.g0);
   int const y0 = cell_of(pos.y - M.cs, M.lo.y, M.cs, M.g1), y1 = cell_of(pos.y + M.cs, M.lo.y, M.cs, M.g1);
   int const z0 = cell_of(pos.z - M.cs, M.lo.z, M.cs, M.g2), z1 = cell_of(pos.z + M.cs, M.lo.z, M.cs, M.g2);
@@ -266,56 +270,69 @@ XYZ_DEV void importon_histogram(const ImpGrid &M, f3 pos, f3 sn, f3 tan, f3 bin,
     for (int y = y0; y <= y1; ++y) {
       int const row = (z * M.g1 + y) * M.g0;
       int const b = __ldg(&M.start[row + x0]), e = __ldg(&M.start[row + x1 + 1]);
-      for (int q = b; q < e; ++q) {
-        float4 const p4 = __ldg(&M.pos[q]);
-        f3 const d = mk3(p4.x - pos.x, p4.y - pos.y, p4.z - pos.z);
-        if (!(dot3(d, d) < M.r2)) continue;
-        f3 const dir = xyz3(__ldg(&M.dir[q]));
-        bool above;
-        int const k = importon_bin(dir, sn, tan, bin, &above);
-        if (!above) continue;
-        f3 const vp = add3(d, scl3(dir, dot3(d, sn)));
-        if (dot3(vp, vp) >= M.r2) continue;
-        c[k] += 1.0f;
+      for (int q0 = b; q0 < e; q0 += 32) {
+        int const q = q0 + lane;
+        int k = -1;
+        if (q < e) {
+          float4 const p4 = __ldg(&M.pos[q]);
+          f3 const d = mk3(p4.x - pos.x, p4.y - pos.y, p4.z - pos.z);
+          if (dot3(d, d) < M.r2) {
+            f3 const dir = xyz3(__ldg(&M.dir[q]));
+            bool above;
+            int const kk = importon_bin(dir, sn, tan, bin, &above);
+            f3 const vp = add3(d, scl3(dir, dot3(d, sn)));
+            if (above && dot3(vp, vp) < M.r2) k = kk;
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+          unsigned const m = __ballot_sync(0xffffffffu, k == t);
+          if (lane == t) mine += __popc(m);
+        }
       }
     }
-  float acc = 0.0f;
+  // inclusive prefix sum over lanes 0..15 of (16 + count)
+  unsigned acc = lane < 16 ? 16u + mine : 0u;
 #pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    acc = k == 0 ? c[0] : acc + c[k];
-    out16[k] = acc;
+  for (int off = 1; off < 16; off <<= 1) {
+    unsigned const o = __shfl_up_sync(0xffffffffu, acc, off);
+    if (lane >= off) acc += o;
   }
+  return static_cast<float>(acc);
 }
 
 // Histograms of an extension queue's hit points (computed as the shading
-// kernel computes them) for the importance-driven shading kernel.
+// kernel computes them) for the importance-driven shading kernel: one warp
+// per queue entry.
 __global__ void k_importon_query(DevScene S, ImpGrid M, const float4 *qo, const float4 *qd, const float4 *hits,
                                  const int32_t *count, float *cdf) {
   int const n = *count;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  int const lane = threadIdx.x & 31;
+  int64_t const warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
     float4 const h = hits[i];
     int32_t const code = __float_as_int(h.w);
-    if (code < 0) continue;
+    if (code < 0) continue;  // the same for the whole warp
     float4 const o4 = qo[i], d4 = qd[i];
     f3 const d = xyz3(d4);
     f3 gn, sn, tan, bin;
     shading_frame(S, code >> 1, code & 1, h.y, h.z, &gn, &sn, &tan, &bin);
     f3 const pos = add3(xyz3(o4), scl3(d, h.x));
-    float out[16];
-    importon_histogram(M, pos, sn, tan, bin, out);
-    float4 *dst = reinterpret_cast<float4 *>(cdf + 16 * static_cast<int64_t>(i));
-#pragma unroll
-    for (int q = 0; q < 4; ++q) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+    float const c = importon_histogram_warp(M, pos, sn, tan, bin, lane);
+    if (lane < 16) cdf[16 * i + lane] = c;
   }
 }
 
 // Histograms of caller-given frames (12 floats: position, tangent, binormal,
 // shading normal), for tests.
 __global__ void k_importon_query_frames(ImpGrid M, const float *fr, int n, float *out) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float *q = fr + 12 * static_cast<int64_t>(i);
-    importon_histogram(M, mk3(q[0], q[1], q[2]), mk3(q[9], q[10], q[11]), mk3(q[3], q[4], q[5]),
-                       mk3(q[6], q[7], q[8]), out + 16 * static_cast<int64_t>(i));
+  int const lane = threadIdx.x & 31;
+  int64_t const warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const float *q = fr + 12 * i;
+    float const c = importon_histogram_warp(M, mk3(q[0], q[1], q[2]), mk3(q[9], q[10], q[11]),
+                                            mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]), lane);
+    if (lane < 16) out[16 * i + lane] = c;
   }
 }
 
