@@ -51,7 +51,8 @@ def workload_config(stats=None):
     cfg = {
         "workload": "spheres-1M: 3 displaced level-7 icospheres + ground + spherical light r=0.3, "
                     "984,322 triangles, 1024x1024, 64 spp, max depth 10, pinhole fov 40, "
-                    "SAH kd-tree (Ct=1, Ci=1.5, leaf<=4), Lambert + NEE/MIS + Russian roulette, XYZ film",
+                    "SAH kd-tree (64 bins, Ct=1, Ci=1.5, leaf<=8, no empty bonus), Lambert + NEE/MIS + Russian roulette, "
+                    "XYZ film",
         "triangles": 984322, "width": W_PIX, "height": H_PIX, "spp": SPP, "max_depth": MAX_DEPTH,
         "seed": SEED, "l2_flush": "256 MiB buffer written between timed steps",
     }
