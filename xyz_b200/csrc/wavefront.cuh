@@ -533,8 +533,11 @@ struct ShadowSink {
   }
 };
 
+// CTAs per SM: extension rays run at 9 (56 registers, no spills: 5 % faster
+// than 10 CTAs at 48 registers with ~50 bytes of spills), shadow rays at 10
+// (measured on B200, 1M-triangle scene).
 template <bool kShadow, bool kCount, int kMode = kModePlain>
-__global__ void __launch_bounds__(kThreads, 10) k_trace_queue(WaveArgs A, int b,
+__global__ void __launch_bounds__(kThreads, kShadow ? 10 : 9) k_trace_queue(WaveArgs A, int b,
                                                           unsigned long long *prof) {
   constexpr bool kBatch = kMode == kModeBatch;
   int32_t *const cnt = A.counts + b * kCountStride;
