@@ -174,6 +174,30 @@ int check_device(int *dev) {
 
 // Material table update from device arrays: albedo (3 per material) into the
 // xyz of the float4 records, emission scale copied as is.
+// The material table from the caller's arrays (uploaded as they are): per
+// material (albedo XYZ, w) with w = 1 for a light, the kind for a mirror or
+// metal, else 0; the metal exponent (1 elsewhere); emission scale 1.  n = 0
+// leaves one zero material.
+__global__ void k_prepare_materials(int n, const float *__restrict__ albedo, const int32_t *__restrict__ is_light,
+                                    const int32_t *__restrict__ kind, const float *__restrict__ shininess,
+                                    float4 *__restrict__ mat, float *__restrict__ shin, float *__restrict__ emission) {
+  int const total = n > 0 ? n : 1;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < total; m += gridDim.x * blockDim.x) {
+    float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float e = 1.0f;
+    if (n > 0) {
+      int const k = kind ? kind[m] : XYZGPU_MATERIAL_LAMBERT;
+      bool const light = is_light[m] != 0;
+      float const kw = light ? 1.0f : (k != XYZGPU_MATERIAL_LAMBERT ? static_cast<float>(k) : 0.0f);
+      r = make_float4(albedo[3 * m], albedo[3 * m + 1], albedo[3 * m + 2], kw);
+      if (!light && k == XYZGPU_MATERIAL_METAL) e = shininess[m];
+    }
+    mat[m] = r;
+    shin[m] = e;
+    emission[m] = 1.0f;
+  }
+}
+
 __global__ void k_set_materials(float4 *__restrict__ mat, float *__restrict__ emission,
                                 const float *__restrict__ albedo_in, const float *__restrict__ emission_in,
                                 int nm) {
@@ -284,29 +308,19 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
     if (!std::isfinite(d->positions[i]))
       return set_error(XYZGPU_E_INVALID, "scene_create: vertex coordinate %lld is not finite",
                        static_cast<long long>(i));
-  std::vector<float4> mat(nm > 0 ? nm : 1);
   std::vector<int32_t> lights;
   std::vector<float> cdf(1, 0.0f);
   bool const smooth = d->normals != nullptr;
-  std::vector<float> shin(mat.size(), 1.0f);
   int n_specular = 0;
   for (int m = 0; m < nm; ++m) {
     int const kind = d->material_kind ? d->material_kind[m] : XYZGPU_MATERIAL_LAMBERT;
     if (kind != XYZGPU_MATERIAL_LAMBERT && kind != XYZGPU_MATERIAL_MIRROR && kind != XYZGPU_MATERIAL_METAL)
       return set_error(XYZGPU_E_INVALID, "scene_create: material %d has unknown kind %d", m, kind);
-    float kw = 0.0f;
-    if (d->is_light[m]) {
-      kw = 1.0f;
-    } else if (kind != XYZGPU_MATERIAL_LAMBERT) {
-      kw = static_cast<float>(kind);
-      ++n_specular;
-    }
+    if (!d->is_light[m] && kind != XYZGPU_MATERIAL_LAMBERT) ++n_specular;
     if (kind == XYZGPU_MATERIAL_METAL && !d->is_light[m]) {
       if (!d->shininess || !(d->shininess[m] > 0.0f) || !std::isfinite(d->shininess[m]))
         return set_error(XYZGPU_E_INVALID, "scene_create: metal material %d needs a shininess > 0", m);
-      shin[m] = d->shininess[m];
     }
-    mat[m] = make_float4(d->albedo_xyz[3 * m], d->albedo_xyz[3 * m + 1], d->albedo_xyz[3 * m + 2], kw);
   }
   for (int i = 0; i < nt; ++i) {
     int32_t const a = d->triangles[3 * i], b = d->triangles[3 * i + 1], c = d->triangles[3 * i + 2];
@@ -339,14 +353,23 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   configure_pool(dev);
   cudaStream_t const st = nullptr;
   int64_t bytes = 0, scratch = 0;
-  float *d_pos = nullptr, *d_nrm = nullptr, *d_box = nullptr;
-  int32_t *d_idx = nullptr, *d_tmat = nullptr;
-  auto fail = [&](int r) {
+  float *d_pos = nullptr, *d_nrm = nullptr, *d_box = nullptr, *d_alb = nullptr, *d_shin = nullptr;
+  int32_t *d_idx = nullptr, *d_tmat = nullptr, *d_lit = nullptr, *d_kind = nullptr;
+  auto free_temps = [&]() {
     cudaFreeAsync(d_pos, st);
     cudaFreeAsync(d_nrm, st);
     cudaFreeAsync(d_idx, st);
     cudaFreeAsync(d_tmat, st);
     cudaFreeAsync(d_box, st);
+    cudaFreeAsync(d_alb, st);
+    cudaFreeAsync(d_lit, st);
+    cudaFreeAsync(d_kind, st);
+    cudaFreeAsync(d_shin, st);
+    d_pos = d_nrm = d_box = d_alb = d_shin = nullptr;
+    d_idx = d_tmat = d_lit = d_kind = nullptr;
+  };
+  auto fail = [&](int r) {
+    free_temps();
     free_scene(s);
     return r;
   };
@@ -362,12 +385,24 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   XYZ_TRY(dev_alloc(&s->d_tri, 3 * static_cast<size_t>(nt), &bytes, st));
   XYZ_TRY(dev_alloc(&s->d_ng, static_cast<size_t>(nt), &bytes, st));
   if (smooth) XYZ_TRY(dev_alloc(&s->d_sn, 3 * static_cast<size_t>(nt), &bytes, st));
-  XYZ_TRY(dev_upload(&s->d_mat, mat.data(), mat.size(), &bytes, st));
-  XYZ_TRY(dev_upload(&s->d_shininess, shin.data(), shin.size(), &bytes, st));
+  // the material table is built on the device from the caller's arrays
+  // (copies of caller memory are fast; a table assembled in freshly
+  // allocated host memory uploads several times slower)
   {
-    std::vector<float> ones(mat.size(), 1.0f);
-    XYZ_TRY(dev_upload(&s->d_emission, ones.data(), ones.size(), &bytes, st));
-    // the upload's source is pageable host memory: the copy has completed on return
+    size_t const nmat = nm > 0 ? static_cast<size_t>(nm) : 1;
+    XYZ_TRY(dev_alloc(&s->d_mat, nmat, &bytes, st));
+    XYZ_TRY(dev_alloc(&s->d_shininess, nmat, &bytes, st));
+    XYZ_TRY(dev_alloc(&s->d_emission, nmat, &bytes, st));
+    if (nm > 0) {
+      XYZ_TRY(dev_upload(&d_alb, d->albedo_xyz, 3 * static_cast<size_t>(nm), &scratch, st));
+      XYZ_TRY(dev_upload(&d_lit, d->is_light, static_cast<size_t>(nm), &scratch, st));
+      if (d->material_kind) XYZ_TRY(dev_upload(&d_kind, d->material_kind, static_cast<size_t>(nm), &scratch, st));
+      if (d->shininess) XYZ_TRY(dev_upload(&d_shin, d->shininess, static_cast<size_t>(nm), &scratch, st));
+    }
+    k_prepare_materials<<<static_cast<int>(std::min<size_t>((nmat + 255) / 256, 4096)), 256, 0, st>>>(
+        nm, d_alb, d_lit, d_kind, d_shin, s->d_mat, s->d_shininess, s->d_emission);
+    cudaError_t const e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(set_error(XYZGPU_E_CUDA, "scene_create: %s", cudaGetErrorString(e)));
   }
   XYZ_TRY(dev_upload(&s->d_lights, lights.data(), lights.size(), &bytes, st));
   XYZ_TRY(dev_upload(&s->d_cdf, cdf.data(), cdf.size(), &bytes, st));
@@ -388,13 +423,7 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   if (cudaMemcpyAsync(box, d_box, sizeof(box), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return fail(set_error(XYZGPU_E_CUDA, "scene_create: triangle preparation failed"));
-  cudaFreeAsync(d_pos, st);
-  cudaFreeAsync(d_nrm, st);
-  cudaFreeAsync(d_idx, st);
-  cudaFreeAsync(d_tmat, st);
-  cudaFreeAsync(d_box, st);
-  d_pos = d_nrm = d_box = nullptr;
-  d_idx = d_tmat = nullptr;
+  free_temps();
 #undef XYZ_TRY
   // root box: the bounds grown by 1e-5 of the extent plus 1e-6 (kd_root_bounds)
   for (int k = 0; k < 3; ++k) {
