@@ -8,6 +8,9 @@
 #include <mutex>
 #include <new>
 
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
 #include "scene.h"
 
 namespace xyzgpu {
@@ -96,14 +99,26 @@ void free_scene(SceneImpl *s) {
 // constructor, xyz/geom/triangle.cpp:35-60): v0, e1 = v1 - v0, e2 = v2 - v0,
 // n = cross(e2, e1), ng = n / |n|, shading normals n0, s1 = n1 - n0,
 // s2 = n2 - n0.  Same float operations as the host (--fmad=false).
+// Vertex or material indices out of range set flag bit 2 and leave the
+// triangle out (nothing is read through them); light_flag[i] marks the
+// triangles of light materials.
 __global__ void k_prepare_triangles(const float *__restrict__ pos, const float *__restrict__ nrm,
                                     const int32_t *__restrict__ idx, const int32_t *__restrict__ tmat,
-                                    int nt, float4 *__restrict__ tri, float4 *__restrict__ ng,
+                                    int nt, int nv, int nm, const int32_t *__restrict__ is_light,
+                                    float4 *__restrict__ tri, float4 *__restrict__ ng,
                                     float4 *__restrict__ sn, float *__restrict__ box_min,
-                                    float *__restrict__ box_max) {
+                                    float *__restrict__ box_max, int *flag, int8_t *__restrict__ light_flag) {
   int const i = blockIdx.x * blockDim.x + threadIdx.x;
   float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  bool valid = false;
   if (i < nt) {
+    int const a = idx[3 * i], b = idx[3 * i + 1], c = idx[3 * i + 2];
+    int const m = tmat[i];
+    valid = a >= 0 && b >= 0 && c >= 0 && a < nv && b < nv && c < nv && m >= 0 && m < nm;
+    light_flag[i] = valid && is_light[m] != 0;
+    if (!valid) atomicOr(flag, 2);
+  }
+  if (valid) {
     int const a = idx[3 * i], b = idx[3 * i + 1], c = idx[3 * i + 2];
     f3 const p0 = mk3(pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]);
     f3 const p1 = mk3(pos[3 * b], pos[3 * b + 1], pos[3 * b + 2]);
@@ -155,6 +170,35 @@ __global__ void k_prepare_triangles(const float *__restrict__ pos, const float *
         atomicMin(reinterpret_cast<unsigned *>(&box_max[k]), static_cast<unsigned>(hv));
     }
   }
+}
+
+// Finite coordinates (flag bit 1).
+__global__ void k_check_finite(const float *__restrict__ p, int64_t n, int *flag) {
+  bool bad = false;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    bad = bad || !isfinite(p[i]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+// The caller's geometry checked on the host, for the message of the first
+// fault (run only when the device checks found one): the same order and
+// wording as the checks the device made.
+int host_geometry_error(const xyzgpu_scene_desc *d) {
+  int const nt = d->n_triangles, nv = d->n_vertices, nm = d->n_materials;
+  for (int64_t i = 0; i < 3ll * nv; ++i)
+    if (!std::isfinite(d->positions[i]))
+      return set_error(XYZGPU_E_INVALID, "scene_create: vertex coordinate %lld is not finite",
+                       static_cast<long long>(i));
+  for (int i = 0; i < nt; ++i) {
+    int32_t const a = d->triangles[3 * i], b = d->triangles[3 * i + 1], c = d->triangles[3 * i + 2];
+    int32_t const m = d->tri_material[i];
+    if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv)
+      return set_error(XYZGPU_E_INVALID, "scene_create: triangle %d has a vertex index out of range", i);
+    if (m < 0 || m >= nm)
+      return set_error(XYZGPU_E_INVALID, "scene_create: triangle %d has material %d out of range", i, m);
+  }
+  return set_error(XYZGPU_E_INVALID, "scene_create: invalid geometry");
 }
 
 int check_device(int *dev) {
@@ -304,12 +348,6 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   if (rc) return rc;
 
   int const nt = d->n_triangles, nv = d->n_vertices, nm = d->n_materials;
-  for (int64_t i = 0; i < 3ll * nv; ++i)
-    if (!std::isfinite(d->positions[i]))
-      return set_error(XYZGPU_E_INVALID, "scene_create: vertex coordinate %lld is not finite",
-                       static_cast<long long>(i));
-  std::vector<int32_t> lights;
-  std::vector<float> cdf(1, 0.0f);
   bool const smooth = d->normals != nullptr;
   int n_specular = 0;
   for (int m = 0; m < nm; ++m) {
@@ -322,31 +360,10 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
         return set_error(XYZGPU_E_INVALID, "scene_create: metal material %d needs a shininess > 0", m);
     }
   }
-  for (int i = 0; i < nt; ++i) {
-    int32_t const a = d->triangles[3 * i], b = d->triangles[3 * i + 1], c = d->triangles[3 * i + 2];
-    int32_t const m = d->tri_material[i];
-    if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv)
-      return set_error(XYZGPU_E_INVALID, "scene_create: triangle %d has a vertex index out of range", i);
-    if (m < 0 || m >= nm)
-      return set_error(XYZGPU_E_INVALID, "scene_create: triangle %d has material %d out of range", i, m);
-    if (d->is_light[m]) {
-      // light CDF in triangle order (xyz/core/scene_mqo.cpp:512-519), with the
-      // area of Triangle::area (xyz/geom/triangle.hpp:57-59)
-      f3 const p0 = mk3(d->positions[3 * a], d->positions[3 * a + 1], d->positions[3 * a + 2]);
-      f3 const p1 = mk3(d->positions[3 * b], d->positions[3 * b + 1], d->positions[3 * b + 2]);
-      f3 const p2 = mk3(d->positions[3 * c], d->positions[3 * c + 1], d->positions[3 * c + 2]);
-      f3 const n = cross3(sub3(p2, p0), sub3(p1, p0));
-      float const area = std::sqrt(dot3(n, n)) * 0.5f;
-      lights.push_back(i);
-      cdf.push_back(cdf.back() + area);
-    }
-  }
-
   SceneImpl *s = new (std::nothrow) SceneImpl();
   if (!s) return set_error(XYZGPU_E_NOMEM, "scene_create: host allocation failed");
   s->device = dev;
   s->n_tris = nt;
-  s->n_lights = static_cast<int>(lights.size());
   s->n_materials = nm;
   s->n_specular = n_specular;
   s->smooth = smooth;
@@ -354,8 +371,18 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   cudaStream_t const st = nullptr;
   int64_t bytes = 0, scratch = 0;
   float *d_pos = nullptr, *d_nrm = nullptr, *d_box = nullptr, *d_alb = nullptr, *d_shin = nullptr;
-  int32_t *d_idx = nullptr, *d_tmat = nullptr, *d_lit = nullptr, *d_kind = nullptr;
+  int32_t *d_idx = nullptr, *d_tmat = nullptr, *d_lit = nullptr, *d_kind = nullptr, *d_flag = nullptr,
+          *d_lid = nullptr;
+  int8_t *d_lflag = nullptr;
+  uint8_t *d_tmp = nullptr;
   auto free_temps = [&]() {
+    cudaFreeAsync(d_flag, st);
+    cudaFreeAsync(d_lid, st);
+    cudaFreeAsync(d_lflag, st);
+    cudaFreeAsync(d_tmp, st);
+    d_flag = d_lid = nullptr;
+    d_lflag = nullptr;
+    d_tmp = nullptr;
     cudaFreeAsync(d_pos, st);
     cudaFreeAsync(d_nrm, st);
     cudaFreeAsync(d_idx, st);
@@ -404,8 +431,6 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
     cudaError_t const e = cudaGetLastError();
     if (e != cudaSuccess) return fail(set_error(XYZGPU_E_CUDA, "scene_create: %s", cudaGetErrorString(e)));
   }
-  XYZ_TRY(dev_upload(&s->d_lights, lights.data(), lights.size(), &bytes, st));
-  XYZ_TRY(dev_upload(&s->d_cdf, cdf.data(), cdf.size(), &bytes, st));
   if (d->albedo_spd) XYZ_TRY(dev_upload(&s->d_spd, d->albedo_spd, 31 * static_cast<size_t>(nm), &bytes, st));
   XYZ_TRY(dev_alloc(&s->d_fetch, 64, &bytes, st));
   XYZ_TRY(dev_alloc(&s->d_trace_counts, 8, &bytes, st));
@@ -413,16 +438,55 @@ int xyzgpu_scene_create(const xyzgpu_scene_desc *d, const xyzgpu_build_params *b
   float const box_init[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
   if (cudaMemcpyAsync(d_box, box_init, sizeof(box_init), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return fail(set_error(XYZGPU_E_CUDA, "scene_create: copy failed"));
+  // checks of the caller's geometry on the device (finite coordinates,
+  // indices in range) and the light triangles in triangle order
+  XYZ_TRY(dev_alloc(&d_flag, 2, &scratch, st));
+  XYZ_TRY(dev_alloc(&d_lflag, static_cast<size_t>(nt), &scratch, st));
+  XYZ_TRY(dev_alloc(&d_lid, static_cast<size_t>(nt), &scratch, st));
+  if (cudaMemsetAsync(d_flag, 0, 2 * sizeof(int), st) != cudaSuccess)
+    return fail(set_error(XYZGPU_E_CUDA, "scene_create: memset failed"));
+  if (nv > 0) k_check_finite<<<static_cast<int>(std::min<int64_t>((3ll * nv + 255) / 256, 2048)), 256, 0, st>>>(
+      d_pos, 3ll * nv, d_flag);
   if (nt > 0) {
-    k_prepare_triangles<<<(nt + 255) / 256, 256, 0, st>>>(d_pos, d_nrm, d_idx, d_tmat, nt, s->d_tri, s->d_ng,
-                                                           s->d_sn, d_box, d_box + 3);
+    k_prepare_triangles<<<(nt + 255) / 256, 256, 0, st>>>(d_pos, d_nrm, d_idx, d_tmat, nt, nv, nm, d_lit, s->d_tri,
+                                                           s->d_ng, s->d_sn, d_box, d_box + 3, d_flag, d_lflag);
+    size_t tmp_bytes = 0;
+    thrust::counting_iterator<int32_t> ids(0);
+    if (cub::DeviceSelect::Flagged(nullptr, tmp_bytes, ids, d_lflag, d_lid, d_flag + 1, nt, st) != cudaSuccess)
+      return fail(set_error(XYZGPU_E_CUDA, "scene_create: light selection failed"));
+    XYZ_TRY(dev_alloc(&d_tmp, tmp_bytes, &scratch, st));
+    if (cub::DeviceSelect::Flagged(d_tmp, tmp_bytes, ids, d_lflag, d_lid, d_flag + 1, nt, st) != cudaSuccess)
+      return fail(set_error(XYZGPU_E_CUDA, "scene_create: light selection failed"));
     cudaError_t const e = cudaGetLastError();
     if (e != cudaSuccess) return fail(set_error(XYZGPU_E_CUDA, "scene_create: %s", cudaGetErrorString(e)));
   }
   float box[6];
+  int flags[2] = {0, 0};
   if (cudaMemcpyAsync(box, d_box, sizeof(box), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(flags, d_flag, sizeof(flags), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return fail(set_error(XYZGPU_E_CUDA, "scene_create: triangle preparation failed"));
+  if (flags[0]) return fail(host_geometry_error(d));
+  // light CDF in triangle order (xyz/core/scene_mqo.cpp:512-519), with the
+  // area of Triangle::area (xyz/geom/triangle.hpp:57-59)
+  std::vector<int32_t> lights(static_cast<size_t>(nt > 0 ? flags[1] : 0));
+  if (!lights.empty() && cudaMemcpy(lights.data(), d_lid, lights.size() * sizeof(int32_t),
+                                    cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(set_error(XYZGPU_E_CUDA, "scene_create: reading the light list failed"));
+  std::vector<float> cdf(1, 0.0f);
+  cdf.reserve(lights.size() + 1);
+  for (int32_t const i : lights) {
+    int32_t const a = d->triangles[3 * i], b = d->triangles[3 * i + 1], c = d->triangles[3 * i + 2];
+    f3 const p0 = mk3(d->positions[3 * a], d->positions[3 * a + 1], d->positions[3 * a + 2]);
+    f3 const p1 = mk3(d->positions[3 * b], d->positions[3 * b + 1], d->positions[3 * b + 2]);
+    f3 const p2 = mk3(d->positions[3 * c], d->positions[3 * c + 1], d->positions[3 * c + 2]);
+    f3 const n = cross3(sub3(p2, p0), sub3(p1, p0));
+    float const area = std::sqrt(dot3(n, n)) * 0.5f;
+    cdf.push_back(cdf.back() + area);
+  }
+  s->n_lights = static_cast<int>(lights.size());
+  XYZ_TRY(dev_upload(&s->d_lights, lights.data(), lights.size(), &bytes, st));
+  XYZ_TRY(dev_upload(&s->d_cdf, cdf.data(), cdf.size(), &bytes, st));
   free_temps();
 #undef XYZ_TRY
   // root box: the bounds grown by 1e-5 of the extent plus 1e-6 (kd_root_bounds)
