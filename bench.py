@@ -604,6 +604,25 @@ def guide_profile_case():
         print(json.dumps({"guide_profile_case": "ok", "film_sum": float(f.sum())}))
 
 
+def adjoint_profile_case():
+    """The adjoint's kernels on a small case for ncu: one primal render and
+    one path-replay adjoint of the 19,392-triangle room at 256 x 256, 8 spp
+    each, max depth 6 (the benchmark's iteration at a sixteenth of its
+    samples)."""
+    import torch
+    from xyz_b200 import api, diff, scenes
+    ds = scenes.diff_scene()
+    with api.Scene(ds.scene) as s:
+        R = diff.Renderer(s, ds.scene.camera, 256, 256, 8, adjoint_spp=8, adjoint_offset=8, max_depth=6,
+                          rr_threshold=0.0)
+        s.set_materials(ds.albedo, ds.emission)
+        img = R.render()
+        g = R.gradient(2.0 * img)
+        torch.cuda.synchronize()
+        print(json.dumps({"adjoint_profile_case": "ok", "film_sum": float(img.sum()),
+                          "grad_norm": float(sum(float(t.double().norm()) for t in g if t is not None))}))
+
+
 def gpu_lead(ms: float = 100.0):
     """Occupies the current stream for about `ms` (torch's spin kernel,
     outside any timed region) so that the host can enqueue the timed work
@@ -847,12 +866,17 @@ def main():
                     help="samples per pixel per step (default 64; smaller for profiler captures)")
     ap.add_argument("--guide-profile-case", action="store_true",
                     help="run only the guide kernels' small profiling case (for ncu) and exit")
+    ap.add_argument("--adjoint-profile-case", action="store_true",
+                    help="run only the adjoint kernels' small profiling case (for ncu) and exit")
     args = ap.parse_args()
     if args.spp is not None:
         global SPP
         SPP = max(1, args.spp)
     if args.guide_profile_case:
         guide_profile_case()
+        return
+    if args.adjoint_profile_case:
+        adjoint_profile_case()
         return
     if args.warmup < 3:
         args.warmup = 3
