@@ -63,8 +63,14 @@ def workload_config(stats=None):
 
 
 def make_scene():
+    """The workload's scene as the XYZ renderer takes it: XYZ albedos only (the
+    generator also makes 31-bin albedo spectra for the spectral modes, 122 MB
+    for this scene, which an XYZ render never reads)."""
     from xyz_b200 import scenes
-    return scenes.spheres_scene(level=7, n_spheres=3, seed=SEED)
+    sd = scenes.spheres_scene(level=7, n_spheres=3, seed=SEED)
+    sd.albedo_spd = None
+    sd.light_power_spd = None
+    return sd
 
 
 # ----------------------------------------------------------------- clocks
@@ -800,8 +806,9 @@ def run_gpu_arm(args, rank, world):
     e2e = None
     if not args.no_e2e:
         h2d = sum(int(a.nbytes) for a in (sd.positions, sd.tris, sd.tri_mat, sd.albedo_xyz, sd.is_light))
-        if sd.normals is not None:
-            h2d += int(sd.normals.nbytes)
+        for extra in (sd.normals, sd.albedo_spd, sd.material_kind, sd.shininess):
+            if extra is not None:
+                h2d += int(extra.nbytes)
         host_film = np.zeros((H_PIX, W_PIX, 3), np.float32)
         torch.cuda.synchronize()
         # wall time per step (the leg includes host work: the scene arrays'
