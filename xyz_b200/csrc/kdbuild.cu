@@ -180,18 +180,26 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock)
       }
     }
     __syncwarp();
-    // exclusive prefix in place: lane k < 6 owns row k
-    if (lane < 6) {
-      uint32_t *row = h + lane * (kKdMaxBins + 1);
-      uint32_t acc = 0u;
-      for (int b = 0; b < B; ++b) {
-        uint32_t const v = row[b];
-        row[b] = acc;
-        acc += v;
+    // exclusive prefix of each of the six rows in place, the whole warp per
+    // row: lane k holds bins 2k and 2k + 1 (B <= 64), an inclusive scan of
+    // the pairs' sums over the lanes; row[B] gets the total
+    for (int q = 0; q < 6; ++q) {
+      uint32_t *row = h + q * (kKdMaxBins + 1);
+      int const b0 = 2 * lane, b1 = 2 * lane + 1;
+      uint32_t const v0 = b0 < B ? row[b0] : 0u, v1 = b1 < B ? row[b1] : 0u;
+      uint32_t const pair = v0 + v1;
+      uint32_t incl = pair;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        uint32_t const t = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += t;
       }
-      row[B] = acc;
+      __syncwarp();
+      if (b0 < B) row[b0] = incl - pair;
+      if (b1 < B) row[b1] = incl - pair + v0;
+      if (lane == 31) row[B] = incl;
+      __syncwarp();
     }
-    __syncwarp();
     float best = INFINITY;
     int best_c = 0x7fffffff;
     for (int c = lane; c < 3 * (B - 1); c += 32) {
