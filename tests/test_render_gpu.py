@@ -143,6 +143,52 @@ def test_invalid_arguments_are_errors():
         api.Scene(bad2)
 
 
+def test_scene_checks_and_degenerate_scenes():
+    """The geometry checks made on the device word their errors as the host
+    checks do, the first fault in the host's order; a scene without lights
+    renders black (no emitter to hit or sample), and one without triangles
+    builds and renders black too."""
+    import torch
+    from xyz_b200 import api, scenes
+    bad = scenes.cornell_box()
+    bad.tri_mat = bad.tri_mat.copy()
+    bad.tri_mat[5] = bad.albedo_xyz.shape[0]
+    with pytest.raises(api.XyzGpuError) as e:
+        api.Scene(bad)
+    assert "triangle 5 has material" in str(e.value) and "out of range" in str(e.value)
+    bad = scenes.cornell_box()
+    bad.tris = bad.tris.copy()
+    bad.tris[7, 2] = -1
+    bad.tri_mat = bad.tri_mat.copy()
+    bad.tri_mat[9] = -3
+    with pytest.raises(api.XyzGpuError) as e:
+        api.Scene(bad)
+    assert "triangle 7 has a vertex index out of range" in str(e.value)
+    bad = scenes.cornell_box()
+    bad.positions = bad.positions.copy()
+    bad.positions[4, 2] = np.inf
+    bad.tris = bad.tris.copy()
+    bad.tris[1, 0] = 10_000
+    with pytest.raises(api.XyzGpuError) as e:
+        api.Scene(bad)
+    assert "vertex coordinate 14 is not finite" in str(e.value)
+    dark = scenes.cornell_box()
+    dark.is_light = np.zeros_like(dark.is_light)
+    with api.Scene(dark) as s:
+        assert s.stats()["n_lights"] == 0
+        f = s.render(dark.camera, 32, 24, 4, seed=1, max_depth=8)
+        torch.cuda.synchronize()
+        assert float(f.abs().sum()) == 0.0
+    empty = scenes.cornell_box()
+    empty.tris = np.zeros((0, 3), np.int32)
+    empty.tri_mat = np.zeros(0, np.int32)
+    with api.Scene(empty) as s:
+        assert s.stats()["n_triangles"] == 0
+        f = s.render(empty.camera, 16, 12, 2, seed=1, max_depth=8)
+        torch.cuda.synchronize()
+        assert float(f.abs().sum()) == 0.0
+
+
 def test_row_stride_renders_the_same_pixels_as_the_full_image():
     """rows=(begin, end, step): every step-th row of a band, the same paths as
     in the full image (bit-identical rows); rows not rendered stay zero."""
