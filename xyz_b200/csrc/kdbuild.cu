@@ -96,9 +96,8 @@ __global__ void k_classify(LevelArrays L, int m, BuildArgs a, int32_t *big_list,
 // SAH over the exclusive prefix sums pre[a][0][i] (starts) and pre[a][1][i]
 // (ends) of bins [0, i).  Candidate c = a * (B - 1) + (i - 1).  Returns the
 // cost; +inf for invalid candidates.
-XYZ_DEV float candidate_cost(const BuildArgs &A, const uint32_t *pre, int c, int n, const float ext[3],
+XYZ_DEV float candidate_cost(const BuildArgs &A, int B, const uint32_t *pre, int c, int n, const float ext[3],
                              float4 lo4, float4 hi4, float sa, float *plane_out, int *nl_out) {
-  int const B = A.bins;
   int const a = c / (B - 1);
   int const i = c - a * (B - 1) + 1;
   if (!(ext[a] > 0.0f)) return INFINITY;
@@ -144,9 +143,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock)
   uint32_t *h = hist[wib];
   int const warp = blockIdx.x * kWarpsPerBlock + wib;
   int const nwarps = gridDim.x * kWarpsPerBlock;
-  int const B = A.bins;
   for (int j = warp; j < m; j += nwarps) {
     int const n = L.count[j];
+    int const B = kd_node_bins(A.bins, n);
     if (n >= kBigRefs && eligible(A, n)) continue;  // a CTA decides this node
     if (!eligible(A, n)) {
       if (lane == 0) {
@@ -165,7 +164,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock)
       }
       continue;
     }
-    for (int t = lane; t < 3 * 2 * (kKdMaxBins + 1); t += 32) h[t] = 0u;
+    // the six rows' first B + 1 entries (the rest is never read)
+    for (int t = lane; t < 6 * (B + 1); t += 32) h[(t / (B + 1)) * (kKdMaxBins + 1) + t % (B + 1)] = 0u;
     __syncwarp();
     int const rb = L.begin[j];
     for (int a = 0; a < 3; ++a) {
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock)
     for (int c = lane; c < 3 * (B - 1); c += 32) {
       float pl;
       int nl;
-      float const cost = candidate_cost(A, h, c, n, ext, lo4, hi4, sa, &pl, &nl);
+      float const cost = candidate_cost(A, B, h, c, n, ext, lo4, hi4, sa, &pl, &nl);
       if (better(cost, c, best, best_c)) {
         best = cost;
         best_c = c;
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock)
     float plane = 0.0f;
     if (best < A.ci * static_cast<float>(n)) {
       int nl_bin;
-      candidate_cost(A, h, best_c, n, ext, lo4, hi4, sa, &plane, &nl_bin);
+      candidate_cost(A, B, h, best_c, n, ext, lo4, hi4, sa, &plane, &nl_bin);
       axis = best_c / (B - 1);
     }
     int nl = 0, nr = 0;
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(kBigThreads) k_decide_big_hist(LevelArrays L, 
   int const ib = blockIdx.x / slices, g = blockIdx.x % slices;
   int const j = big_list[ib];
   int const n = L.count[j];
-  int const B = A.bins;
+  int const B = kd_node_bins(A.bins, n);
   int const tid = threadIdx.x;
   float4 const lo4 = L.blo[j], hi4 = L.bhi[j];
   float const ext[3] = {hi4.x - lo4.x, hi4.y - lo4.y, hi4.z - lo4.z};
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(kBigThreads)
   __shared__ int s_idx[kBigThreads / 32];
   int const j = big_list[blockIdx.x];
   int const n = L.count[j];
-  int const B = A.bins;
+  int const B = kd_node_bins(A.bins, n);
   int const tid = threadIdx.x;
   float4 const lo4 = L.blo[j], hi4 = L.bhi[j];
   float const ext[3] = {hi4.x - lo4.x, hi4.y - lo4.y, hi4.z - lo4.z};
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kBigThreads)
   for (int c = tid; c < 3 * (B - 1); c += kBigThreads) {
     float pl;
     int nl;
-    float const cost = candidate_cost(A, h, c, n, ext, lo4, hi4, sa, &pl, &nl);
+    float const cost = candidate_cost(A, B, h, c, n, ext, lo4, hi4, sa, &pl, &nl);
     if (better(cost, c, best, best_c)) {
       best = cost;
       best_c = c;
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(kBigThreads)
   float plane = 0.0f;
   if (best < A.ci * static_cast<float>(n)) {
     int nl_bin;
-    candidate_cost(A, h, best_c, n, ext, lo4, hi4, sa, &plane, &nl_bin);
+    candidate_cost(A, B, h, best_c, n, ext, lo4, hi4, sa, &plane, &nl_bin);
     axis = best_c / (B - 1);
   }
   // exact left / right counts: k_emit_big_count per slice, k_big_totals per node

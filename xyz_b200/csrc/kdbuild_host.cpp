@@ -80,7 +80,7 @@ SplitChoice choose_split(const LevelNode &nd, const Box *boxes, const BuildConfi
   for (int k = 0; k < 3; ++k) ext[k] = nd.bounds.hi[k] - nd.bounds.lo[k];
   float const sa = half_area(ext);
   if (!(sa > 0.0f)) return best;
-  int const B = cfg.bins;
+  int const B = kd_node_bins(cfg.bins, n);
   float best_cost = cfg.cost_intersect * static_cast<float>(n);
   uint32_t start[kKdMaxBins], end[kKdMaxBins];
   for (int a = 0; a < 3; ++a) {

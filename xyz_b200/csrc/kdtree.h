@@ -24,6 +24,21 @@ constexpr uint32_t kKdLeafTag = 3u;
 constexpr int kKdMaxDepthLimit = 60;  // traversal stack holds this many entries
 constexpr int kKdMaxBins = 64;
 
+#ifdef __CUDACC__
+#define XYZ_KD_HD __host__ __device__
+#else
+#define XYZ_KD_HD
+#endif
+
+// SAH bins per axis for a node of n references: the configured count, fewer
+// for small nodes (twice the references, at least 16), whose few references
+// leave most of 64 bins empty.  The host and the device builder use the same
+// rule, so their trees are identical.
+inline XYZ_KD_HD int kd_node_bins(int bins, int64_t n) {
+  int64_t const want = n * 2 < 16 ? 16 : n * 2;
+  return want < bins ? static_cast<int>(want) : bins;
+}
+
 struct BuildConfig {
   int leaf_max_tris = 4;
   int max_depth = 0;  // resolved before building
