@@ -139,10 +139,13 @@ __device__ __forceinline__ void store_row8(uint8_t *buf, int r, int c, int cols,
 // input s in [0, 1], 32 bins of exp(-(s - (j + 1/2) / 32)^2 / (2 sigma^2)),
 // sigma = 1/32.  Bins more than 4.5 sigma from s are exactly 0 (exp(-10) and
 // below; the oracle applies the same cut): the row is cleared, then the at
-// most 10 bins of the window are computed and stored one by one.  In bin
-// units (u = 32 s, t_j = u - j - 1/2) the bins are g_j = exp(-t_j^2 / 2), and
+// most 10 bins of the window are computed.  In bin units (u = 32 s,
+// t_j = u - j - 1/2) the bins are g_j = exp(-t_j^2 / 2), and
 // g_{j+1} = g_j exp(t_j - 1/2), exp(t_{j+1} - 1/2) = exp(t_j - 1/2) / e: two
-// exponentials per input and two products per bin.
+// exponentials per input and two products per bin.  The window is stored as
+// bf16 pairs at even columns (4-byte stores, the window's neighbours in a
+// pair being 0), which halves the shared-memory stores of one-by-one 2-byte
+// writes and their bank conflicts.
 __device__ void encode_row(uint8_t *x, int r, const GuideDev &G, const float f[6]) {
 #pragma unroll
   for (int q = 0; q < kIn; q += 8) *reinterpret_cast<uint4 *>(x + tc::blocked_offset(r, q, kIn)) = make_uint4(0, 0, 0, 0);
@@ -155,13 +158,28 @@ __device__ void encode_row(uint8_t *x, int r, const GuideDev &G, const float f[6
     float const t0 = u - (static_cast<float>(jlo) + 0.5f);
     float g = __expf(-0.5f * t0 * t0);
     float ratio = __expf(t0 - 0.5f);
+    float v[12];
+    v[0] = v[11] = 0.0f;
 #pragma unroll
     for (int t = 0; t < 10; ++t) {
       int const j = jlo + t;
-      if (j < kBins && fabsf(u - (static_cast<float>(j) + 0.5f)) <= 4.5f)
-        *reinterpret_cast<__nv_bfloat16 *>(x + tc::blocked_offset(r, dim * kBins + j, kIn)) = __float2bfloat16_rn(g);
+      v[t + 1] = (j < kBins && fabsf(u - (static_cast<float>(j) + 0.5f)) <= 4.5f) ? g : 0.0f;
       g *= ratio;
       ratio *= 0.36787944117144233f;  // 1 / e
+    }
+    // pairs from the even column at or below the window's first: bins
+    // (jlo + 2k, jlo + 2k + 1) when jlo is even, (jlo - 1 + 2k, jlo + 2k) when odd
+    int const odd = jlo & 1;
+    int const e0 = jlo - odd;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      int const c = e0 + 2 * k;
+      if (c < kBins) {
+        float const a = odd ? v[2 * k] : v[2 * k + 1];
+        float const b = odd ? v[2 * k + 1] : (k < 5 ? v[2 * k + 2] : 0.0f);
+        __nv_bfloat162 const pr = __floats2bfloat162_rn(a, b);
+        *reinterpret_cast<__nv_bfloat162 *>(x + tc::blocked_offset(r, dim * kBins + c, kIn)) = pr;
+      }
     }
   }
 }
