@@ -287,7 +287,8 @@ def adjoint_bench(steps: int, warmup: int):
 def batch_bench(steps: int, warmup: int):
     """Batched workload: 64 scenes (seeds 0-63, 1k-500k triangles, displaced
     icospheres and box stacks), resolutions in {128,256,512,1024}^2, 4-64 spp,
-    max depth 8, in one graph launch after autotuning; against the same 64
+    max depth 8, in one graph launch after autotuning (the wave and bounce
+    loops are conditional nodes the device runs); against the same 64
     renders issued one xyzgpu_render call after another.  Device time."""
     import torch
     from xyz_b200 import api, scenes
@@ -325,7 +326,9 @@ def batch_bench(steps: int, warmup: int):
         return {"msamples_per_s": round(paths / ms / 1e3, 1), "ms_per_launch": round(ms, 3),
                 "sequential_renders_msamples_per_s": round(paths / single_ms / 1e3, 1),
                 "paths": paths, "triangles": int(sum(e.scene.n_tris for e in work)),
-                "waves": st["waves"], "graph_nodes": st["graph_nodes"], "autotuned": chosen,
+                "waves": st["waves"], "graph_nodes": st["graph_nodes"],
+                "graph_top_nodes": st["graph_top_nodes"], "host_calls_per_launch": 1,
+                "device_kernel_launches_per_launch": st["kernel_launches_per_launch"], "autotuned": chosen,
                 "config": "64 scenes (seeds 0-63), 1k-500k triangles log-uniform, displaced icospheres "
                           "(odd) and box stacks (even), 128^2..1024^2, 4-64 spp, max depth 8"}
     finally:

@@ -318,8 +318,11 @@ int xyzgpu_adjoint(xyzgpu_scene scene, const xyzgpu_camera *camera,
  * carries its block, so traversal, shading and film kernels fetch the scene,
  * camera and estimator parameters per path.  A job renders the same film as
  * xyzgpu_render with its parameters (same paths, same per-pixel sample order).
- * The launch sequence of the whole batch (all waves) is captured once in a
- * CUDA graph and replayed by xyzgpu_batch_launch. */
+ * xyzgpu_batch_launch is one cudaGraphLaunch of a graph captured at creation
+ * whose loops over the waves and over each wave's bounces are conditional
+ * (WHILE) nodes run by the device: the kernels read the current wave and
+ * bounce from device memory, so the graph has the same few nodes however many
+ * waves the batch has, and a wave's bounce loop ends when its rays run out. */
 typedef struct {
   xyzgpu_scene scene;            /* must outlive the batch */
   xyzgpu_camera camera;
@@ -367,10 +370,14 @@ int xyzgpu_batch_autotune(xyzgpu_batch batch, int trials, int probe_spp, void *s
 typedef struct {
   uint64_t paths, waves, kernel_launches_per_launch, extension_rays, shadow_rays;
   int64_t device_bytes;     /* path buffers, tables and scratch of the batch */
-  int graph_nodes;          /* nodes of the captured graph (0 without a graph) */
+  int graph_nodes;          /* nodes of the captured graph, its loop bodies included
+                               (0 without a graph) */
+  int graph_top_nodes;      /* nodes at the graph's top level: the start kernel and
+                               the wave loop */
 } xyzgpu_batch_stats;
 
-/* Statistics of the batch; ray counts are those of the last launch (synchronises). */
+/* Statistics of the batch; ray and kernel counts are those of the last launch
+ * (synchronises). */
 int xyzgpu_batch_stats_get(xyzgpu_batch batch, xyzgpu_batch_stats *out);
 
 int xyzgpu_batch_config_get(xyzgpu_batch batch, xyzgpu_batch_config *out);

@@ -49,7 +49,10 @@ def test_batch_films_equal_single_renders(cfg):
             if cfg.get("wave_paths") == 20000:
                 assert st["waves"] > 3
             if cfg.get("use_graph", 1):
-                assert st["graph_nodes"] > 0
+                # one start kernel and the wave loop at the top; the loops'
+                # bodies hold the same dozen nodes however many waves there are
+                assert st["graph_top_nodes"] == 2
+                assert st["graph_nodes"] == 12
             for j, r in zip(jobs, ref):
                 assert torch.equal(j.film.view(torch.int32), r.view(torch.int32))
             # a second replay gives the same films
@@ -161,3 +164,48 @@ def test_batch_films_match_the_oracle_on_the_same_streams():
         close = (np.abs(film - ref) <= 1e-6 + 1e-4 * np.abs(ref)).all(axis=-1).mean()
         assert close >= 0.98, close
         assert abs(film.sum() - ref.sum()) / ref.sum() < 1e-2
+
+
+@pytest.mark.parametrize("use_graph", [1, 0])
+def test_batch_mixed_depths_and_early_ending_waves(use_graph):
+    """Jobs of different max_depth share waves (a wave runs the bounces of its
+    deepest job), and a job whose camera looks away from its scene ends after
+    its first bounce: the device's bounce loop stops there in a graph launch,
+    while the host-issued launch runs every bounce; films equal single renders."""
+    import dataclasses
+    import torch
+    from xyz_b200 import api
+    entries = _workload()
+    depths = [1, 3, 8, 2, 5, 8]
+    sd0, w0, h0, spp0 = entries[0]
+    cam = sd0.camera
+    # up and away from the floor (y = 0, |x|, |z| <= 10), the objects and the
+    # light near the origin: every camera ray escapes
+    away = dataclasses.replace(cam, at=(cam.eye[0], cam.eye[1] + 1.0, cam.eye[2] + 1.0))
+    scenes_ = [api.Scene(sd) for sd, *_ in entries]
+    try:
+        ref = []
+        for s, (sd, w, h, spp), d in zip(scenes_, entries, depths):
+            ref.append(s.render(sd.camera, w, h, spp, seed=9, max_depth=d).clone())
+        ref_away = scenes_[0].render(away, w0, h0, spp0, seed=9, max_depth=8).clone()
+        jobs = [api.BatchJob(s, sd.camera, w, h, spp, seed=9, max_depth=d)
+                for s, (sd, w, h, spp), d in zip(scenes_, entries, depths)]
+        with api.Batch(jobs, wave_paths=30000, use_graph=use_graph) as b:
+            b.launch()
+            torch.cuda.synchronize()
+            st = b.stats()
+            assert st["waves"] > 2
+            for j, r in zip(jobs, ref):
+                assert torch.equal(j.film.view(torch.int32), r.view(torch.int32))
+        lone = api.BatchJob(scenes_[0], away, w0, h0, spp0, seed=9, max_depth=8)
+        with api.Batch([lone], use_graph=use_graph) as b:
+            b.launch()
+            torch.cuda.synchronize()
+            st = b.stats()
+            assert torch.equal(lone.film.view(torch.int32), ref_away.view(torch.int32))
+            assert st["extension_rays"] == w0 * h0 * spp0
+            # start kernel + 5 per wave + 4 per bounce run
+            assert st["kernel_launches_per_launch"] == (1 + 5 + 4 if use_graph else 1 + 5 + 4 * 8)
+    finally:
+        for s in scenes_:
+            s.close()

@@ -138,7 +138,7 @@ class BatchConfig(C.Structure):
 class BatchStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("waves", C.c_uint64), ("kernel_launches_per_launch", C.c_uint64),
                 ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("device_bytes", C.c_int64),
-                ("graph_nodes", C.c_int)]
+                ("graph_nodes", C.c_int), ("graph_top_nodes", C.c_int)]
 
 
 class RenderProfile(C.Structure):

@@ -12,12 +12,20 @@
 // (grid = CTAs per SM x SMs, lanes refilled from a work counter); the others
 // stride over their queues.
 //
-// The whole launch sequence (film clears, per wave: counters, ray generation,
-// per bounce: closest hit, shading, shadow rays; film; tallies) is captured
-// into one CUDA graph at creation and replayed by xyzgpu_batch_launch.  The
-// graph's kernels read the job table from device memory, so sample offsets can
-// change between launches without re-capture.  The batch owns its path buffers
-// (the graph holds their addresses).
+// A launch is one CUDA graph whose control flow runs on the device: a start
+// kernel (film clears, tally, cursor), then a conditional WHILE node over the
+// waves whose body is: wave start (the cursor takes the wave's entry from the
+// device wave table, counters cleared), ray generation, a nested WHILE node over
+// the bounces (closest hit, shading, shadow rays, bounce end), film and tallies,
+// wave end.  The bounce loop ends when the wave's bounces are done or its
+// extension queue is empty, the wave loop after the last wave.  The batched
+// kernels read the wave and bounce from the device cursor, so the graph has the
+// same dozen nodes however many waves the batch has, and the host issues one
+// cudaGraphLaunch per batch.  The same kernels issued one by one from the host
+// (use_graph = 0, and the autotuner's probes) render the same films.  Sample
+// offsets live in the job table and can change between launches without
+// re-capture.  The batch owns its path buffers (the graph holds their
+// addresses).
 //
 // Autotuner: coordinate descent over the pixel tile of the slot order (tiles
 // make camera rays of neighbouring lanes coherent), the wave size (occupancy of
@@ -39,11 +47,11 @@ namespace {
 
 constexpr int64_t kDefaultBatchWave = int64_t{1} << 24;
 
-struct WavePlan {
-  int first_block = 0, n_blocks = 0;
-  int64_t npaths = 0, film_threads = 0;
-  int iters = 0;
-};
+using WavePlan = BatchWave;
+
+// Tally words the control kernels count in: waves and bounces run by the launch.
+constexpr int kTallyWaves = 3, kTallyBounces = 4;
+static_assert(kTallyBounces < kTallyIterBase, "batch tally words");
 
 struct Batch {
   int device = 0;
@@ -55,13 +63,16 @@ struct Batch {
   BatchJob *d_jobs = nullptr;
   WaveBlock *d_blocks = nullptr;
   size_t d_blocks_cap = 0;
+  BatchWave *d_waves = nullptr;
+  size_t d_waves_cap = 0;
+  BatchCursor *d_cursor = nullptr;
   RenderWorkspace ws;
   unsigned long long *d_tally = nullptr;
   cudaStream_t cap_stream = nullptr;
   cudaStream_t last_stream = nullptr;
   bool launched = false;
   cudaGraphExec_t exec = nullptr;
-  int graph_nodes = 0;
+  int graph_nodes = 0, graph_top_nodes = 0;
   uint64_t paths = 0, launches_per_launch = 0;
   int max_iters = 0;
   int grid_raygen = 0, grid_trace_e = 0, grid_trace_s = 0, grid_shade = 0, grid_film = 0;
@@ -80,7 +91,7 @@ int plan_waves(Batch &b, int64_t cap, int spp_cap) {
   b.blocks.clear();
   b.waves.clear();
   b.paths = 0;
-  WavePlan cur;
+  WavePlan cur{};
   int64_t used = 0;
   auto close = [&]() {
     if (cur.n_blocks > 0) b.waves.push_back(cur);
@@ -128,9 +139,21 @@ int upload_tables(Batch &b, const std::vector<float *> *films, cudaStream_t st) 
   std::vector<BatchJob> t = b.table;
   for (size_t j = 0; j < t.size(); ++j) {
     t[j].tile = job_tile(b, j);
+    t[j].clear = b.jobs[j].params.accumulate ? 0 : 1;
     if (films) t[j].film = (*films)[j];
   }
   XYZ_CUDA_TRY(cudaMemcpyAsync(b.d_jobs, t.data(), t.size() * sizeof(BatchJob), cudaMemcpyHostToDevice, st));
+  if (b.waves.size() > b.d_waves_cap) {
+    XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFree(b.d_waves);
+    b.d_waves = nullptr;
+    b.d_waves_cap = 0;
+    XYZ_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&b.d_waves), b.waves.size() * sizeof(BatchWave)));
+    b.d_waves_cap = b.waves.size();
+  }
+  if (!b.waves.empty())
+    XYZ_CUDA_TRY(cudaMemcpyAsync(b.d_waves, b.waves.data(), b.waves.size() * sizeof(BatchWave),
+                                 cudaMemcpyHostToDevice, st));
   if (b.blocks.size() > b.d_blocks_cap) {
     XYZ_CUDA_TRY(cudaStreamSynchronize(st));
     cudaFree(b.d_blocks);
@@ -158,15 +181,69 @@ void set_grids(Batch &b) {
   b.grid_trace_s = (want > 0 ? std::min(want, occ_s) : occ_s) * sms;
 }
 
-// Issues the whole launch sequence on `st`: film clears, then every wave.
-int issue(Batch &b, cudaStream_t st, const std::vector<float *> &films, bool clear_films) {
-  uint64_t launches = 0;
-  XYZ_CUDA_TRY(cudaMemsetAsync(b.d_tally, 0, kTallyWords * sizeof(unsigned long long), st));
-  for (size_t j = 0; j < b.jobs.size(); ++j) {
-    xyzgpu_render_params const &p = b.jobs[j].params;
-    if (clear_films && !p.accumulate)
-      XYZ_CUDA_TRY(cudaMemsetAsync(films[j], 0, 3 * static_cast<size_t>(p.width) * p.height * sizeof(float), st));
+// ------------------------------------------------------- control kernels
+// Launch start: the tally is cleared, the films of jobs that do not accumulate
+// are zeroed (grid y strides over the jobs) and the cursor goes to wave 0.
+__global__ void __launch_bounds__(kThreads) k_batch_begin(const BatchJob *jobs, int n_jobs,
+                                                          unsigned long long *tally, BatchCursor *cur) {
+  if (blockIdx.x == 0 && blockIdx.y == 0) {
+    for (int i = threadIdx.x; i < kTallyWords; i += blockDim.x) tally[i] = 0;
+    if (threadIdx.x == 0) {
+      cur->wave = 0;
+      cur->bounce = 0;
+    }
   }
+  int64_t const stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int j = blockIdx.y; j < n_jobs; j += gridDim.y) {
+    BatchJob const &J = jobs[j];
+    if (!J.clear) continue;
+    int64_t const n = 3 * static_cast<int64_t>(J.W) * J.H;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+      J.film[i] = 0.0f;
+  }
+}
+
+// Wave start: the cursor takes the entry of its wave and bounce 0; the wave's
+// queue counters are cleared.  In a graph it also opens the bounce loop.
+template <bool kGraph>
+__global__ void k_batch_wave_begin(const BatchWave *waves, BatchCursor *cur, int32_t *counts,
+                                   cudaGraphConditionalHandle bounce_loop) {
+  BatchWave const w = waves[cur->wave];
+  int const nc = (w.iters + 2) * kCountStride;
+  for (int i = threadIdx.x; i < nc; i += blockDim.x) counts[i] = 0;
+  if (threadIdx.x == 0) {
+    cur->w = w;
+    cur->bounce = 0;
+    if constexpr (kGraph) cudaGraphSetConditional(bounce_loop, w.iters > 0 ? 1u : 0u);
+  }
+}
+
+// Bounce end: the cursor moves to the next bounce, which runs (in a graph)
+// while the wave has bounces left and rays in its extension queue.
+template <bool kGraph>
+__global__ void k_batch_bounce_end(BatchCursor *cur, const int32_t *counts, unsigned long long *tally,
+                                   cudaGraphConditionalHandle bounce_loop) {
+  int const b = cur->bounce + 1;
+  cur->bounce = b;
+  tally[kTallyBounces] += 1;
+  if constexpr (kGraph) {
+    bool const more = b < cur->w.iters && counts[b * kCountStride + kCExt] > 0;
+    cudaGraphSetConditional(bounce_loop, more ? 1u : 0u);
+  }
+}
+
+// Wave end: the cursor moves to the next wave; the wave loop (in a graph)
+// ends after the last one.
+template <bool kGraph>
+__global__ void k_batch_wave_end(BatchCursor *cur, int n_waves, unsigned long long *tally,
+                                 cudaGraphConditionalHandle wave_loop) {
+  int const w = cur->wave + 1;
+  cur->wave = w;
+  tally[kTallyWaves] += 1;
+  if constexpr (kGraph) cudaGraphSetConditional(wave_loop, w < n_waves ? 1u : 0u);
+}
+
+WaveArgs wave_args(const Batch &b) {
   WaveArgs A;
   std::memset(&A, 0, sizeof(A));
   RenderWorkspace const &wv = b.ws;
@@ -189,57 +266,148 @@ int issue(Batch &b, cudaStream_t st, const std::vector<float *> &films, bool cle
   A.s_slot = wv.s_slot;
   A.hero = 1;
   A.jobs = b.d_jobs;
+  A.blocks = b.d_blocks;
+  A.cursor = b.d_cursor;
+  return A;
+}
+
+dim3 begin_grid(const Batch &b) {
+  return dim3(static_cast<unsigned>(std::max(1, sm_count(b.device))),
+              static_cast<unsigned>(std::min<size_t>(b.jobs.size(), 65535)));
+}
+
+// Issues the launch from the host, kernel by kernel, on `st`: the start
+// kernel, then every wave of the plan with all of its bounces.  The films are
+// the job table's (the autotuner points them at scratch films).
+int issue(Batch &b, cudaStream_t st) {
+  WaveArgs const A = wave_args(b);
+  int const n_waves = static_cast<int>(b.waves.size());
+  k_batch_begin<<<begin_grid(b), kThreads, 0, st>>>(b.d_jobs, static_cast<int>(b.jobs.size()), b.d_tally,
+                                                     b.d_cursor);
+  uint64_t launches = 1;
   for (WavePlan const &w : b.waves) {
-    A.blocks = b.d_blocks + w.first_block;
-    A.n_blocks = w.n_blocks;
-    A.npaths = w.npaths;
-    A.film_threads = w.film_threads;
-    int const iters = w.iters;
-    XYZ_CUDA_TRY(cudaMemsetAsync(wv.counts, 0, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t), st));
-    int const gr = static_cast<int>(std::min<int64_t>(b.grid_raygen, (w.npaths + kThreads - 1) / kThreads));
-    k_raygen<true><<<gr, kThreads, 0, st>>>(A);
-    for (int it = 0; it < iters; ++it) {
+    k_batch_wave_begin<false><<<1, kThreads, 0, st>>>(b.d_waves, b.d_cursor, b.ws.counts, 0);
+    k_raygen<true><<<b.grid_raygen, kThreads, 0, st>>>(A);
+    for (int it = 0; it < w.iters; ++it) {
       k_trace_queue<false, false, kModeBatch><<<b.grid_trace_e, kThreads, 0, st>>>(A, it, nullptr);
       k_shade<kModeBatch><<<b.grid_shade, kThreads, 0, st>>>(A, it);
       k_trace_queue<true, false, kModeBatch><<<b.grid_trace_s, kThreads, 0, st>>>(A, it, nullptr);
+      k_batch_bounce_end<false><<<1, 1, 0, st>>>(b.d_cursor, b.ws.counts, b.d_tally, 0);
     }
-    int const gf = static_cast<int>(std::min<int64_t>(b.grid_film, (w.film_threads + kThreads - 1) / kThreads));
-    k_film_batch<<<gf, kThreads, 0, st>>>(A);
-    k_tally<<<1, 32, 0, st>>>(A, iters, b.d_tally);
-    launches += 3 + 3 * static_cast<uint64_t>(iters);
+    k_film_batch<<<b.grid_film, kThreads, 0, st>>>(A);
+    k_tally<<<1, 32, 0, st>>>(A, 0, b.d_tally);
+    k_batch_wave_end<false><<<1, 1, 0, st>>>(b.d_cursor, n_waves, b.d_tally, 0);
+    launches += 5 + 4 * static_cast<uint64_t>(w.iters);
     XYZ_CUDA_TRY(cudaGetLastError());
   }
   b.launches_per_launch = launches;
   return XYZGPU_OK;
 }
 
-std::vector<float *> job_films(const Batch &b) {
-  std::vector<float *> f(b.jobs.size());
-  for (size_t j = 0; j < b.jobs.size(); ++j) f[j] = b.jobs[j].film;
-  return f;
-}
-
 void drop_graph(Batch &b) {
   if (b.exec) cudaGraphExecDestroy(b.exec);
   b.exec = nullptr;
-  b.graph_nodes = 0;
+  b.graph_nodes = b.graph_top_nodes = 0;
 }
 
+size_t node_count(cudaGraph_t g) {
+  size_t n = 0;
+  cudaGraphGetNodes(g, nullptr, &n);
+  return n;
+}
+
+// Captures `emit`'s launches on the capture stream into `g` after `deps`
+// (ndeps of them) and returns the last node captured in *last.
+template <class F>
+cudaError_t capture_into(cudaStream_t cs, cudaGraph_t g, const cudaGraphNode_t *deps, size_t ndeps, F &&emit,
+                         cudaGraphNode_t *last) {
+  cudaError_t e = cudaStreamBeginCaptureToGraph(cs, g, deps, nullptr, ndeps, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  emit();
+  cudaError_t const le = cudaGetLastError();
+  cudaStreamCaptureStatus status;
+  const cudaGraphNode_t *tail = nullptr;
+  size_t ntail = 0;
+  e = cudaStreamGetCaptureInfo(cs, &status, nullptr, nullptr, &tail, &ntail);
+  cudaGraphNode_t const t = (e == cudaSuccess && ntail == 1) ? tail[0] : nullptr;
+  cudaGraph_t out = nullptr;
+  cudaError_t const ee = cudaStreamEndCapture(cs, &out);
+  if (le != cudaSuccess) return le;
+  if (e != cudaSuccess) return e;
+  if (ee != cudaSuccess) return ee;
+  if (!t) return cudaErrorStreamCaptureUnjoined;
+  *last = t;
+  return cudaSuccess;
+}
+
+// Adds a WHILE node after `dep` to `g` and returns its body graph.
+cudaError_t add_while(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h, cudaGraphNode_t *node,
+                      cudaGraph_t *body) {
+  cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaError_t const e = cudaGraphAddNode(node, g, &dep, 1, &p);
+  if (e != cudaSuccess) return e;
+  *body = p.conditional.phGraph_out[0];
+  return cudaSuccess;
+}
+
+// Builds the launch graph: start kernel -> WHILE(waves) { wave start, ray
+// generation -> WHILE(bounces) { closest hit, shading, shadow rays, bounce
+// end } -> film, tally, wave end }.
 int capture(Batch &b) {
   drop_graph(b);
   if (!b.cfg.use_graph) return XYZGPU_OK;
   if (!b.cap_stream) XYZ_CUDA_TRY(cudaStreamCreateWithFlags(&b.cap_stream, cudaStreamNonBlocking));
-  XYZ_CUDA_TRY(cudaStreamBeginCapture(b.cap_stream, cudaStreamCaptureModeThreadLocal));
-  int const rc = issue(b, b.cap_stream, job_films(b), true);
+  cudaStream_t const cs = b.cap_stream;
+  WaveArgs const A = wave_args(b);
+  int const n_waves = static_cast<int>(b.waves.size());
+  int const n_jobs = static_cast<int>(b.jobs.size());
   cudaGraph_t g = nullptr;
-  cudaError_t const e = cudaStreamEndCapture(b.cap_stream, &g);
-  if (rc) {
-    if (g) cudaGraphDestroy(g);
-    return rc;
+  XYZ_CUDA_TRY(cudaGraphCreate(&g, 0));
+  cudaError_t e = cudaSuccess;
+  cudaGraphConditionalHandle wave_loop = 0, bounce_loop = 0;
+  cudaGraphNode_t n_begin = nullptr, n_waves_node = nullptr, n_raygen = nullptr, n_bounces = nullptr,
+                  n_tail = nullptr;
+  cudaGraph_t wave_body = nullptr, bounce_body = nullptr;
+  do {
+    e = cudaGraphConditionalHandleCreate(&wave_loop, g, n_waves > 0 ? 1u : 0u, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) break;
+    e = capture_into(cs, g, nullptr, 0, [&] {
+      k_batch_begin<<<begin_grid(b), kThreads, 0, cs>>>(b.d_jobs, n_jobs, b.d_tally, b.d_cursor);
+    }, &n_begin);
+    if (e != cudaSuccess) break;
+    e = add_while(g, n_begin, wave_loop, &n_waves_node, &wave_body);
+    if (e != cudaSuccess) break;
+    e = cudaGraphConditionalHandleCreate(&bounce_loop, wave_body, 0u, 0u);
+    if (e != cudaSuccess) break;
+    e = capture_into(cs, wave_body, nullptr, 0, [&] {
+      k_batch_wave_begin<true><<<1, kThreads, 0, cs>>>(b.d_waves, b.d_cursor, b.ws.counts, bounce_loop);
+      k_raygen<true><<<b.grid_raygen, kThreads, 0, cs>>>(A);
+    }, &n_raygen);
+    if (e != cudaSuccess) break;
+    e = add_while(wave_body, n_raygen, bounce_loop, &n_bounces, &bounce_body);
+    if (e != cudaSuccess) break;
+    e = capture_into(cs, bounce_body, nullptr, 0, [&] {
+      k_trace_queue<false, false, kModeBatch><<<b.grid_trace_e, kThreads, 0, cs>>>(A, 0, nullptr);
+      k_shade<kModeBatch><<<b.grid_shade, kThreads, 0, cs>>>(A, 0);
+      k_trace_queue<true, false, kModeBatch><<<b.grid_trace_s, kThreads, 0, cs>>>(A, 0, nullptr);
+      k_batch_bounce_end<true><<<1, 1, 0, cs>>>(b.d_cursor, b.ws.counts, b.d_tally, bounce_loop);
+    }, &n_tail);
+    if (e != cudaSuccess) break;
+    e = capture_into(cs, wave_body, &n_bounces, 1, [&] {
+      k_film_batch<<<b.grid_film, kThreads, 0, cs>>>(A);
+      k_tally<<<1, 32, 0, cs>>>(A, 0, b.d_tally);
+      k_batch_wave_end<true><<<1, 1, 0, cs>>>(b.d_cursor, n_waves, b.d_tally, wave_loop);
+    }, &n_tail);
+  } while (false);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return set_error(XYZGPU_E_CUDA, "batch: building the launch graph failed: %s", cudaGetErrorString(e));
   }
-  if (e != cudaSuccess) return set_error(XYZGPU_E_CUDA, "batch: graph capture failed: %s", cudaGetErrorString(e));
-  size_t nodes = 0;
-  cudaGraphGetNodes(g, nullptr, &nodes);
+  size_t const top = node_count(g);
+  size_t const nodes = top + node_count(wave_body) + node_count(bounce_body);
   cudaError_t const e2 = cudaGraphInstantiate(&b.exec, g, 0);
   cudaGraphDestroy(g);
   if (e2 != cudaSuccess) {
@@ -247,6 +415,7 @@ int capture(Batch &b) {
     return set_error(XYZGPU_E_CUDA, "batch: graph instantiation failed: %s", cudaGetErrorString(e2));
   }
   b.graph_nodes = static_cast<int>(nodes);
+  b.graph_top_nodes = static_cast<int>(top);
   return XYZGPU_OK;
 }
 
@@ -303,6 +472,8 @@ void xyzgpu_batch_destroy(xyzgpu_batch h) {
   if (b.cap_stream) cudaStreamDestroy(b.cap_stream);
   cudaFree(b.d_jobs);
   cudaFree(b.d_blocks);
+  cudaFree(b.d_waves);
+  cudaFree(b.d_cursor);
   cudaFree(b.d_tally);
   free_wave_buffers(b.ws);
   cudaSetDevice(prev);
@@ -377,7 +548,8 @@ int xyzgpu_batch_create(const xyzgpu_batch_job *jobs, int n_jobs, const xyzgpu_b
   };
   if (cudaSetDevice(b.device) != cudaSuccess) return fail(set_error(XYZGPU_E_CUDA, "batch_create: cudaSetDevice failed"));
   if (cudaMalloc(reinterpret_cast<void **>(&b.d_jobs), n_jobs * sizeof(BatchJob)) != cudaSuccess ||
-      cudaMalloc(reinterpret_cast<void **>(&b.d_tally), kTallyWords * sizeof(unsigned long long)) != cudaSuccess)
+      cudaMalloc(reinterpret_cast<void **>(&b.d_tally), kTallyWords * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(reinterpret_cast<void **>(&b.d_cursor), sizeof(BatchCursor)) != cudaSuccess)
     return fail(set_error(XYZGPU_E_NOMEM, "batch_create: allocating the job table failed"));
   int rc = prepare(b, 0, nullptr, nullptr);
   if (rc) return fail(rc);
@@ -397,7 +569,7 @@ int xyzgpu_batch_launch(xyzgpu_batch h, void *stream) {
   if (b.exec) {
     XYZ_CUDA_TRY(cudaGraphLaunch(b.exec, st));
   } else {
-    int const rc = issue(b, st, job_films(b), true);
+    int const rc = issue(b, st);
     if (rc) return rc;
   }
   b.last_stream = st;
@@ -456,7 +628,7 @@ int xyzgpu_batch_autotune(xyzgpu_batch h, int trials, int probe_spp, void *strea
     float best = INFINITY;
     for (int t = 0; t < trials + 1; ++t) {  // the first run warms up
       XYZ_CUDA_TRY(cudaEventRecord(e0, st));
-      r = issue(b, st, films, true);
+      r = issue(b, st);
       if (r) return r;
       XYZ_CUDA_TRY(cudaEventRecord(e1, st));
       XYZ_CUDA_TRY(cudaEventSynchronize(e1));
@@ -544,12 +716,16 @@ int xyzgpu_batch_stats_get(xyzgpu_batch h, xyzgpu_batch_stats *out) {
   XYZ_CUDA_TRY(cudaMemcpy(t, b.d_tally, sizeof(t), cudaMemcpyDeviceToHost));
   out->paths = b.paths;
   out->waves = b.waves.size();
-  out->kernel_launches_per_launch = b.launches_per_launch;
+  // kernels of the last launch: the start kernel, 5 per wave and 4 per bounce
+  // (the bounce loop of a graph launch ends early when a wave runs out of rays)
+  out->kernel_launches_per_launch =
+      b.launched ? 1 + 5 * t[kTallyWaves] + 4 * t[kTallyBounces] : b.launches_per_launch;
   out->extension_rays = b.launched ? t[0] : 0;
   out->shadow_rays = b.launched ? t[1] : 0;
   out->device_bytes = b.ws.capacity * kBytesPerPath +
                       static_cast<int64_t>(b.jobs.size() * sizeof(BatchJob) + b.d_blocks_cap * sizeof(WaveBlock));
   out->graph_nodes = b.graph_nodes;
+  out->graph_top_nodes = b.graph_top_nodes;
   return XYZGPU_OK;
 }
 

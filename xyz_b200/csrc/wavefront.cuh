@@ -73,6 +73,7 @@ struct BatchJob {
   uint64_t seed;
   uint32_t spp_offset;  // first sample index of the job's render
   float *film;          // W * H * 3 sums, device
+  int clear;            // the launch zeroes the film first (the job does not accumulate)
 };
 
 struct WaveBlock {
@@ -82,6 +83,21 @@ struct WaveBlock {
   int64_t npix;      // the job's pixels
   int64_t slot_off;  // first path slot of the block: slot = slot_off + s * npix + p
   int64_t pix_off;   // first film thread of the block (film kernel)
+};
+
+// A wave of a batch: its blocks are blocks[first_block .. first_block + n_blocks).
+struct BatchWave {
+  int first_block, n_blocks;
+  int64_t npaths, film_threads;  // path slots; pixels of all its blocks (film threads)
+  int iters;                     // bounces: the largest max_depth of its jobs
+};
+
+// Where a batch launch is, in device memory: the wave and bounce the batched
+// kernels work on and a copy of that wave's entry.  The batch's control
+// kernels advance it, so the same kernels serve every wave and bounce.
+struct BatchCursor {
+  int wave, bounce;
+  BatchWave w;
 };
 
 // Variants of the shading and shadow kernels: the plain render, the replay
@@ -130,9 +146,8 @@ struct WaveArgs {
   float *g_em;
   // batched renders
   const BatchJob *jobs;
-  const WaveBlock *blocks;
-  int n_blocks;
-  int64_t film_threads;  // pixels of all blocks of the wave
+  const WaveBlock *blocks;    // all blocks of the batch; a record's block indexes it
+  const BatchCursor *cursor;  // the current wave and bounce
   // guided renders: the guide's mixture per extension-queue entry (40 fp16:
   // per lobe weight, concentration, mean xyz), the one-sample MIS probability
   // of the guide, and training records (16 floats x train_bounces per path:
@@ -272,9 +287,9 @@ XYZ_DEV void slot_to_pixel_sample(const WaveArgs &A, int64_t slot, uint32_t *pix
   *sample = A.s0 + static_cast<uint32_t>(sl);
 }
 
-// Block of a path slot in a batched wave (blocks are in slot order).
-XYZ_DEV int block_of_slot(const WaveArgs &A, int64_t slot) {
-  int lo = 0, hi = A.n_blocks - 1;
+// Block of a path slot in a batched wave (the wave's blocks are in slot order).
+XYZ_DEV int block_of_slot(const WaveArgs &A, const BatchWave &w, int64_t slot) {
+  int lo = w.first_block, hi = w.first_block + w.n_blocks - 1;
   while (lo < hi) {
     int const mid = (lo + hi + 1) >> 1;
     if (A.blocks[mid].slot_off <= slot)
@@ -361,9 +376,12 @@ XYZ_DEV int32_t warp_append(int32_t *counter, bool want) {
 template <bool kBatch>
 __global__ void __launch_bounds__(kThreads) k_raygen(WaveArgs A) {
   int64_t const stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t slot = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; slot < A.npaths;
+  BatchWave wv{};
+  if constexpr (kBatch) wv = A.cursor->w;
+  int64_t const npaths = kBatch ? wv.npaths : A.npaths;
+  for (int64_t slot = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; slot < npaths;
        slot += stride) {
-    int const block = kBatch ? block_of_slot(A, slot) : 0;
+    int const block = kBatch ? block_of_slot(A, wv, slot) : 0;
     uint32_t pixel, sample;
     path_pixel_sample<kBatch>(A, block, slot, &pixel, &sample);
     uint64_t const seed = params_of<kBatch>(A, block).seed;
@@ -423,7 +441,7 @@ __global__ void __launch_bounds__(kThreads) k_raygen(WaveArgs A) {
     A.misc[slot] = pack_misc(dim, 1u, 1u);
     A.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) A.counts[kCExt] = static_cast<int32_t>(A.npaths);
+  if (blockIdx.x == 0 && threadIdx.x == 0) A.counts[kCExt] = static_cast<int32_t>(npaths);
 }
 
 // ------------------------------------------------------------------ trace
@@ -540,6 +558,7 @@ template <bool kShadow, bool kCount, int kMode = kModePlain>
 __global__ void __launch_bounds__(kThreads, kShadow ? 10 : 9) k_trace_queue(WaveArgs A, int b,
                                                           unsigned long long *prof) {
   constexpr bool kBatch = kMode == kModeBatch;
+  if constexpr (kBatch) b = A.cursor->bounce;
   int32_t *const cnt = A.counts + b * kCountStride;
   int const n = kShadow ? cnt[kCShadow] : cnt[kCExt];
   int const lane = threadIdx.x & 31;
@@ -586,8 +605,10 @@ __global__ void __launch_bounds__(kThreads, kShadow ? 10 : 9) k_trace_queue(Wave
 constexpr int kTallyIterBase = 16;
 constexpr int kTallyWords = kTallyIterBase + 2 * XYZGPU_PROFILE_MAX_ITERS;
 
+// Batched waves (A.cursor set) take their bounce count from the cursor.
 __global__ void k_tally(WaveArgs A, int iters, unsigned long long *tally) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (A.cursor) iters = A.cursor->w.iters;
   unsigned long long e = 0, sh = 0, vis = 0;
   for (int b = 0; b < iters; ++b) {
     unsigned long long const eb = A.counts[b * kCountStride + kCExt];
@@ -735,6 +756,7 @@ __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shad
   // mirror and metal materials exist in plain and batched renders only (the
   // other modes refuse such scenes), so the other variants carry no code for them
   constexpr bool kSpecMat = kMode == kModePlain || kMode == kModeBatch;
+  if constexpr (kBatch) b = A.cursor->bounce;
   int32_t *const cnt = A.counts + b * kCountStride;
   int32_t *const cnt_next = A.counts + (b + 1) * kCountStride;
   int const n = cnt[kCExt];
@@ -1369,8 +1391,9 @@ __global__ void __launch_bounds__(kThreads) k_film(WaveArgs A, float *__restrict
 // samples are added in sample order into the job's film.
 __global__ void __launch_bounds__(kThreads) k_film_batch(WaveArgs A) {
   int64_t const stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < A.film_threads; q += stride) {
-    int lo = 0, hi = A.n_blocks - 1;
+  BatchWave const wv = A.cursor->w;
+  for (int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < wv.film_threads; q += stride) {
+    int lo = wv.first_block, hi = wv.first_block + wv.n_blocks - 1;
     while (lo < hi) {
       int const mid = (lo + hi + 1) >> 1;
       if (A.blocks[mid].pix_off <= q)
