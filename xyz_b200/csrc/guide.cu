@@ -138,50 +138,61 @@ __device__ __forceinline__ void store_row8(uint8_t *buf, int r, int c, int cols,
 // Row r of the input encoding from a raw point (position, normal): per
 // input s in [0, 1], 32 bins of exp(-(s - (j + 1/2) / 32)^2 / (2 sigma^2)),
 // sigma = 1/32.  Bins more than 4.5 sigma from s are exactly 0 (exp(-10) and
-// below; the oracle applies the same cut): the row is cleared, then the at
-// most 10 bins of the window are computed.  In bin units (u = 32 s,
+// below; the oracle applies the same cut): an input's 32 columns are cleared,
+// then the at most 10 bins of its window are computed.  In bin units (u = 32 s,
 // t_j = u - j - 1/2) the bins are g_j = exp(-t_j^2 / 2), and
 // g_{j+1} = g_j exp(t_j - 1/2), exp(t_{j+1} - 1/2) = exp(t_j - 1/2) / e: two
 // exponentials per input and two products per bin.  The window is stored as
 // bf16 pairs at even columns (4-byte stores, the window's neighbours in a
 // pair being 0), which halves the shared-memory stores of one-by-one 2-byte
 // writes and their bank conflicts.
-__device__ void encode_row(uint8_t *x, int r, const GuideDev &G, const float f[6]) {
+//
+// Input coordinate of feature `dim` in [0, 1]: the position in the scene's
+// bounds, a normal component mapped from [-1, 1].
+__device__ __forceinline__ float encode_coord(const GuideDev &G, int dim, float f) {
+  float const s = dim < 3 ? (f - G.lo[dim]) * G.inv_ext[dim] : (f + 1.0f) * 0.5f;
+  return fminf(fmaxf(s, 0.0f), 1.0f);
+}
+
+// The kBins columns c0 .. c0 + kBins - 1 of row r of a blocked buffer of C
+// columns: one input coordinate s.
+__device__ __forceinline__ void encode_dim(uint8_t *x, int r, int C, int c0, float s) {
 #pragma unroll
-  for (int q = 0; q < kIn; q += 8) *reinterpret_cast<uint4 *>(x + tc::blocked_offset(r, q, kIn)) = make_uint4(0, 0, 0, 0);
+  for (int q = 0; q < kBins; q += 8)
+    *reinterpret_cast<uint4 *>(x + tc::blocked_offset(r, c0 + q, C)) = make_uint4(0, 0, 0, 0);
+  float const u = s * static_cast<float>(kBins);
+  int const jlo = max(0, static_cast<int>(ceilf(u - 5.0f)));
+  float const t0 = u - (static_cast<float>(jlo) + 0.5f);
+  float g = __expf(-0.5f * t0 * t0);
+  float ratio = __expf(t0 - 0.5f);
+  float v[12];
+  v[0] = v[11] = 0.0f;
 #pragma unroll
-  for (int dim = 0; dim < 6; ++dim) {
-    float s = dim < 3 ? (f[dim] - G.lo[dim]) * G.inv_ext[dim] : (f[dim] + 1.0f) * 0.5f;
-    s = fminf(fmaxf(s, 0.0f), 1.0f);
-    float const u = s * static_cast<float>(kBins);
-    int const jlo = max(0, static_cast<int>(ceilf(u - 5.0f)));
-    float const t0 = u - (static_cast<float>(jlo) + 0.5f);
-    float g = __expf(-0.5f * t0 * t0);
-    float ratio = __expf(t0 - 0.5f);
-    float v[12];
-    v[0] = v[11] = 0.0f;
+  for (int t = 0; t < 10; ++t) {
+    int const j = jlo + t;
+    v[t + 1] = (j < kBins && fabsf(u - (static_cast<float>(j) + 0.5f)) <= 4.5f) ? g : 0.0f;
+    g *= ratio;
+    ratio *= 0.36787944117144233f;  // 1 / e
+  }
+  // pairs from the even column at or below the window's first: bins
+  // (jlo + 2k, jlo + 2k + 1) when jlo is even, (jlo - 1 + 2k, jlo + 2k) when odd
+  int const odd = jlo & 1;
+  int const e0 = jlo - odd;
 #pragma unroll
-    for (int t = 0; t < 10; ++t) {
-      int const j = jlo + t;
-      v[t + 1] = (j < kBins && fabsf(u - (static_cast<float>(j) + 0.5f)) <= 4.5f) ? g : 0.0f;
-      g *= ratio;
-      ratio *= 0.36787944117144233f;  // 1 / e
-    }
-    // pairs from the even column at or below the window's first: bins
-    // (jlo + 2k, jlo + 2k + 1) when jlo is even, (jlo - 1 + 2k, jlo + 2k) when odd
-    int const odd = jlo & 1;
-    int const e0 = jlo - odd;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      int const c = e0 + 2 * k;
-      if (c < kBins) {
-        float const a = odd ? v[2 * k] : v[2 * k + 1];
-        float const b = odd ? v[2 * k + 1] : (k < 5 ? v[2 * k + 2] : 0.0f);
-        __nv_bfloat162 const pr = __floats2bfloat162_rn(a, b);
-        *reinterpret_cast<__nv_bfloat162 *>(x + tc::blocked_offset(r, dim * kBins + c, kIn)) = pr;
-      }
+  for (int k = 0; k < 6; ++k) {
+    int const c = e0 + 2 * k;
+    if (c < kBins) {
+      float const a = odd ? v[2 * k] : v[2 * k + 1];
+      float const b = odd ? v[2 * k + 1] : (k < 5 ? v[2 * k + 2] : 0.0f);
+      __nv_bfloat162 const pr = __floats2bfloat162_rn(a, b);
+      *reinterpret_cast<__nv_bfloat162 *>(x + tc::blocked_offset(r, c0 + c, C)) = pr;
     }
   }
+}
+
+__device__ void encode_row(uint8_t *x, int r, const GuideDev &G, const float f[6]) {
+#pragma unroll
+  for (int dim = 0; dim < 6; ++dim) encode_dim(x, r, kIn, dim * kBins, encode_coord(G, dim, f[dim]));
 }
 
 // ---------------------------------------------------------------- tiles
@@ -417,17 +428,18 @@ __device__ void teardown(uint32_t tmem, uint32_t ncols, bool aborted, uint32_t m
   if (threadIdx.x < 32) tc::tmem_free(tmem, ncols);
 }
 
-// Inference CTAs: three groups of four warps, each with its own 128-row tile,
-// buffer and accumulator, sharing the weights; while one group waits for its
-// MMAs the others run their epilogues or gather their next rows.  A group's
-// hidden activations reuse its encoding buffer (the first layer's MMA has
-// finished reading it before the first epilogue writes).
-constexpr int kGroups = 3;
+// Inference CTAs: four groups of four warps, each with its own 128-row tile,
+// two 16 KB buffers and accumulator, sharing the weights; while one group waits
+// for its MMAs the others run their encodings, epilogues or gathers.  The first
+// layer runs in three K-chunks of two inputs (64 columns) through the two
+// buffers, the hidden activations then alternate between them
+// (forward_infer).
+constexpr int kGroups = 4;
 constexpr int kInferThreads = kGroups * kRows;
 
 struct __align__(128) InferSmem {
   WeightsSmem wt;
-  uint8_t x[kGroups][kRows * kIn * 2];
+  uint8_t x[kGroups][2 * kHBytes];
   uint64_t mbar[kGroups];
   uint32_t tmem;
 };
@@ -444,6 +456,60 @@ __device__ Tile infer_tile(InferSmem &S, int gi) {
   c.bar = 1 + gi;
   c.t = threadIdx.x & (kRows - 1);
   return c;
+}
+
+// Forward pass of this thread's row from its features (inference CTAs),
+// leaving the raw outputs (with bias) in out[64].  The first layer's K-chunks
+// go through the group's buffers A and B: chunk 0 (inputs 0, 1) -> A, chunk 1
+// -> B, and chunk 2 -> A once chunk 0's MMAs (committed on their own) have
+// read it, so a chunk's MMAs overlap the next chunk's encoding.  Hidden layer
+// l - 1's activations go to A for even l - 1, B for odd: the MMA that read that
+// buffer last has completed by then.
+__device__ bool forward_infer(const WeightsSmem &wt, const GuideDev &G, Tile &c, uint32_t &phase,
+                              const float f[6], float *out) {
+  uint8_t *const buf[2] = {c.x, c.x + kHBytes};
+  constexpr int kChunk = 2 * kBins;  // columns of a K-chunk
+  uint32_t const id = tc::idesc_bf16(kRows, kW, false, false);
+  uint32_t const b0 = tc::smem_addr(wt.w) + wblk_off(0);
+#pragma unroll
+  for (int k = 0; k < kIn / kChunk; ++k) {
+    uint8_t *const dst = buf[k & 1];
+    if (k == 2 && !await_mma(c, phase)) return false;
+    encode_dim(dst, c.t, kChunk, 0, encode_coord(G, 2 * k, f[2 * k]));
+    encode_dim(dst, c.t, kChunk, kBins, encode_coord(G, 2 * k + 1, f[2 * k + 1]));
+    publish(c.bar);
+    if (c.t == 0) {
+      tc::fence_after_sync();
+      if (k == 0)
+        tc::mma_bf16(c.tmem, tc::desc_kmajor(tc::smem_addr(wt.ones), kBiasK),
+                     tc::desc_kmajor(tc::smem_addr(wt.bias[0]), kBiasK), id, false);
+      uint32_t const a0 = tc::smem_addr(dst);
+#pragma unroll
+      for (int ks = 0; ks < kChunk / 16; ++ks)
+        tc::mma_bf16(c.tmem, tc::desc_kmajor(a0 + ks * 256, kChunk),
+                     tc::desc_kmajor(b0 + (k * (kChunk / 16) + ks) * 256, kIn), id, true);
+      if (k != 1) tc::mma_commit(c.mbar);
+    }
+  }
+  if (!await_mma(c, phase)) return false;
+  float v[kW];
+  read_acc(c.tmem, v);
+  for (int l = 1; l < kLayers; ++l) {
+    uint8_t *const dst = buf[(l - 1) & 1];
+#pragma unroll
+    for (int q = 0; q < kW; q += 8) store_row8_relu(dst, c.t, q, kW, v + q);
+    publish(c.bar);
+    if (c.t == 0) {
+      tc::fence_after_sync();
+      issue_forward(wt, l, dst, c.tmem);
+      tc::mma_commit(c.mbar);
+    }
+    if (!await_mma(c, phase)) return false;
+    read_acc(c.tmem, v);
+  }
+#pragma unroll
+  for (int j = 0; j < kW; ++j) out[j] = v[j];
+  return true;
 }
 
 // Raw outputs of n points (features: n x 6 = position, normal).
@@ -463,9 +529,8 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     float f[6] = {0, 0, 0, 0, 0, 1};
     if (row < n)
       for (int k = 0; k < 6; ++k) f[k] = feat[6 * static_cast<int64_t>(row) + k];
-    encode_row(c.x, c.t, G, f);
     float o[kW];
-    if (!forward(S.wt, c, phase, false, o)) {
+    if (!forward_infer(S.wt, G, c, phase, f, o)) {
       if (c.t == 0) atomicExch(G.err, 1);
       aborted = true;
       break;
@@ -692,9 +757,8 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_guide_infer(const __grid_c
     infer_features(I, cur, f);
     if (valid(tile + step)) infer_gather(I, row_of(tile + step), nxt);
     float4 const h2 = valid(tile + 2 * step) ? I.hits[row_of(tile + 2 * step)] : miss_hit();
-    encode_row(c.x, c.t, G, f);
     float o[kW];
-    if (!forward(S.wt, c, phase, false, o)) {
+    if (!forward_infer(S.wt, G, c, phase, f, o)) {
       if (c.t == 0) atomicExch(G.err, 1);
       aborted = true;
       break;
