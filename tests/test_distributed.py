@@ -101,3 +101,64 @@ def test_a_rank_that_leaves_is_reported_not_waited_for(tmp_path):
     # rank 0's reduce fails with an error instead of hanging
     assert procs[0].exitcode == 0
     assert (tmp_path / "error0.txt").exists()
+
+
+def test_jobs_assigned_by_cost_once_each_and_balanced():
+    from xyz_b200 import scenes
+    from xyz_b200.distributed import assign_by_cost, job_cost
+    work = [(e.scene.n_tris, e.width, e.height, e.spp) for e in scenes.batch_workload(16)]
+    costs = [job_cost(*w) for w in work]
+    for world in (1, 2, 3, 8):
+        parts = assign_by_cost(costs, world)
+        assert sorted(j for p in parts for j in p) == list(range(len(costs)))
+        loads = [sum(costs[j] for j in p) for p in parts]
+        # longest-first greedy: no rank exceeds the mean by more than one job
+        assert max(loads) <= sum(costs) / world + max(costs) + 1e-6
+        assert parts == assign_by_cost(costs, world)
+    assert assign_by_cost([5.0, 1.0, 4.0, 2.0], 2) == [[0, 1], [2, 3]]
+    with pytest.raises(ValueError):
+        assign_by_cost([1.0], 0)
+
+
+class _FakeGuide:
+    """Stands in for api.Guide on CPU: a parameter vector."""
+
+    def __init__(self, p):
+        self.p = np.asarray(p, np.float32)
+
+    def params(self):
+        return self.p.copy()
+
+    def set_params(self, p):
+        self.p = np.asarray(p, np.float32).copy()
+
+
+def _guide_worker(rank, world, port, out_dir):
+    import datetime
+    import sys
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from xyz_b200.distributed import broadcast_guide
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    try:
+        g = _FakeGuide(np.full(28992, float(rank + 1), np.float32) * np.arange(28992, dtype=np.float32))
+        broadcast_guide(g, src=0)
+        np.save(os.path.join(out_dir, f"params{rank}.npy"), g.p)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_guide_weights_broadcast_from_the_training_rank(tmp_path):
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_guide_worker, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(60)
+    assert all(p.exitcode == 0 for p in procs)
+    p0, p1 = np.load(tmp_path / "params0.npy"), np.load(tmp_path / "params1.npy")
+    assert np.array_equal(p0, np.arange(28992, dtype=np.float32))
+    assert np.array_equal(p1, p0)
