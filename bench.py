@@ -241,7 +241,8 @@ def adjoint_bench(steps: int, warmup: int):
     """Differentiable-rendering iteration on the 19,392-triangle room: render
     512 x 512 x 32 spp, L2 loss gradient to a target, 32 spp path-replay adjoint
     on the next 32 samples, max depth 6, Russian roulette off.  Returns
-    ms per iteration (primal + adjoint, CUDA events) and its split."""
+    ms per iteration (primal + adjoint, CUDA events, each iteration enqueued
+    behind a lead kernel) and its split."""
     import torch
     from xyz_b200 import api, diff, scenes
     W = H = 512
@@ -265,6 +266,9 @@ def adjoint_bench(steps: int, warmup: int):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         prim = adj = 0.0
         for _ in range(steps):
+            # the iteration is enqueued behind a lead kernel, so the host's
+            # enqueueing time does not show as idle GPU time between the events
+            gpu_lead(20.0)
             ev[0].record()
             img = R.render()
             d_img = 2.0 * (img - target)
@@ -592,6 +596,118 @@ def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_s
     return out
 
 
+def pinhole_rays(cam, width, height, n, rng):
+    """n pinhole rays through uniformly jittered random pixels of a width x
+    height image of `cam` (its eye, look-at point and vertical field of view
+    film_size / focal_length), as rows o.xyz, tmin, d.xyz, tmax."""
+    eye = np.asarray(cam.eye, np.float64)
+    fwd = np.asarray(cam.at, np.float64) - eye
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, (0.0, 1.0, 0.0))
+    right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    pix = rng.integers(0, width * height, n)
+    x = ((pix % width) + rng.random(n)) / width
+    y = ((pix // width) + rng.random(n)) / height
+    film = cam.film_size
+    d = (np.outer((x - 0.5) * film * width / height, right) + np.outer((0.5 - y) * film, up) +
+         cam.focal_length * fwd)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.empty((n, 8), np.float32)
+    r[:, 0:3] = eye
+    r[:, 3] = 1e-5
+    r[:, 4:7] = d
+    r[:, 7] = np.inf
+    return r
+
+
+def cosine_bounce_rays(sd, prim, hits, n, rng):
+    """n rays leaving recorded hit points (drawn with replacement from the
+    primary rays that hit) in cosine-weighted directions about the hit
+    triangle's geometric normal, turned to face the incoming ray."""
+    ids = hits[:, 3].view(np.int32)
+    hit = np.flatnonzero(ids >= 0)
+    sel = rng.choice(hit, n, replace=True)
+    tri = ids[sel] >> 1
+    o = prim[sel, 0:3].astype(np.float64) + hits[sel, 0:1].astype(np.float64) * prim[sel, 4:7]
+    v = sd.positions[sd.tris[tri]].astype(np.float64)
+    ng = np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0])
+    ng /= np.linalg.norm(ng, axis=1, keepdims=True)
+    ng[np.einsum("ij,ij->i", ng, prim[sel, 4:7]) > 0] *= -1.0
+    a = np.where(np.abs(ng[:, 0:1]) > 0.9, [[0.0, 1.0, 0.0]], [[1.0, 0.0, 0.0]])
+    t1 = np.cross(ng, a)
+    t1 /= np.linalg.norm(t1, axis=1, keepdims=True)
+    t2 = np.cross(ng, t1)
+    u1, u2 = rng.random(n), rng.random(n)
+    rr, ph = np.sqrt(u1), 2.0 * np.pi * u2
+    d = (t1 * (rr * np.cos(ph))[:, None] + t2 * (rr * np.sin(ph))[:, None] +
+         ng * np.sqrt(np.maximum(0.0, 1.0 - u1))[:, None])
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.empty((n, 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 3] = 1e-5
+    r[:, 4:7] = d
+    r[:, 7] = np.inf
+    return r
+
+
+def trace_micro_bench(scene, sd, n=1 << 24, seed=0, reps=5):
+    """Closest-hit throughput of xyzgpu_trace_closest on 2^24 rays of the
+    workload's scene: half pinhole camera rays, half cosine bounces from
+    recorded hit points of those (seed 0), resident on the device (512 MB of
+    rays, larger than L2).  CUDA-event time per launch (median of reps), work
+    per ray from one counted launch."""
+    import torch
+    rng = np.random.default_rng(seed)
+    half = n // 2
+    prim = pinhole_rays(sd.camera, W_PIX, H_PIX, half, rng)
+    rays = torch.from_numpy(prim).cuda()
+    hits = torch.empty((half, 4), dtype=torch.float32, device="cuda")
+    scene.trace_device(rays, hits)
+    h = hits.cpu().numpy()
+    bounce = cosine_bounce_rays(sd, prim, h, half, rng)
+    all_rays = torch.from_numpy(np.concatenate([prim, bounce])).cuda()
+    all_hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    del rays, hits
+    peak, peak_kind = measured_peaks()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(r, hts):
+        scene.trace_device(r, hts)
+        out = []
+        for _ in range(reps):
+            e0.record()
+            scene.trace_device(r, hts)
+            e1.record()
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return statistics.median(out)
+
+    res = {}
+    for name, lo, hi in (("all", 0, n), ("primary", 0, half), ("bounce", half, n)):
+        r, hts = all_rays[lo:hi], all_hits[lo:hi]
+        ms = timed(r, hts)
+        c = scene.trace_device(r, hts, counted=True)
+        nr = max(1, c["rays"])
+        algo = (RAY_IO_BYTES * c["rays"] + NODE_BYTES * c["nodes_visited"] +
+                (REF_BYTES + TRI_BYTES_ALGO) * c["tri_tests"]) / nr
+        gbs = algo * (hi - lo) / (ms * 1e-3) / 1e9
+        res[name] = {"rays": hi - lo, "ms": round(ms, 3), "mrays_per_s": round((hi - lo) / ms / 1e3, 1),
+                     "hit_rate": round(c["hits"] / nr, 4),
+                     "per_ray": {"nodes": round(c["nodes_visited"] / nr, 2),
+                                 "leaves": round(c["leaves_visited"] / nr, 2),
+                                 "tri_tests": round(c["tri_tests"] / nr, 2)},
+                     "algorithmic_bytes_per_ray": round(algo, 1),
+                     "achieved_gbs": round(gbs, 1), "frac_of_hbm": round(gbs / peak, 4)}
+    res["peak_gbs"] = peak
+    res["peak_source"] = peak_kind
+    res["config"] = ("2^24 rays of the workload's scene and kd-tree: 2^23 pinhole camera rays through "
+                     "jittered random pixels, 2^23 cosine-weighted bounces from their recorded hit points "
+                     "(seed 0); device-resident, xyzgpu_trace_closest")
+    del all_rays, all_hits
+    return res
+
+
 def guide_profile_case():
     """The guide's kernels on a small case for ncu: one Adam step on 65,536
     synthetic training rows (k_guide_gradient), then one guided 64-spp pass
@@ -855,8 +971,9 @@ def run_gpu_arm(args, rank, world):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(sd)
-    adjoint = batch = guiding = None
+    adjoint = batch = guiding = micro = None
     if rank == 0 and world == 1 and not args.no_extras:
+        micro = trace_micro_bench(scene, sd)
         adjoint = adjoint_bench(args.steps, args.warmup)
         batch = batch_bench(args.steps, args.warmup)
         guiding = guide_bench()
@@ -870,7 +987,7 @@ def run_gpu_arm(args, rank, world):
             "config": workload_config(stats) | {"parallelism": f"sample-parallel x{world}",
                                                  "waves_per_step": counters["waves"]},
             "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-            "adjoint": adjoint, "batch": batch, "guiding": guiding,
+            "trace_micro": micro, "adjoint": adjoint, "batch": batch, "guiding": guiding,
             "clocks": clk, "wall_ms_timed_region": round(wall_ms, 1),
             "render_counters": counters,
         }
