@@ -414,7 +414,7 @@ GUIDE_QUERY_FLOPS = 2 * (192 * 64 + 3 * 64 * 64 + 64 * 40)
 
 
 def guide_bench(band: int = 32, ref_spp: int = 65536, pass_spp: int = 64, plan_spp: int = 2048,
-                max_seconds: float = 30.0, guide_cfg=None, variants=(), repeats: int = 2):
+                max_seconds: float = 30.0, guide_cfg=None, variants=(), repeats: int = 3):
     """Time to relative MSE 0.01, guided vs plain, on the indirect-lit room
     (196,146 triangles; light only through a 0.1 m gap), 1024 x 1024 camera,
     max depth 10, Russian roulette 0.2.  The error is measured on `band` image
