@@ -47,7 +47,9 @@ REF_BYTES = 4
 RAY_IO_BYTES = 32 + 16
 
 
-def workload_config(stats=None):
+def workload_config():
+    """The workload, identical in both arms' lines (the GPU arm's kd-tree
+    statistics, parallelism and waves go beside it)."""
     cfg = {
         "workload": "spheres-1M: 3 displaced level-7 icospheres + ground + spherical light r=0.3, "
                     "984,322 triangles, 1024x1024, 64 spp, max depth 10, pinhole fov 40, "
@@ -56,9 +58,6 @@ def workload_config(stats=None):
         "triangles": 984322, "width": W_PIX, "height": H_PIX, "spp": SPP, "max_depth": MAX_DEPTH,
         "seed": SEED, "l2_flush": "256 MiB buffer written between timed steps",
     }
-    if stats:
-        cfg["kd_tree"] = {"nodes": stats["n_nodes"], "leaf_refs": stats["n_leaf_refs"],
-                          "depth": stats["max_depth"], "build_ms": round(stats["build_ms"], 1)}
     return cfg
 
 
@@ -984,8 +983,10 @@ def run_gpu_arm(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene generator)",
-            "config": workload_config(stats) | {"parallelism": f"sample-parallel x{world}",
-                                                 "waves_per_step": counters["waves"]},
+            "config": workload_config(),
+            "kd_tree": {"nodes": stats["n_nodes"], "leaf_refs": stats["n_leaf_refs"],
+                        "depth": stats["max_depth"], "build_ms": round(stats["build_ms"], 1)},
+            "parallelism": f"sample-parallel x{world}", "waves_per_step": counters["waves"],
             "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
             "trace_micro": micro, "adjoint": adjoint, "batch": batch, "guiding": guiding,
             "clocks": clk, "wall_ms_timed_region": round(wall_ms, 1),
