@@ -142,10 +142,10 @@ __device__ __forceinline__ void store_row8(uint8_t *buf, int r, int c, int cols,
 // then the at most 10 bins of its window are computed.  In bin units (u = 32 s,
 // t_j = u - j - 1/2) the bins are g_j = exp(-t_j^2 / 2), and
 // g_{j+1} = g_j exp(t_j - 1/2), exp(t_{j+1} - 1/2) = exp(t_j - 1/2) / e: two
-// exponentials per input and two products per bin.  The window is stored as
-// bf16 pairs at even columns (4-byte stores, the window's neighbours in a
-// pair being 0), which halves the shared-memory stores of one-by-one 2-byte
-// writes and their bank conflicts.
+// exponentials per input and two products per bin, from the even column at
+// or below the window's first bin.  The window is stored as bf16 pairs at
+// even columns (4-byte stores, a neighbour outside the window being 0),
+// which halves the shared-memory stores of one-by-one 2-byte writes.
 //
 // Input coordinate of feature `dim` in [0, 1]: the position in the scene's
 // bounds, a normal component mapped from [-1, 1].
@@ -161,30 +161,24 @@ __device__ __forceinline__ void encode_dim(uint8_t *x, int r, int C, int c0, flo
   for (int q = 0; q < kBins; q += 8)
     *reinterpret_cast<uint4 *>(x + tc::blocked_offset(r, c0 + q, C)) = make_uint4(0, 0, 0, 0);
   float const u = s * static_cast<float>(kBins);
-  int const jlo = max(0, static_cast<int>(ceilf(u - 5.0f)));
-  float const t0 = u - (static_cast<float>(jlo) + 0.5f);
+  // the even column at or below the first bin within 4.5 sigma: the at most
+  // 10 bins within reach lie in the 12 columns from it, stored as 6 pairs
+  int const e0 = max(0, static_cast<int>(ceilf(u - 5.0f))) & ~1;
+  float const t0 = u - (static_cast<float>(e0) + 0.5f);
   float g = __expf(-0.5f * t0 * t0);
   float ratio = __expf(t0 - 0.5f);
   float v[12];
-  v[0] = v[11] = 0.0f;
 #pragma unroll
-  for (int t = 0; t < 10; ++t) {
-    int const j = jlo + t;
-    v[t + 1] = (j < kBins && fabsf(u - (static_cast<float>(j) + 0.5f)) <= 4.5f) ? g : 0.0f;
+  for (int t = 0; t < 12; ++t) {
+    v[t] = (e0 + t < kBins && fabsf(t0 - static_cast<float>(t)) <= 4.5f) ? g : 0.0f;
     g *= ratio;
     ratio *= 0.36787944117144233f;  // 1 / e
   }
-  // pairs from the even column at or below the window's first: bins
-  // (jlo + 2k, jlo + 2k + 1) when jlo is even, (jlo - 1 + 2k, jlo + 2k) when odd
-  int const odd = jlo & 1;
-  int const e0 = jlo - odd;
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
     int const c = e0 + 2 * k;
     if (c < kBins) {
-      float const a = odd ? v[2 * k] : v[2 * k + 1];
-      float const b = odd ? v[2 * k + 1] : (k < 5 ? v[2 * k + 2] : 0.0f);
-      __nv_bfloat162 const pr = __floats2bfloat162_rn(a, b);
+      __nv_bfloat162 const pr = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
       *reinterpret_cast<__nv_bfloat162 *>(x + tc::blocked_offset(r, c0 + c, C)) = pr;
     }
   }
