@@ -28,8 +28,8 @@
 // addresses).
 //
 // Autotuner: coordinate descent over the pixel tile of the slot order (tiles
-// make camera rays of neighbouring lanes coherent), the wave size (occupancy of
-// late bounces vs. memory) and the trace grid (CTAs per SM); each candidate is
+// make camera rays of neighbouring lanes coherent), the wave size (2^22 to
+// 2^27 paths: occupancy of late bounces vs. memory) and the trace grid (CTAs per SM); each candidate is
 // timed with CUDA events on this batch (optionally with capped samples) into
 // scratch films.
 #include <algorithm>
@@ -661,7 +661,7 @@ int xyzgpu_batch_autotune(xyzgpu_batch h, int trials, int probe_spp, void *strea
     int const occ = occupancy_grid(k_trace_queue<false, false, kModeBatch>, b.device) / sm_count(b.device);
     std::vector<int> tiles = {1, 4, 8, 16};
     std::vector<int> waves;
-    for (int64_t w = int64_t{1} << 22; w <= (int64_t{1} << 26); w <<= 1)
+    for (int64_t w = int64_t{1} << 22; w <= (int64_t{1} << 27); w <<= 1)
       if (w >= max_pix && w <= afford && w / 2 < total) waves.push_back(static_cast<int>(w));
     std::vector<int> ctas = {occ, std::max(1, occ * 2 / 3), std::max(1, occ / 2)};
     for (int knob = 0; knob < 3 && rc == XYZGPU_OK; ++knob) {
