@@ -293,11 +293,15 @@ int xyzgpu_scene_get_materials(xyzgpu_scene scene, float *albedo_xyz, float *emi
  * produces for the same scene, camera and parameters, adds
  *   d_albedo[3m + c] += sum_p d_film[p] . d film[p] / d albedo[m][c]
  *   d_emission[m]    += sum_p d_film[p] . d film[p] / d emission[m]
- * for the same sample paths (same seed and sample indices): each wave is traced
+ * for the same sample paths (same seed and sample indices): each wave runs
  * twice, a primal pass that keeps every path's radiance and a replay pass that
  * regenerates the same paths and, at each vertex, scatters
  * d_film . (radiance collected from that vertex on) / albedo into the vertex's
  * material and d_film . (emitted contribution at unit scale) into the light's.
+ * The primal pass also records each path's closest hit and shadow-ray result
+ * per bounce (20 bytes per path and bounce, stream-ordered device memory), and
+ * the replay reads them instead of tracing rays; when that memory cannot be
+ * had, the replay traces its paths again (same result).
  * The path sampling (Lambert cosine lobe, light choice by area, MIS weights) does
  * not depend on albedo or emission, so with Russian roulette off
  * (rr_threshold = 0) the result is the exact derivative of the rendered film;

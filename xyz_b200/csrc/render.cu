@@ -209,14 +209,31 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
                        "adjoint: allocating the primal radiance of %lld paths failed: %s",
                        static_cast<long long>(cap), cudaGetErrorString(e));
   }
-  // frees the adjoint's buffer on every return below
+  // Adjoint: the primal pass records each path's extension hits and shadow
+  // results per bounce (20 B per path and bounce) so that the replay traces no
+  // rays; without room for them the replay traces its paths again.
+  float4 *hit_cache = nullptr;
+  float *vis_cache = nullptr;
+  if (adj) {
+    int64_t const per_wave = std::min<int64_t>(cap, std::max<int64_t>(1, npix_total * rp.spp));
+    size_t const entries = static_cast<size_t>(per_wave) * static_cast<size_t>(iters);
+    if (cudaMallocAsync(reinterpret_cast<void **>(&hit_cache), entries * sizeof(float4), st) != cudaSuccess ||
+        cudaMallocAsync(reinterpret_cast<void **>(&vis_cache), entries * sizeof(float), st) != cudaSuccess) {
+      cudaGetLastError();  // not an error: the replay traces instead
+      if (hit_cache) cudaFreeAsync(hit_cache, st);
+      if (vis_cache) cudaFreeAsync(vis_cache, st);
+      hit_cache = nullptr;
+      vis_cache = nullptr;
+    }
+  }
+  // frees the adjoint's buffers on every return below
   struct FreeAsync {
-    float4 *p;
+    void *p;
     cudaStream_t st;
     ~FreeAsync() {
       if (p) cudaFreeAsync(p, st);
     }
-  } ltot_guard{ltot, st};
+  } ltot_guard{ltot, st}, hit_guard{hit_cache, st}, vis_guard{vis_cache, st};
 
   Grids const G = wave_grids(s.device);
   int const prof = rp.profile;
@@ -316,6 +333,14 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       XYZ_CUDA_TRY(cudaMemsetAsync(wv.counts, 0, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t), st));
       if (A.train_bounces > 0)
         XYZ_CUDA_TRY(cudaMemsetAsync(A.records, 0, static_cast<size_t>(A.npaths) * A.train_bounces * 16 * sizeof(float), st));
+      bool const cached = hit_cache != nullptr;
+      if (cached) {
+        // all-ones words are NaN: "no visible shadow ray" until the primal writes one
+        XYZ_CUDA_TRY(cudaMemsetAsync(vis_cache, 0xff, static_cast<size_t>(A.npaths) * iters * sizeof(float), st));
+        A.hit_cache = hit_cache;
+        A.vis_cache = vis_cache;
+        A.cache_stride = iters;
+      }
       int const gr = static_cast<int>(std::min<int64_t>(G.raygen, (A.npaths + kThreads - 1) / kThreads));
 #define XYZ_MARK(cls, start)              \
   do {                                    \
@@ -329,9 +354,13 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
         k_raygen<false><<<gr, kThreads, 0, st>>>(A);
         XYZ_MARK(0, false);
         ++launches;
+        // a replay over cached intersections traces no rays
+        bool const trace = !(replay && cached);
         for (int b = 0; b < iters; ++b) {
           XYZ_MARK(1, true);
-          if (counting)
+          if (!trace)
+            ;
+          else if (counting)
             k_trace_queue<false, true><<<G.trace_e, kThreads, 0, st>>>(A, b, pc);
           else
             k_trace_queue<false, false><<<G.trace_e, kThreads, 0, st>>>(A, b, pc);
@@ -374,7 +403,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
             k_shade<kModePlain><<<G.shade, kThreads, 0, st>>>(A, b);
           XYZ_MARK(2, false);
           XYZ_MARK(3, true);
-          if (counting)
+          if (!trace)
+            ;
+          else if (counting)
             k_trace_queue<true, true><<<G.trace_s, kThreads, 0, st>>>(A, b, pc);
           else if (replay)
             k_trace_queue<true, false, kModeAdjoint><<<G.trace_s_adj, kThreads, 0, st>>>(A, b, pc);
@@ -385,7 +416,7 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
           else
             k_trace_queue<true, false><<<G.trace_s, kThreads, 0, st>>>(A, b, pc);
           XYZ_MARK(3, false);
-          launches += 3;
+          launches += trace ? 3 : 1;
         }
         return XYZGPU_OK;
       };
@@ -396,6 +427,11 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
         int const gs = static_cast<int>(std::min<int64_t>(G.film, (A.npaths + kThreads - 1) / kThreads));
         k_adj_stash<<<gs, kThreads, 0, st>>>(A);
         ++launches;
+        if (cached) {
+          // the counters of an adjoint with cached intersections are the primal's rays
+          k_tally<<<1, 32, 0, st>>>(A, iters, w.tally);
+          ++launches;
+        }
         XYZ_CUDA_TRY(cudaMemsetAsync(wv.counts, 0, static_cast<size_t>(iters + 2) * kCountStride * sizeof(int32_t), st));
         int const rr = pass(true);
         if (rr) return rr;
@@ -408,8 +444,10 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
         XYZ_MARK(4, false);
         ++launches;
       }
-      k_tally<<<1, 32, 0, st>>>(A, iters, w.tally);
-      ++launches;
+      if (!(adj && cached)) {
+        k_tally<<<1, 32, 0, st>>>(A, iters, w.tally);
+        ++launches;
+      }
       XYZ_CUDA_TRY(cudaGetLastError());
       if (guide && A.train_bounces > 0) {
         XYZ_MARK(5, true);

@@ -144,6 +144,13 @@ struct WaveArgs {
   const float *dfilm;
   float *g_alb;
   float *g_em;
+  // adjoint with cached intersections: the primal pass records every path's
+  // extension hit and its shadow ray's target distance (NaN: not visible) per
+  // bounce, at slot * cache_stride + bounce; the replay reads them instead of
+  // tracing (both null otherwise)
+  float4 *hit_cache;
+  float *vis_cache;
+  int cache_stride;
   // batched renders
   const BatchJob *jobs;
   const WaveBlock *blocks;    // all blocks of the batch; a record's block indexes it
@@ -481,6 +488,7 @@ struct ShadowSink {
   static constexpr bool kTarget = true;  // only "is the target the closest hit?" matters
   const WaveArgs *A;
   uint32_t visible;
+  int bounce;
   XYZ_DEV int32_t target(int i) const { return __ldg(&A->s_target[i]); }
   XYZ_DEV void load(int i, f3 &o, f3 &d, float &tmin, float &tmax) const {
     float4 const a = __ldcs(&A->s_o[i]), b = __ldcs(&A->s_d[i]);
@@ -525,6 +533,8 @@ struct ShadowSink {
     }
     float4 pb = A->s_pb[i];
     int32_t const slot = kSpec ? A->s_slot[i] : __float_as_int(pb.w);
+    if (kMode == kModePlain && !kSpec && A->vis_cache)
+      A->vis_cache[static_cast<int64_t>(slot) * A->cache_stride + bounce] = h.t;
     if (kAdj) {
       // replay: pb is the unit-emission power; the light's scale is applied
       // here and the unit contribution goes to that light's emission gradient
@@ -566,18 +576,18 @@ __global__ void __launch_bounds__(kThreads, kShadow ? 10 : 9) k_trace_queue(Wave
   TraceCount tc{0u, 0u, 0u};
   uint32_t visible = 0;
   if (kShadow && kMode != kModePlain) {
-    ShadowSink<false, kMode> sink{&A, 0u};
+    ShadowSink<false, kMode> sink{&A, 0u, b};
     trace_persistent<kCount, kBatch>(A.S, n, &cnt[kCFetchSh], sink, tc);
     visible = sink.visible;
   } else if (kBatch) {
     ExtSink<true> sink{A.q_o[qi], A.q_d[qi], A.hits, &A};
     trace_persistent<kCount, true>(A.S, n, &cnt[kCFetchExt], sink, tc);
   } else if (kShadow && A.spectral) {
-    ShadowSink<true> sink{&A, 0u};
+    ShadowSink<true> sink{&A, 0u, b};
     trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
     visible = sink.visible;
   } else if (kShadow) {
-    ShadowSink<false> sink{&A, 0u};
+    ShadowSink<false> sink{&A, 0u, b};
     trace_persistent<kCount>(A.S, n, &cnt[kCFetchSh], sink, tc);
     visible = sink.visible;
   } else {
@@ -784,7 +794,9 @@ __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shad
     if (use_guide && i < n) load_mix(A.mix + 40 * static_cast<int64_t>(i), M);
     if (i < n) {
       slot = A.q_slot[qi][i];
-      float4 const h = A.hits[i];
+      int64_t const cache_at = static_cast<int64_t>(slot) * A.cache_stride + b;
+      float4 const h = (kAdj && A.hit_cache) ? A.hit_cache[cache_at] : A.hits[i];
+      if (kMode == kModePlain && A.hit_cache) A.hit_cache[cache_at] = h;
       int32_t const code = __float_as_int(h.w);
       if (code >= 0) {
         tri = code >> 1;
@@ -913,6 +925,32 @@ __global__ void __launch_bounds__(kThreads, kMode == kModeGuided ? 5 : 0) k_shad
                     pbv = mul3(S.power, beta);
                     light_mat = ls.mat;
                     if (!kAdj) pbv = scl3(pbv, __ldg(&S.emission[ls.mat]));
+                    if (kAdj && A.vis_cache) {
+                      // replay with cached intersections: the primal's shadow
+                      // ray gave the target's distance (NaN if it was not
+                      // visible); the shadow kernel's term, computed here
+                      push_sh = false;
+                      float const ts = A.vis_cache[static_cast<int64_t>(slot) * A.cache_stride + b];
+                      if (ts > 0.0f) {
+                        float const G = nk2nk3 / (ts * ts);
+                        float const dimp = static_cast<float>(kInvPi * static_cast<double>(G));
+                        float const dexp = 1.0f / S.light_area;
+                        float const dens = dimp / dexp;
+                        double const wgt = (static_cast<double>(G) * (kInvPi * kInvPi)) *
+                                           static_cast<double>(1.0f / (1.0f + dens * dens));
+                        float const *df = A.dfilm + 3 * static_cast<int64_t>(pixel);
+                        float const gl = df[0] * static_cast<float>(static_cast<double>(pbv.x) * wgt) +
+                                         df[1] * static_cast<float>(static_cast<double>(pbv.y) * wgt) +
+                                         df[2] * static_cast<float>(static_cast<double>(pbv.z) * wgt);
+                        if (gl != 0.0f) atomicAdd(&A.g_em[light_mat], gl);
+                        f3 const pe = scl3(pbv, __ldg(&S.emission[light_mat]));
+                        float4 L = A.radiance[slot];
+                        L.x += static_cast<float>(static_cast<double>(pe.x) * wgt);
+                        L.y += static_cast<float>(static_cast<double>(pe.y) * wgt);
+                        L.z += static_cast<float>(static_cast<double>(pe.z) * wgt);
+                        A.radiance[slot] = L;
+                      }
+                    }
                     if (use_guide) nee_pl = nk2 * static_cast<float>(kInvPi);
                     if (kImp) rho = use_imp ? importon_density(ic, v, sn, tan, bin) : 1.0f;
                     if (kSpecMat && kind == 3) {
