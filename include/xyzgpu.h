@@ -301,7 +301,8 @@ int xyzgpu_scene_get_materials(xyzgpu_scene scene, float *albedo_xyz, float *emi
  * The primal pass also records each path's closest hit and shadow-ray result
  * per bounce (20 bytes per path and bounce, stream-ordered device memory), and
  * the replay reads them instead of tracing rays; when that memory cannot be
- * had, the replay traces its paths again (same result).
+ * had, or the environment variable XYZGPU_ADJOINT_TRACE_REPLAY is set, the
+ * replay traces its paths again (same result).
  * The path sampling (Lambert cosine lobe, light choice by area, MIS weights) does
  * not depend on albedo or emission, so with Russian roulette off
  * (rr_threshold = 0) the result is the exact derivative of the rendered film;

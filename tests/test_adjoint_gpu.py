@@ -1,5 +1,6 @@
 """Path-replay adjoint (xyzgpu_adjoint) on the GPU: against the oracle's
-per-contribution gradient on the same sample paths, against central finite
+per-contribution gradient on the same sample paths (replaying recorded
+intersections and re-tracing), against central finite
 differences (h = 1e-3) of the GPU's own renders on 256 random parameters of the
 differentiable room scene, through the torch.autograd.Function harness, and its
 argument checks."""
@@ -12,7 +13,21 @@ from tests.helpers import ensure_port
 pytestmark = pytest.mark.gpu
 
 
-def test_adjoint_matches_oracle_gradient_on_same_paths():
+# the replay over intersections recorded by the primal pass (the default) and
+# the replay that traces its paths again (XYZGPU_ADJOINT_TRACE_REPLAY)
+REPLAYS = ["recorded", "traced"]
+
+
+def _replay_mode(monkeypatch, replay):
+    if replay == "traced":
+        monkeypatch.setenv("XYZGPU_ADJOINT_TRACE_REPLAY", "1")
+    else:
+        monkeypatch.delenv("XYZGPU_ADJOINT_TRACE_REPLAY", raising=False)
+
+
+@pytest.mark.parametrize("replay", REPLAYS)
+def test_adjoint_matches_oracle_gradient_on_same_paths(monkeypatch, replay):
+    _replay_mode(monkeypatch, replay)
     import torch
     from xyz_b200 import api, scenes
     sd = scenes.cornell_box(pinhole=True)
@@ -38,9 +53,11 @@ def test_adjoint_matches_oracle_gradient_on_same_paths():
     np.testing.assert_allclose(ge, ge_ref, rtol=2e-3, atol=2e-3 * np.abs(ge_ref).max())
 
 
-def test_adjoint_matches_oracle_with_russian_roulette_held():
+@pytest.mark.parametrize("replay", REPLAYS)
+def test_adjoint_matches_oracle_with_russian_roulette_held(monkeypatch, replay):
     """With Russian roulette on, both hold the roulette's survival scale
     constant: the same gradient on the same paths."""
+    _replay_mode(monkeypatch, replay)
     import torch
     from xyz_b200 import api, scenes
     sd = scenes.cornell_box(pinhole=True)

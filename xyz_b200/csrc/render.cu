@@ -1,6 +1,7 @@
 // Host side of xyzgpu_render / xyzgpu_adjoint (single scene) and
 // xyzgpu_render_noalloc; the kernels are in wavefront.cuh.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -214,7 +215,8 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   // rays; without room for them the replay traces its paths again.
   float4 *hit_cache = nullptr;
   float *vis_cache = nullptr;
-  if (adj) {
+  // XYZGPU_ADJOINT_TRACE_REPLAY set: the replay traces (no recorded intersections)
+  if (adj && !std::getenv("XYZGPU_ADJOINT_TRACE_REPLAY")) {
     int64_t const per_wave = std::min<int64_t>(cap, std::max<int64_t>(1, npix_total * rp.spp));
     size_t const entries = static_cast<size_t>(per_wave) * static_cast<size_t>(iters);
     if (cudaMallocAsync(reinterpret_cast<void **>(&hit_cache), entries * sizeof(float4), st) != cudaSuccess ||
