@@ -219,7 +219,9 @@ void xyzgpu_render_params_default(xyzgpu_render_params *rp);
  * `film` (W*H*3 XYZ sums).  Wavefront: ray generation, closest hit, shading
  * (emitter MIS, next-event estimation, Russian roulette, Lambert sampling),
  * shadow rays and film accumulation are separate kernels over SoA queues.
- * A host film is copied in and out through pinned staging inside the call. */
+ * A host film is copied in and out inside the call: directly when it is in
+ * page-locked memory (cudaMallocHost, cudaHostRegister), else through a pinned
+ * staging buffer. */
 int xyzgpu_render(xyzgpu_scene scene, const xyzgpu_camera *camera,
                   const xyzgpu_render_params *rp, float *film, void *stream);
 

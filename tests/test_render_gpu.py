@@ -119,6 +119,13 @@ def test_host_film_equals_device_film():
         h2 = h.copy()
         s.render(sd.camera, 40, 30, 3, seed=8, max_depth=8, film=h2, accumulate=True)
         assert np.allclose(h2, 2 * h, rtol=1e-6)
+        # a film in page-locked memory is copied to and from directly: the same sums
+        import torch
+        p = torch.zeros((30, 40, 3), dtype=torch.float32, pin_memory=True).numpy()
+        s.render(sd.camera, 40, 30, 3, seed=8, max_depth=8, film=p)
+        assert np.array_equal(p, h)
+        s.render(sd.camera, 40, 30, 3, seed=8, max_depth=8, film=p, accumulate=True)
+        assert np.array_equal(p, h2)
 
 
 def test_invalid_arguments_are_errors():

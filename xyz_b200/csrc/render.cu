@@ -182,6 +182,13 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   // pin and unpin host memory every time); the device lock held for the whole
   // call serialises their use, and the call returns only after the read-back.
   RenderWorkspace &fs = sw.ws;
+  // A host film in page-locked memory is copied to and from directly.
+  bool film_locked = false;
+  if (!adj && rp.film_location == XYZGPU_FILM_HOST) {
+    cudaPointerAttributes pa;
+    film_locked = cudaPointerGetAttributes(&pa, film) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+  }
   if (!adj && rp.film_location == XYZGPU_FILM_HOST) {
     if (fs.film_elems < film_elems) {
       XYZ_CUDA_TRY(cudaStreamSynchronize(st));
@@ -195,7 +202,9 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
       fs.film_elems = film_elems;
     }
     film_dev = fs.film_dev;
-    if (rp.accumulate) {
+    if (rp.accumulate && film_locked) {
+      XYZ_CUDA_TRY(cudaMemcpyAsync(film_dev, film, film_elems * sizeof(float), cudaMemcpyHostToDevice, st));
+    } else if (rp.accumulate) {
       std::memcpy(fs.film_pinned, film, film_elems * sizeof(float));
       XYZ_CUDA_TRY(cudaMemcpyAsync(film_dev, fs.film_pinned, film_elems * sizeof(float),
                                    cudaMemcpyHostToDevice, st));
@@ -464,7 +473,10 @@ int render_launch(SceneImpl &s, const xyzgpu_camera &cam, const xyzgpu_render_pa
   }
   XYZ_CUDA_TRY(cudaEventRecord(sw.done, st));
   sw.last = st;
-  if (!adj && rp.film_location == XYZGPU_FILM_HOST) {
+  if (!adj && rp.film_location == XYZGPU_FILM_HOST && film_locked) {
+    XYZ_CUDA_TRY(cudaMemcpyAsync(film, film_dev, film_elems * sizeof(float), cudaMemcpyDeviceToHost, st));
+    XYZ_CUDA_TRY(cudaStreamSynchronize(st));
+  } else if (!adj && rp.film_location == XYZGPU_FILM_HOST) {
     XYZ_CUDA_TRY(cudaMemcpyAsync(fs.film_pinned, film_dev, film_elems * sizeof(float), cudaMemcpyDeviceToHost, st));
     XYZ_CUDA_TRY(cudaStreamSynchronize(st));
     std::memcpy(film, fs.film_pinned, film_elems * sizeof(float));
