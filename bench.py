@@ -190,19 +190,19 @@ def cpu_sample(lib, threads, rows, spp, s0):
     return rows * W_PIX * spp / dt / 1e6, dt
 
 
-def cpu_baseline(sd, target_s=12.0, single_s=4.0):
+def cpu_baseline(sd, target_s=12.0):
     lib, kind, threads, build_s = cpu_setup(sd)
     rows, spp = cpu_plan(lib, threads, target_s)
     v, dt = cpu_sample(lib, threads, rows, spp, 0)
-    # the same renderer on one host thread, on a smaller band
-    rows1, spp1 = cpu_plan(lib, 1, single_s)
+    # the same renderer on one host thread: the same rows, one sample per pixel
+    rows1, spp1 = rows, 1
     v1, dt1 = cpu_sample(lib, 1, rows1, spp1, 0)
     return {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": kind,
             "build": getattr(lib, "build", "-O2"),
             "sample": f"{spp} spp over {rows} of 1024 rows (centre band) of the same scene and "
                       f"camera, {rows * W_PIX * spp} paths in {dt:.1f} s; tree build {build_s:.1f} s untimed",
             "single_core_value": round(v1, 4),
-            "single_core_sample": f"{spp1} spp over {rows1} rows (centre band), "
+            "single_core_sample": f"{spp1} spp over the same {rows1} rows, "
                                   f"{rows1 * W_PIX * spp1} paths in {dt1:.1f} s on 1 thread"}
 
 
